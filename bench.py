@@ -1,0 +1,476 @@
+"""Benchmark of the B200 Physis stencil path.
+
+Default workload (one GPU): 7-point diffusion, 512^3 float, one "step" = one
+solve of 1000 time steps run as PSStencilRun(m(g1->g2), m(g2->g1), 500) on
+the seeded cos-product field + U[0,1e-3) noise. Metric: lattice updates per
+second (GLUPS), whole job. Inputs (537 MB per grid) exceed the 126 MB L2, so
+no flush is needed between steps.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+                    [--workload c2|c2f64|c3|c1]
+
+Under torchrun (N > 1) every rank runs an independent replica on its own
+GPU (the path does not shard on one node: there is no data exchange), the
+timed region is bracketed by barriers and device syncs, and rank 0 prints the
+max over ranks. `--impl reference` times the reference's own CPU target
+(libphysis_rt_ref built from the reference sources, oracle/_ref) on the host
+cores for the same metric.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+COEF = [0.1, 0.1, 0.1, 0.1, 0.1, 0.1, 0.4]  # ce cw cn cs ct cb cc
+
+WORKLOADS = {
+    # name: (kernel, dtype, dims, time steps per solve, bytes per lattice update)
+    "c2": ("diffusion7", np.float32, (512, 512, 512), 1000, 8),
+    "c2f64": ("diffusion7", np.float64, (256, 256, 256), 1000, 16),
+    "c3": ("himeno", np.float32, (257, 257, 513), 200, 56),
+    "c1": ("diffusion7", np.float32, (64, 64, 64), 100, 8),
+}
+
+
+def describe(wl):
+    k, dt, dims, steps, _ = WORKLOADS[wl]
+    if k == "himeno":
+        return ("19-point Himeno Jacobi %dx%dx%d fp32, %d sweeps per solve, FP64 residual fused "
+                "per sweep" % (dims + (steps,)))
+    return ("7-point diffusion %dx%dx%d %s, %d time steps per solve (double-buffered "
+            "PSStencilRun), clamped faces" % (dims + ("fp32" if dt == np.float32 else "fp64", steps)))
+
+
+def peaks():
+    try:
+        with open(PEAKS_PATH) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# Inputs
+# ---------------------------------------------------------------------------
+def c2_field(dims, dtype, seed=2024):
+    """0.125(1-cos 2pi x/N)(1-cos 2pi y/N)(1-cos 2pi z/N) + U[0,1e-3), seeded."""
+    nx, ny, nz = dims
+    cx = (1 - np.cos(2 * np.pi * np.arange(nx) / nx)).astype(np.float64)
+    cy = (1 - np.cos(2 * np.pi * np.arange(ny) / ny)).astype(np.float64)
+    cz = (1 - np.cos(2 * np.pi * np.arange(nz) / nz)).astype(np.float64)
+    rng = np.random.default_rng(seed)
+    out = np.empty((nz, ny, nx), dtype=dtype)
+    for z in range(nz):
+        plane = 0.125 * cz[z] * np.outer(cy, cx) + 1e-3 * rng.random((ny, nx))
+        out[z] = plane.astype(dtype)
+    return out
+
+
+def himeno_fields(dims, seed=77):
+    from tests.gpu_util import himeno_inputs
+    nx, ny, nz = dims
+    return himeno_inputs((nz, ny, nx), seed)
+
+
+# ---------------------------------------------------------------------------
+# Clock sampling during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.QUERY,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# Our arm
+# ---------------------------------------------------------------------------
+class Dist:
+    def __init__(self, gpus):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+        if self.world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(self.local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                    device_id=torch.device("cuda", self.local))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def max(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum(self, v):
+        if not self.pg:
+            return v
+        import torch
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+def load_traffic(kernel_name):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            t = json.load(f)
+        return t.get(kernel_name)
+    except Exception:
+        return None
+
+
+def cpu_baseline_sample(wl, field=None):
+    """The reference CPU target (1 thread) on a bounded sample of the workload."""
+    from oracle import oracle
+    k, dt, dims, steps, bpl = WORKLOADS[wl]
+    nx, ny, nz = dims
+    use_ref = oracle.ref_available()
+    if k == "himeno":
+        p, coef = himeno_fields(dims)
+        sweeps = 4
+        if use_ref:
+            _, secs = oracle.ref_himeno(p, coef, 0.8, sweeps)
+        else:
+            t0 = time.perf_counter()
+            oracle.himeno(p, coef, 0.8, sweeps)
+            secs = time.perf_counter() - t0
+        pts = (nx - 2) * (ny - 2) * (nz - 2) * sweeps
+        sample = "%dx%dx%d, %d sweeps" % (nx, ny, nz, sweeps)
+    else:
+        f = field if field is not None else c2_field(dims, dt)
+        count = 12 if nx * ny * nz >= 1 << 26 else 100
+        if use_ref:
+            _, secs = oracle.ref_diffusion7(f, count, np.asarray(COEF, dt))
+        else:
+            t0 = time.perf_counter()
+            oracle.diffusion7(f, count, np.asarray(COEF, dt))
+            secs = time.perf_counter() - t0
+        pts = nx * ny * nz * count
+        sample = "%dx%dx%d %s, %d time steps" % (nx, ny, nz, np.dtype(dt).name, count)
+    kind = "reference" if use_ref else "port"
+    who = ("reference CPU target: libphysis_rt_ref built from the reference runtime sources + "
+           "translator-shaped run loop" if use_ref else "oracle port (C restatement)")
+    return {"value": pts / secs / 1e9, "unit": "GLUPS", "cores": 1, "kind": kind,
+            "sample": sample + "; " + who + "; run loop only, copies excluded"}
+
+
+def run_ours(args):
+    dist = Dist(args.gpus)
+    os.environ["PHYSIS_B200_DEVICE"] = str(dist.local)
+    import physis_b200 as ps
+    ps.PSInit()
+    wl = args.workload
+    kname, dt, dims, tsteps, bpl = WORKLOADS[wl]
+    nx, ny, nz = dims
+    ptype = ps.PS_FLOAT if dt == np.float32 else ps.PS_DOUBLE
+    kernel = ps.HIMENO19 if kname == "himeno" else ps.DIFFUSION7
+    tune = ps.autotune(kernel, ptype, dims) if args.tune else ps.tune_get(kernel, ptype, dims)
+    if args.plain:
+        ps.set_impl(ps.IMPL_PLAIN)
+
+    # Inputs, pinned host buffers for the end-to-end leg.
+    if kname == "himeno":
+        p, coef = himeno_fields(dims)
+        host = p
+        grids = [ps.PSGrid3DFloatNew(nx, ny, nz) for _ in range(14)]
+        ps.PSGridCopyin(grids[0], p)
+        ps.PSGridCopyin(grids[1], p)
+        for i in range(12):
+            ps.PSGridCopyin(grids[2 + i], coef[i])
+        dom = ps.PSDomain3DNew(1, nx - 1, 1, ny - 1, 1, nz - 1)
+        m1 = ps.PSStencilMap(ps.HIMENO19, dom, *grids, 0.8)
+        m2 = ps.PSStencilMap(ps.HIMENO19, dom, *([grids[1], grids[0]] + grids[2:]), 0.8)
+        ps.himeno_residual_enable(m1, tsteps)
+        ps.himeno_residual_enable(m2, tsteps)
+        pts_per_step = (nx - 2) * (ny - 2) * (nz - 2) * tsteps
+        g_io = grids[0]
+    else:
+        host = c2_field(dims, dt)
+        grids = [ps.grid_new(ptype, dims), ps.grid_new(ptype, dims)]
+        ps.PSGridCopyin(grids[0], host)
+        dom = ps.PSDomain3DNew(0, nx, 0, ny, 0, nz)
+        m1 = ps.PSStencilMap(ps.DIFFUSION7, dom, grids[0], grids[1], *COEF)
+        m2 = ps.PSStencilMap(ps.DIFFUSION7, dom, grids[1], grids[0], *COEF)
+        pts_per_step = nx * ny * nz * tsteps
+        g_io = grids[0]
+
+    def solve():
+        ps.PSStencilRun(m1, m2, tsteps // 2)
+        return ps.last_run_stats()
+
+    # ---- device-resident timing ------------------------------------------
+    for _ in range(args.warmup):
+        solve()
+    ps.sync()
+    sampler = ClockSampler(dist.local)
+    dist.barrier()
+    ps.sync()
+    sampler.start()
+    ms_list, launches = [], 0
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ms, n = solve()
+        ms_list.append(ms)
+        launches += n
+    ps.sync()
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop()
+    dist.barrier()
+    dev_s = sum(ms_list) / 1e3
+    dev_s_max = dist.max(dev_s)
+    total_pts = dist.sum(pts_per_step * args.steps)
+    value = total_pts / dev_s_max / 1e9
+    per_launch_s = dev_s / launches
+    alg_bytes = bpl * (pts_per_step / tsteps)
+    hbm, peak_kind = peaks()
+    achieved = alg_bytes / per_launch_s / 1e9
+    kname_traffic = "k_himeno_tma" if kname == "himeno" else (
+        "k_diff7_tma_f32" if dt == np.float32 else "k_diff7_tma_f64")
+    if args.plain:
+        kname_traffic = kname_traffic.replace("tma", "plain")
+    traffic = load_traffic("%s_%dx%dx%d" % (kname_traffic, nx, ny, nz))
+
+    # ---- end to end through the C ABI, host buffers --------------------------
+    import ctypes
+    nbytes = host.nbytes
+    hp = ctypes.c_void_p()
+    ps.check(ps.lib.psb_host_alloc(nbytes, ctypes.byref(hp)), "psb_host_alloc")
+    pinned = np.ctypeslib.as_array((ctypes.c_char * nbytes).from_address(hp.value))
+    pinned = pinned.view(host.dtype).reshape(host.shape)
+    pinned[...] = host
+    e2e_steps = max(1, min(args.steps, 3))
+    ps.PSGridCopyin(g_io, pinned)
+    solve()
+    ps.PSGridCopyout(g_io, pinned)
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        ps.PSGridCopyin(g_io, pinned)
+        solve()
+        ps.PSGridCopyout(g_io, pinned)
+    e2e_s = dist.max(time.perf_counter() - t0)
+    e2e_value = dist.sum(pts_per_step * e2e_steps) / e2e_s / 1e9
+    ps.check(ps.lib.psb_host_free(hp), "psb_host_free")
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(wl, host if kname != "himeno" else None)
+
+    line = {
+        "metric": "lattice_updates_per_s_" + wl,
+        "value": value,
+        "unit": "GLUPS",
+        "n_gpus": dist.world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dev_s_max / args.steps * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if dt == np.float32 else "f64",
+        "data": "synthetic",
+        "config": {
+            "workload": describe(wl),
+            "step": "one solve of %d time steps (PSStencilRun of two maps x %d)" % (tsteps, tsteps // 2),
+            "inputs_vs_l2": "%.0f MB per grid > 126 MB L2; no flush needed" % (host.nbytes / 1e6),
+            "parallelism": "replicas (one independent solve per GPU, no exchange)",
+            "impl": "plain" if args.plain else "autotuned",
+            "tune": tune,
+            "hbm_gbs_effective": value * bpl,
+            "wall_s_timed": wall,
+        },
+        "roofline": {
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": hbm,
+            "unit": "GB/s",
+            "frac": achieved / hbm,
+            "traffic": traffic,
+            "peak_source": peak_kind,
+            "algorithmic_bytes_per_launch": alg_bytes,
+            "avg_launch_us": per_launch_s * 1e6,
+        },
+        "e2e": {"value": e2e_value, "unit": "GLUPS", "h2d_bytes_per_step": int(nbytes),
+                "d2h_bytes_per_step": int(nbytes), "steps": e2e_steps,
+                "path": "PSGridCopyin(pinned) + PSStencilRun + PSGridCopyout(pinned) via the C ABI"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "cpu_baseline": cpu,
+    }
+    for g in grids:
+        ps.PSGridFree(g)
+    dist.close()
+    if dist.rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# Reference arm
+# ---------------------------------------------------------------------------
+def _ref_worker(args):
+    wl, dims, dt_name, count, seed = args
+    sys.path.insert(0, ROOT)
+    from oracle import oracle
+    dt = np.dtype(dt_name)
+    k = WORKLOADS[wl][0]
+    if k == "himeno":
+        p, coef = himeno_fields(dims, seed)
+        _, secs = oracle.ref_himeno(p, coef, 0.8, count)
+        nx, ny, nz = dims
+        return (nx - 2) * (ny - 2) * (nz - 2) * count, secs
+    f = c2_field(dims, dt, seed)
+    _, secs = oracle.ref_diffusion7(f, count, np.asarray(COEF, dt))
+    return dims[0] * dims[1] * dims[2] * count, secs
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import oracle
+    wl = args.workload
+    kname, dt, dims, tsteps, bpl = WORKLOADS[wl]
+    if not oracle.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "reference CPU runtime (oracle/_ref) was not built: reference sources "
+                          "absent at build time"}), flush=True)
+        return
+    import multiprocessing as mp
+    ncpu = os.cpu_count() or 1
+    try:
+        avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
+    except Exception:
+        avail = 16 << 30
+    per = (14 if kname == "himeno" else 3) * int(np.prod(dims)) * np.dtype(dt).itemsize
+    procs = max(1, min(ncpu, int(avail * 0.6 // per), args.ref_procs))
+    count = 2 if kname != "himeno" else 2
+    ctx = mp.get_context("spawn")
+    vals = []
+    with ctx.Pool(procs) as pool:
+        for i in range(args.warmup + args.steps):
+            jobs = [(wl, dims, np.dtype(dt).name, count, 1000 + j) for j in range(procs)]
+            t0 = time.perf_counter()
+            res = pool.map(_ref_worker, jobs)
+            wall = time.perf_counter() - t0
+            pts = sum(r[0] for r in res)
+            loop = max(r[1] for r in res)
+            if i >= args.warmup:
+                vals.append((pts, loop, wall))
+    pts = sum(v[0] for v in vals)
+    loop_s = sum(v[1] for v in vals)
+    value = pts / loop_s / 1e9
+    sample = ("%d independent %dx%dx%d %s solves of %d %s each per step, one per process, "
+              "run loop timed (copies excluded)" % (procs, dims[0], dims[1], dims[2],
+                                                     np.dtype(dt).name, count,
+                                                     "sweeps" if kname == "himeno" else "time steps"))
+    line = {
+        "metric": "lattice_updates_per_s_" + wl, "value": value, "unit": "GLUPS",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": loop_s / len(vals) * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32" if dt == np.float32 else "f64", "data": "synthetic",
+        "config": {"workload": describe(wl), "parallelism": "%d host processes" % procs},
+        "impl": "reference",
+        "cpu_baseline": {"value": value, "unit": "GLUPS", "cores": procs, "kind": "reference",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--tune", action="store_true", help="autotune before timing")
+    ap.add_argument("--plain", action="store_true", help="time the plain one-launch kernel")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-procs", type=int, default=64)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

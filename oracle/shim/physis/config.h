@@ -1,0 +1,1 @@
+/* Empty build-configuration header for the reference runtime (oracle build only). */

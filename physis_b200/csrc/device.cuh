@@ -1,0 +1,173 @@
+// Device helpers shared by the kernels: exact arithmetic, TMA/mbarrier PTX,
+// bounded waits and periodic halo images.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "internal.h"
+
+namespace psb {
+
+// Round-to-nearest multiply and add that the compiler never contracts into
+// an FMA: with these, a kernel computes a*b + c*d ... with exactly the
+// roundings of the reference CPU target built with -ffp-contract=off.
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ int32_t xmul(int32_t a, int32_t b) { return a * b; }
+__device__ __forceinline__ int64_t xmul(int64_t a, int64_t b) { return a * b; }
+__device__ __forceinline__ int32_t xadd(int32_t a, int32_t b) { return a + b; }
+__device__ __forceinline__ int64_t xadd(int64_t a, int64_t b) { return a + b; }
+
+// Vector of 16 bytes of T (4 floats or 2 doubles).
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<float> {
+  static constexpr int N = 4;
+  float v[4];
+};
+template <>
+struct Vec16<double> {
+  static constexpr int N = 2;
+  double v[2];
+};
+
+template <typename T>
+__device__ __forceinline__ Vec16<T> lds16(const T *p) {
+  Vec16<T> r;
+  if constexpr (sizeof(T) == 4) {
+    float4 q = *reinterpret_cast<const float4 *>(p);
+    r.v[0] = q.x; r.v[1] = q.y; r.v[2] = q.z; r.v[3] = q.w;
+  } else {
+    double2 q = *reinterpret_cast<const double2 *>(p);
+    r.v[0] = q.x; r.v[1] = q.y;
+  }
+  return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void stg16(T *p, const Vec16<T> &r) {
+  if constexpr (sizeof(T) == 4) {
+    *reinterpret_cast<float4 *>(p) = make_float4(r.v[0], r.v[1], r.v[2], r.v[3]);
+  } else {
+    *reinterpret_cast<double2 *>(p) = make_double2(r.v[0], r.v[1]);
+  }
+}
+
+// Streaming 16-byte global load that does not allocate in L1 (coefficient
+// fields are read exactly once per sweep).
+template <typename T>
+__device__ __forceinline__ Vec16<T> ldg16_stream(const T *p) {
+  Vec16<T> r;
+  if constexpr (sizeof(T) == 4) {
+    float4 q = __ldcs(reinterpret_cast<const float4 *>(p));
+    r.v[0] = q.x; r.v[1] = q.y; r.v[2] = q.z; r.v[3] = q.w;
+  } else {
+    double2 q = __ldcs(reinterpret_cast<const double2 *>(p));
+    r.v[0] = q.x; r.v[1] = q.y;
+  }
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// mbarrier + TMA (sm_90+ PTX, used here on sm_100a). No cluster multicast.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n"
+      ".reg .pred p;\n"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      "selp.u32 %0, 1, 0, p;\n"
+      "}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Wait for the barrier phase with a clock bound (~1.5 s at 1.9 GHz). Returns
+// false if it gave up; the caller then records an error and leaves.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > 3000000000LL) return false;
+  }
+  return true;
+}
+
+// 3-D tiled TMA load of one box into shared memory, completing on bar.
+// Coordinates are in elements; x * sizeof(T) must be a multiple of 16.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, uint64_t *bar,
+                                            int x, int y, int z) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
+  asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
+// ---------------------------------------------------------------------------
+// Periodic halo images. A pitched grid keeps `halo` ghost cells around the
+// interior; for periodic reads, ghost cell q must hold the value of the
+// interior cell ((q + n) % n) per axis. A kernel that writes interior point
+// p therefore also writes every ghost cell whose wrapped position is p.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ int wrap_images(int x, int n, int h, int *out) {
+  int k = 0;
+  out[k++] = x;
+  if (x >= n - h && x - n >= -h) out[k++] = x - n;
+  if (x < h && x + n < n + h) out[k++] = x + n;
+  return k;
+}
+
+template <typename T>
+__device__ __forceinline__ void store_periodic_images(T *origin, int64_t sy, int64_t sz,
+                                                      const int *n, int h, int x, int y, int z,
+                                                      T v) {
+  if (x >= h && x < n[0] - h && y >= h && y < n[1] - h && z >= h && z < n[2] - h) return;
+  int ix[3], iy[3], iz[3];
+  int kx = wrap_images(x, n[0], h, ix);
+  int ky = wrap_images(y, n[1], h, iy);
+  int kz = wrap_images(z, n[2], h, iz);
+  for (int c = 0; c < kz; c++)
+    for (int b = 0; b < ky; b++)
+      for (int a = 0; a < kx; a++) {
+        if (a == 0 && b == 0 && c == 0) continue;
+        origin[(int64_t)ix[a] + iy[b] * sy + iz[c] * sz] = v;
+      }
+}
+
+}  // namespace psb

@@ -1,0 +1,186 @@
+// Internal declarations of the B200 runtime (not part of the C ABI).
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/physis_b200.h"
+
+namespace psb {
+
+// ---------------------------------------------------------------------------
+// Device-side views
+// ---------------------------------------------------------------------------
+
+// A strided view of one grid: element (x, y, z) lives at
+// origin[x + y*sy + z*sz]. Dense grids have sy = nx, sz = nx*ny; pitched
+// grids have 128-byte rows and a resident halo around the origin.
+struct GridView {
+  void *origin;
+  int64_t sy, sz;
+  int n[3];
+  int type;      // PSPrimitiveType or -1 when unknown
+  int halo;      // cells of resident halo in every direction (0 for dense)
+};
+
+struct Dom3 {
+  int lo[3];
+  int hi[3];
+};
+
+// ---------------------------------------------------------------------------
+// Host-side objects
+// ---------------------------------------------------------------------------
+
+struct GridImpl {
+  __PSGrid pub;  // must stay first: handles are cast to __PSGrid*
+  union {
+    __PSGrid1D_dev d1;
+    __PSGrid2D_dev d2;
+    __PSGrid3D_dev d3;
+  } dev;
+  int type = -1;
+  int layout = PSB_LAYOUT_DENSE;
+  void *alloc = nullptr;
+  size_t alloc_bytes = 0;
+  int64_t sy = 0, sz = 0;     // element strides
+  int64_t origin_off = 0;     // elements from alloc to logical (0,0,0)
+  int64_t pitch = 0, rows = 0, planes = 0;
+  int pad_left = 0;           // x cells left of the origin
+  int halo = 0;               // y/z halo cells (and minimum x halo)
+  int ghost_valid = PSB_BOUNDARY_NONE;  // which halo content is current
+  bool user_type = false;
+  __PSGrid_devFreeFunc user_free = nullptr;
+  uint32_t magic = 0x50534232u;
+  // TMA descriptors built on demand, keyed by box shape.
+  std::map<uint64_t, CUtensorMap> tmaps;
+
+  int64_t nelems() const { return pub.num_elms; }
+  GridView view() const;
+};
+
+GridImpl *as_impl(const void *g);  // nullptr if g is not a grid of ours
+
+struct MapImpl {
+  int kernel_id = 0;
+  __PSDomain dom;
+  GridImpl *grids[PSB_MAX_GRIDS] = {};
+  int ngrids = 0;
+  double params[PSB_MAX_PARAMS] = {};
+  int nparams = 0;
+  int color = -1;           // -1 all points; 0 red; 1 black; 2 red then black
+  bool live = false;
+  // Himeno residual bookkeeping.
+  int residual_len = 0;
+  double *d_partials = nullptr;  // one per CTA
+  unsigned *d_ticket = nullptr;
+  unsigned *d_counter = nullptr;
+  double *d_history = nullptr;
+  int partials_cap = 0;
+};
+
+struct GenericDesc {
+  psb_generic_stencil host;
+  void *dev = nullptr;  // device copy of the compact table
+};
+
+// Kernel launch configuration for the fast paths.
+struct TuneKey {
+  int kernel, type, nx, ny, nz;
+  bool operator<(const TuneKey &o) const;
+};
+
+struct Runtime {
+  bool inited = false;
+  int device = 0;
+  int sm_count = 148;
+  size_t smem_optin = 227 * 1024;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_start = nullptr, ev_stop = nullptr;
+  cudaEvent_t ev_join = nullptr;  // orders the runtime stream with the legacy stream
+  int *d_error = nullptr;     // device error word (timeouts)
+  psb_status last_status = PSB_OK;
+  int impl = PSB_IMPL_AUTO;
+  bool use_graph = true;
+  double last_ms = 0.0;
+  int64_t last_launches = 0;
+  bool last_timed = false;
+  std::vector<MapImpl> maps;
+  std::vector<GenericDesc> generics;
+  std::map<TuneKey, psb_tune_config> tune;
+  bool tune_loaded = false;
+  std::string tune_path;
+  std::recursive_mutex mu;
+  // CUDA graphs of run loops, keyed by the map list and unroll.
+  std::map<std::string, cudaGraphExec_t> graphs;
+};
+
+Runtime &rt();
+// Order the runtime stream after work already queued on the legacy default
+// stream (where generated kernels launch), and the reverse.
+void legacy_join_in();
+void legacy_join_out();
+psb_status set_status(psb_status s);
+psb_status ensure_init();
+psb_status cuda_status(cudaError_t e, const char *what);
+// Group-1 style fatal check: print and exit like the reference.
+void fatal_cuda(cudaError_t e, const char *file, int line);
+#define PSB_FATAL(x)                                   \
+  do {                                                 \
+    cudaError_t e__ = (x);                             \
+    if (e__ != cudaSuccess) ::psb::fatal_cuda(e__, __FILE__, __LINE__); \
+  } while (0)
+#define PSB_TRY(x)                                                  \
+  do {                                                              \
+    cudaError_t e__ = (x);                                          \
+    if (e__ != cudaSuccess) return ::psb::cuda_status(e__, #x);     \
+  } while (0)
+#define PSB_CHECK(s)                         \
+  do {                                       \
+    psb_status s__ = (s);                    \
+    if (s__ != PSB_OK) return set_status(s__); \
+  } while (0)
+
+int type_size(int type);
+int type_from_size(int elm_size);  // float for 4, double for 8
+
+// TMA descriptor of a 3-D (or lower) grid, box (bx, by, 1). Coordinates used
+// by kernels are relative to the allocation for pitched grids (origin at
+// (pad_left, halo, halo)) and to the logical origin for dense grids.
+psb_status get_tmap(GridImpl *g, int bx, int by, const CUtensorMap **out);
+bool tma_eligible(const GridImpl *g);
+
+// Stencil launches (one application of map m on the runtime stream).
+psb_status launch_map(MapImpl &m, int color, int64_t *launches);
+psb_status prepare_ghosts(MapImpl &m);
+psb_status launch_halo_fill(GridImpl *g, int mode, cudaStream_t s);
+
+// Kernel launchers implemented in the .cu files.
+psb_status diffusion7_launch(MapImpl &m, const psb_tune_config &cfg, cudaStream_t s,
+                             int64_t *launches);
+psb_status himeno_launch(MapImpl &m, const psb_tune_config &cfg, cudaStream_t s,
+                         int64_t *launches);
+psb_status generic_launch(MapImpl &m, const GenericDesc &d, int color, cudaStream_t s,
+                          int64_t *launches);
+psb_status reduce_view(const GridView &v, int type, int op, const Dom3 &dom, double *result,
+                       cudaStream_t s);
+
+// Drop cached CUDA graphs (they bake grid pointers and tile shapes).
+void drop_all_graphs();
+void maps_forget_grid(const GridImpl *g);
+
+// Autotuning.
+psb_tune_config default_config(int kernel, int type, const int *n);
+psb_status tune_lookup(int kernel, int type, const int *n, psb_tune_config *cfg);
+
+// Host monotonic seconds.
+double now_s();
+
+}  // namespace psb

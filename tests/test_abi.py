@@ -1,0 +1,105 @@
+"""The C-ABI library: it loads and exports every symbol the header declares
+(CPU only: nothing here launches GPU work)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+
+
+def _strip_inline_bodies(text):
+    """Drop the bodies of static inline helpers (they are not exports)."""
+    out, i = [], 0
+    while True:
+        j = text.find("static inline", i)
+        if j < 0:
+            out.append(text[i:])
+            return "".join(out)
+        out.append(text[i:j])
+        k = text.find("{", j)
+        depth, m = 0, k
+        while m < len(text):
+            depth += text[m] == "{"
+            depth -= text[m] == "}"
+            m += 1
+            if depth == 0:
+                break
+        i = m
+
+
+def declared_functions():
+    names = set()
+    for hdr in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not hdr.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", hdr)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = _strip_inline_bodies(text)
+        text = re.sub(r"#[^\n]*(\\\n[^\n]*)*", "", text)
+        for m in re.finditer(r"([A-Za-z_][A-Za-z_0-9]*)\s*\(([^;{}]*)\)\s*;", text):
+            name = m.group(1)
+            pre = text[max(0, m.start() - 200):m.start()]
+            if "typedef" in pre.split(";")[-1]:
+                continue
+            names.add(name)
+    return sorted(names)
+
+
+def test_header_declares_the_reference_abi():
+    names = set(declared_functions())
+    for n in ["PSInit", "PSFinalize", "__PSGridNew", "__PSGridFree", "__PSGridCopyin",
+              "__PSGridCopyout", "__PSGridSwap", "__PSGridGetID", "__PSGridSet",
+              "PSDomain1DNew", "PSDomain2DNew", "PSDomain3DNew", "__PSReduceGridFloat",
+              "__PSReduceGridDouble", "__PSCheckCudaError", "__PSRandomInit",
+              "PSGrid3DFloatNew", "PSGrid3DDoubleNew", "PSGridCopyin", "PSGridCopyout",
+              "PSGridFree", "__PSStencilMap", "PSReduce"]:
+        assert n in names, n
+
+
+def test_library_exports_every_declared_symbol():
+    import physis_b200
+    lib = ctypes.CDLL(physis_b200.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+    assert hasattr(lib, "__ps_trace")
+
+
+def test_struct_layouts_match_reference_abi():
+    import physis_b200 as ps
+    # __PSGrid: void *p0; int dim[3]; int elm_size; int num_dims; int64 num_elms; dev*
+    assert ctypes.sizeof(ps.PSGridStruct) == 48
+    assert ps.PSGridStruct.num_elms.offset == 32 and ps.PSGridStruct.dev.offset == 40
+    assert ctypes.sizeof(ps.PSDomain) == 48
+
+
+def test_domain_constructors_need_no_gpu():
+    import physis_b200 as ps
+    d = ps.PSDomain3DNew(1, 31, 2, 30, 3, 29)
+    assert list(d.min) == [1, 2, 3] and list(d.max) == [31, 30, 29]
+    assert list(d.local_min) == [1, 2, 3] and list(d.local_max) == [31, 30, 29]
+    d2 = ps.PSDomain2DNew(0, 5, 1, 6)
+    assert list(d2.local_max)[:2] == [5, 6]
+
+
+def test_status_strings():
+    import physis_b200 as ps
+    for code, text in ps.STATUS.items():
+        assert ps.lib.psb_status_string(code).decode() == text
+
+
+def test_tune_cache_roundtrip(tmp_path, monkeypatch):
+    """The autotuner's cache is host-only state: set/get without a GPU."""
+    import subprocess
+    import sys
+    path = tmp_path / "tune.json"
+    code = (
+        "import physis_b200 as ps\n"
+        "ps.tune_set(ps.DIFFUSION7, ps.PS_FLOAT, (64, 64, 64), impl=2, tile_x=128, tile_y=4,"
+        " z_chunk=32, stages=8, t_depth=1)\n"
+        "print(ps.tune_get(ps.DIFFUSION7, ps.PS_FLOAT, (64, 64, 64)))\n")
+    env = dict(os.environ, PHYSIS_B200_TUNE_CACHE=str(path), PYTHONPATH=ROOT)
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    assert "'tile_x': 128" in out.stdout
