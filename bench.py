@@ -255,8 +255,9 @@ def run_ours(args):
         dom = ps.PSDomain3DNew(1, nx - 1, 1, ny - 1, 1, nz - 1)
         m1 = ps.PSStencilMap(ps.HIMENO19, dom, *grids, 0.8)
         m2 = ps.PSStencilMap(ps.HIMENO19, dom, *([grids[1], grids[0]] + grids[2:]), 0.8)
-        ps.himeno_residual_enable(m1, tsteps)
-        ps.himeno_residual_enable(m2, tsteps)
+        if not args.no_residual:
+            ps.himeno_residual_enable(m1, tsteps)
+            ps.himeno_residual_enable(m2, tsteps)
         pts_per_step = (nx - 2) * (ny - 2) * (nz - 2) * tsteps
         g_io = grids[0]
     else:
@@ -313,18 +314,20 @@ def run_ours(args):
     pinned = np.ctypeslib.as_array((ctypes.c_char * nbytes).from_address(hp.value))
     pinned = pinned.view(host.dtype).reshape(host.shape)
     pinned[...] = host
-    e2e_steps = max(1, min(args.steps, 3))
-    ps.PSGridCopyin(g_io, pinned)
-    solve()
-    ps.PSGridCopyout(g_io, pinned)
-    dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2e_steps):
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 3))
+    e2e_value = None
+    if e2e_steps:
         ps.PSGridCopyin(g_io, pinned)
         solve()
         ps.PSGridCopyout(g_io, pinned)
-    e2e_s = dist.max(time.perf_counter() - t0)
-    e2e_value = dist.sum(pts_per_step * e2e_steps) / e2e_s / 1e9
+        dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            ps.PSGridCopyin(g_io, pinned)
+            solve()
+            ps.PSGridCopyout(g_io, pinned)
+        e2e_s = dist.max(time.perf_counter() - t0)
+        e2e_value = dist.sum(pts_per_step * e2e_steps) / e2e_s / 1e9
     ps.check(ps.lib.psb_host_free(hp), "psb_host_free")
 
     cpu = None
@@ -463,7 +466,17 @@ def main():
     ap.add_argument("--plain", action="store_true", help="time the plain one-launch kernel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-procs", type=int, default=64)
+    ap.add_argument("--dims", default=None, help="override grid extents nx,ny,nz (profiling)")
+    ap.add_argument("--time-steps", type=int, default=None,
+                    help="override time steps per solve (profiling)")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-residual", action="store_true", help="c3: skip the fused residual")
     args = ap.parse_args()
+    if args.dims or args.time_steps:
+        k, dt, dims, ts, bpl = WORKLOADS[args.workload]
+        if args.dims:
+            dims = tuple(int(v) for v in args.dims.split(","))
+        WORKLOADS[args.workload] = (k, dt, dims, args.time_steps or ts, bpl)
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -103,7 +103,9 @@ void orc_himeno_f32(int nx, int ny, int nz, float *p0, float *p1,
   float *src = p0, *dst = p1;
 #define P(i, j, k) src[IDX3(i, j, k, nx, ny)]
   for (int it = 0; it < sweeps; it++) {
-    double g = 0.0;
+    /* gosa with Neumaier compensation so the checker is accurate to a few
+       ulp whatever the summation order of the implementation under test */
+    double g = 0.0, gc = 0.0;
     for (int k = 1; k < nz - 1; k++)
       for (int j = 1; j < ny - 1; j++)
         for (int i = 1; i < nx - 1; i++) {
@@ -121,9 +123,12 @@ void orc_himeno_f32(int nx, int ny, int nz, float *p0, float *p1,
           float ss = (s0 * a3[o] - P(i, j, k)) * bnd[o];
           float v = P(i, j, k) + omega * ss;
           dst[o] = v;
-          g += (double)ss * (double)ss;
+          double q = (double)ss * (double)ss;
+          double t = g + q;
+          if (fabs(g) >= fabs(q)) gc += (g - t) + q; else gc += (q - t) + g;
+          g = t;
         }
-    if (gosa) gosa[it] = g;
+    if (gosa) gosa[it] = g + gc;
     float *t = src;
     src = dst;
     dst = t;

@@ -107,6 +107,7 @@ struct Runtime {
   cudaEvent_t ev_join = nullptr;  // orders the runtime stream with the legacy stream
   int *d_error = nullptr;     // device error word (timeouts)
   psb_status last_status = PSB_OK;
+  char last_error[256] = {0};  // text of the last CUDA failure
   int impl = PSB_IMPL_AUTO;
   bool use_graph = true;
   double last_ms = 0.0;

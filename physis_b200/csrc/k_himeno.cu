@@ -149,30 +149,83 @@ __global__ void __launch_bounds__(256) k_himeno_plain(HimenoViews v, Dom3 d, flo
 }
 
 // --------------------------------------------------------------------------
-// TMA kernel (all 14 grids share one layout)
+// TMA kernel (all 14 grids share one layout), warp-specialised like the
+// 7-point kernel: a producer warp streams pressure planes (box TX+2V by
+// TY+2) through a ring of shared-memory stages, consumer warps wait on the
+// plane they need and release the one they are done with. Each consumer
+// thread owns V = 4 consecutive x points of one row and streams its twelve
+// coefficient vectors straight from global memory (read once, 16 bytes
+// per load), issued before it waits for the next plane so they overlap.
 // --------------------------------------------------------------------------
 struct HimenoGeom {
   int ax0, ay0, az0;
   int tiles_x, tiles_y, zchunk, stages, bx, by, stage_bytes, x_base;
-  int nx;  // row length, bounds the 16-byte coefficient loads
+  int nx;          // row length, bounds the 16-byte coefficient loads
+  int tx_threads;  // consumer threads along x (TX / V)
+  int ty_threads;  // consumer rows (TY)
 };
 
-__global__ void __launch_bounds__(256) k_himeno_tma(const __grid_constant__ CUtensorMap tin,
+__device__ __forceinline__ void consumer_bar(int nct) {
+  asm volatile("bar.sync 1, %0;" ::"r"(nct) : "memory");
+}
+
+// Residual of one CTA over its consumer threads (fixed order), then the
+// last CTA combines all partials in index order.
+__device__ void residual_finish_ws(const Residual &res, double mine, double *scratch, int nct,
+                                   int *shared_flag, bool skip) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = nct >> 5;
+  for (int o = 16; o > 0; o >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, o);
+  if (lane == 0) scratch[warp] = mine;
+  consumer_bar(nct);
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < nw; w++) t += scratch[w];
+    int last = 0;
+    if (!skip) {
+      res.partials[blockIdx.x] = t;
+      __threadfence();
+      unsigned k = atomicAdd(res.ticket, 1u);
+      last = (k == gridDim.x - 1);
+    }
+    *shared_flag = last;
+  }
+  consumer_bar(nct);
+  if (!*shared_flag) return;
+  __threadfence();
+  double acc = 0.0;
+  for (unsigned i = tid; i < gridDim.x; i += nct) acc += __ldcg(&res.partials[i]);
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  consumer_bar(nct);
+  if (lane == 0) scratch[warp] = acc;
+  consumer_bar(nct);
+  if (tid == 0) {
+    double sum = 0.0;
+    for (int w = 0; w < nw; w++) sum += scratch[w];
+    unsigned c = *res.counter;
+    res.history[c % (unsigned)res.history_len] = sum;
+    *res.counter = c + 1;
+    *res.ticket = 0;
+    __threadfence();
+  }
+}
+
+__global__ void __launch_bounds__(544) k_himeno_tma(const __grid_constant__ CUtensorMap tin,
                                                     float *pout, HimenoCoef cf, int64_t sy,
                                                     int64_t sz, Dom3 d, float omega,
                                                     HimenoGeom geo, Residual res, int *err) {
   constexpr int V = 4;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char *smem = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
-  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-  volatile int *flags = reinterpret_cast<volatile int *>(smem + 8 * 32);
-  double *scratch = reinterpret_cast<double *>(smem + 8 * 32 + 16);  // 32 doubles
-  unsigned char *ring = smem + 640;
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *empty = full + 32;
+  double *scratch = reinterpret_cast<double *>(smem + 512);   // 17 doubles
+  int *flag = reinterpret_cast<int *>(smem + 512 + 8 * 17);    // CTA-wide flags
+  unsigned char *ring = smem + 768;
 
-  const int tx = threadIdx.x, ty = threadIdx.y;
-  const int tid = ty * blockDim.x + tx;
-  const int TX = blockDim.x * V, TY = blockDim.y;
   const int S = geo.stages;
+  const int nct = geo.tx_threads * geo.ty_threads;
+  const int ncw = nct >> 5;
+  const int TX = geo.tx_threads * V, TY = geo.ty_threads;
   int b = blockIdx.x;
   const int tile_x = b % geo.tiles_x;
   b /= geo.tiles_x;
@@ -184,53 +237,76 @@ __global__ void __launch_bounds__(256) k_himeno_tma(const __grid_constant__ CUte
   const int ze = min(zb + geo.zchunk, d.hi[2]);
   const int nzl = ze - zb;
   const int np = nzl + 2;
-  const uint32_t tx_bytes = (uint32_t)(geo.bx * geo.by * sizeof(float));
+  const int tid = threadIdx.x;
 
   if (tid == 0) {
-    for (int i = 0; i < S; i++) mbar_init(&bars[i], 1);
-    flags[0] = 0;
-    flags[1] = 0;
+    for (int i = 0; i < S; i++) {
+      mbar_init(&full[i], 1);
+      mbar_init(&empty[i], ncw);
+    }
+    flag[1] = 0;
     mbar_fence_init();
-    tma_prefetch_desc(&tin);
   }
   __syncthreads();
-  int issued = 0;
-  auto issue = [&](int j) {
-    const int slot = j % S;
-    mbar_arrive_expect_tx(&bars[slot], tx_bytes);
-    tma_load_3d(ring + slot * geo.stage_bytes, &tin, &bars[slot], x0 - V + geo.ax0,
-                y0 - 1 + geo.ay0, zb - 1 + j + geo.az0);
-  };
-  if (tid == 0) {
-    const int first = min(S, np);
-    for (int j = 0; j < first; j++) issue(j);
-    issued = first;
+
+  if (tid >= nct) {
+    if (tid != nct) return;
+    tma_prefetch_desc(&tin);
+    const uint32_t bytes = (uint32_t)(geo.bx * geo.by * sizeof(float));
+    int slot = 0, round = 0, issued = 0;
+    bool ok = true;
+    for (int j = 0; j < np; j++) {
+      if (round > 0 && !mbar_wait_bounded(&empty[slot], (round - 1) & 1)) {
+        ok = false;
+        break;
+      }
+      mbar_arrive_expect_tx(&full[slot], bytes);
+      tma_load_3d(ring + slot * geo.stage_bytes, &tin, &full[slot], x0 - V + geo.ax0,
+                  y0 - 1 + geo.ay0, zb - 1 + j + geo.az0);
+      issued++;
+      if (++slot == S) {
+        slot = 0;
+        round++;
+      }
+    }
+    if (!ok) {
+      atomicExch(err, 1);
+      for (int j = 0; j < issued; j++) {
+        long long t0 = clock64();
+        while (!mbar_try_wait(&full[j % S], (j / S) & 1) && clock64() - t0 < 200000000LL) {
+        }
+      }
+    }
+    return;
   }
+
+  // ---------------- consumers ----------------
+  const int tx = tid % geo.tx_threads, ty = tid / geo.tx_threads;
+  const int lane = tid & 31;
   const int BX = geo.bx;
   const int rc = (ty + 1) * BX + V + tx * V;
-  auto plane = [&](int j) -> const float * {
-    return reinterpret_cast<const float *>(ring + (j % S) * geo.stage_bytes);
-  };
   const int xg0 = x0 + tx * V;
   const int yg = y0 + ty;
   const bool row_in = yg >= d.lo[1] && yg < d.hi[1];
   const bool vec_ok = xg0 + V <= geo.nx;
+  const bool xvec = xg0 >= d.lo[0] && xg0 + V <= d.hi[0];
+  auto wait_plane = [&](int slot, int round) -> bool {
+    bool ok = mbar_wait_bounded(&full[slot], round & 1);
+    return __all_sync(0xffffffffu, ok);
+  };
+  auto plane_ptr = [&](int slot) -> const float * {
+    return reinterpret_cast<const float *>(ring + slot * geo.stage_bytes);
+  };
   double acc = 0.0;
-  bool bad = false;
-  // Wait for planes 0 and 1 first (prologue, flag slot 1).
-  if (tid == 0) {
-    bool ok = mbar_wait_bounded(&bars[0], 0) && mbar_wait_bounded(&bars[1 % S], (1 / S) & 1);
-    flags[1] = ok ? 0 : 1;
-  }
-  __syncthreads();
-  bad = flags[1] != 0;
+  bool bad = !wait_plane(0, 0);
+  bad = bad || !wait_plane(1 % S, 1 / S);
+  int s_m = 0, s_c = 1 % S;        // slots of planes z-1 and z
+  int s_p = 1 % S, r_p = 0;        // slot / round of plane z+1 (advanced before use)
+  int64_t off = (int64_t)xg0 + (int64_t)yg * sy + (int64_t)zb * sz;
   for (int jj = 0; jj < nzl && !bad; jj++) {
     const int z = zb + jj;
-    // Coefficients of this plane: issue the 12 streaming loads before the
-    // ring wait so they overlap it.
     float co[12][V];
     if (row_in) {
-      const int64_t off = (int64_t)xg0 + (int64_t)yg * sy + (int64_t)z * sz;
 #pragma unroll
       for (int i = 0; i < 12; i++) {
         if (vec_ok) {
@@ -243,21 +319,17 @@ __global__ void __launch_bounds__(256) k_himeno_tma(const __grid_constant__ CUte
         }
       }
     }
-    const int jt = jj + 2;
-    if (tid == 0) flags[jj & 1] = mbar_wait_bounded(&bars[jt % S], (jt / S) & 1) ? 0 : 1;
-    __syncthreads();
-    if (flags[jj & 1]) {
+    if (++s_p == S) {
+      s_p = 0;
+      r_p++;
+    }
+    if (!wait_plane(s_p, r_p)) {
       bad = true;
       break;
     }
-    // Plane jj-1 was last read in iteration jj-1: refill its slot.
-    if (tid == 0 && jj >= 1 && issued < np && issued == jj - 1 + S) {
-      issue(issued);
-      issued++;
-    }
-    const float *pm = plane(jj), *pc = plane(jj + 1), *pp = plane(jt);
+    const float *pm = plane_ptr(s_m), *pc = plane_ptr(s_c), *pp = plane_ptr(s_p);
     if (row_in) {
-      float out[V];
+      float outv[V];
 #pragma unroll
       for (int v = 0; v < V; v++) {
         const int o = rc + v;
@@ -265,34 +337,42 @@ __global__ void __launch_bounds__(256) k_himeno_tma(const __grid_constant__ CUte
 #pragma unroll
         for (int i = 0; i < 12; i++) c[i] = co[i][v];
         float ss;
-        out[v] = himeno_point(c, pc[o], pc[o + 1], pc[o - 1], pc[o + BX], pc[o - BX], pp[o],
-                              pm[o], pp[o + BX], pp[o - BX], pm[o + BX], pm[o - BX],
-                              pc[o + 1 + BX], pc[o + 1 - BX], pc[o - 1 + BX], pc[o - 1 - BX],
-                              pp[o + 1], pm[o + 1], pp[o - 1], pm[o - 1], omega, &ss);
+        outv[v] = himeno_point(c, pc[o], pc[o + 1], pc[o - 1], pc[o + BX], pc[o - BX], pp[o],
+                               pm[o], pp[o + BX], pp[o - BX], pm[o + BX], pm[o - BX],
+                               pc[o + 1 + BX], pc[o + 1 - BX], pc[o - 1 + BX], pc[o - 1 - BX],
+                               pp[o + 1], pm[o + 1], pp[o - 1], pm[o - 1], omega, &ss);
         if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) acc += (double)ss * (double)ss;
       }
-      float *dst = pout + (int64_t)xg0 + (int64_t)yg * sy + (int64_t)z * sz;
-      if (xg0 >= d.lo[0] && xg0 + V <= d.hi[0]) {
-        *reinterpret_cast<float4 *>(dst) = make_float4(out[0], out[1], out[2], out[3]);
+      float *dst = pout + off;
+      if (xvec) {
+        *reinterpret_cast<float4 *>(dst) = make_float4(outv[0], outv[1], outv[2], outv[3]);
       } else {
 #pragma unroll
         for (int v = 0; v < V; v++)
-          if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) dst[v] = out[v];
+          if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) dst[v] = outv[v];
       }
     }
+    // Plane z-1 is done for this warp.
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&empty[s_m]);
+    s_m = s_c;
+    s_c = s_p;
+    off += sz;
+    (void)z;
   }
   if (bad) {
-    if (tid == 0) {
+    if (lane == 0) {
       atomicExch(err, 1);
-      for (int j = 0; j < issued; j++) {
-        long long t0 = clock64();
-        while (!mbar_try_wait(&bars[j % S], (j / S) & 1) && clock64() - t0 < 100000000LL) {
-        }
-      }
+      atomicExch(&flag[1], 1);
     }
-    return;
   }
-  if (res.partials) residual_finish(res, acc, scratch);
+  if (res.partials) {
+    // All consumer warps meet here (a timed-out warp too), so the named
+    // barriers below always complete.
+    consumer_bar(nct);
+    const bool skip = flag[1] != 0;
+    residual_finish_ws(res, acc, scratch, nct, &flag[0], skip);
+  }
 }
 
 // --------------------------------------------------------------------------
@@ -330,10 +410,12 @@ psb_status himeno_launch(MapImpl &m, const psb_tune_config &cfg, cudaStream_t s,
   Residual res = {nullptr, m.d_ticket, m.d_counter, m.d_history, m.residual_len};
   if (tma) {
     constexpr int V = 4;
-    int TX = std::max(V, cfg.tile_x / V * V);
-    int TY = std::max(1, cfg.tile_y);
-    if ((TX / V) * TY > 256) TY = 256 / (TX / V);
     HimenoGeom geo;
+    geo.tx_threads = std::max(1, cfg.tile_x / V);
+    geo.ty_threads = std::max(1, cfg.tile_y);
+    while ((geo.tx_threads * geo.ty_threads) % 32) geo.ty_threads++;
+    if (geo.tx_threads * geo.ty_threads > 512) return set_status(PSB_ERR_INVALID);
+    const int TX = geo.tx_threads * V, TY = geo.ty_threads;
     geo.bx = TX + 2 * V;
     geo.by = TY + 2;
     const CUtensorMap *map = nullptr;
@@ -351,20 +433,25 @@ psb_status himeno_launch(MapImpl &m, const psb_tune_config &cfg, cudaStream_t s,
       geo.nx = p0->pub.dim[0];
       int nzc = (d.hi[2] - d.lo[2] + geo.zchunk - 1) / geo.zchunk;
       int64_t nblocks = (int64_t)geo.tiles_x * geo.tiles_y * nzc;
-      size_t smem = 128 + 640 + (size_t)geo.stages * geo.stage_bytes;
+      size_t smem = 128 + 768 + (size_t)geo.stages * geo.stage_bytes;
       if (smem <= rt().smem_optin && nblocks < 0x7fffffff) {
-        static bool configured = false;
-        if (!configured) {
+        static size_t configured = 0;
+        if (smem > 48 * 1024 && smem > configured) {
+          // The opt-in limit covers static plus dynamic shared memory.
+          cudaFuncAttributes fa;
+          PSB_TRY(cudaFuncGetAttributes(&fa, k_himeno_tma));
+          size_t cap = rt().smem_optin - fa.sharedSizeBytes;
+          if (smem > cap) return set_status(PSB_ERR_INVALID);
           PSB_TRY(cudaFuncSetAttribute(k_himeno_tma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)rt().smem_optin));
-          configured = true;
+                                       (int)cap));
+          configured = cap;
         }
         PSB_CHECK(ensure_residual(m, (int)nblocks));
         if (m.residual_len > 0) res.partials = m.d_partials;
         HimenoCoef cf;
         for (int i = 0; i < 12; i++) cf.f[i] = (const float *)m.grids[2 + i]->view().origin;
-        dim3 block(TX / V, TY, 1);
-        k_himeno_tma<<<(unsigned)nblocks, block, smem, s>>>(
+        const int threads = geo.tx_threads * geo.ty_threads + 32;
+        k_himeno_tma<<<(unsigned)nblocks, threads, smem, s>>>(
             *map, (float *)m.grids[1]->view().origin, cf, p0->sy, p0->sz, d, omega, geo, res,
             rt().d_error);
         (*launches)++;

@@ -223,26 +223,26 @@ static psb_status run_maps(MapImpl **ms, int n, int iter) {
   int64_t launches = 0;
   legacy_join_in();
   PSB_TRY(cudaEventRecord(r.ev_start, r.stream));
-  const bool graph = r.use_graph && iter >= 2;
+  // The first iteration always runs eagerly: it performs every lazy set-up
+  // (TMA descriptors, residual buffers, kernel attributes) outside stream
+  // capture. The remaining iterations replay a CUDA graph of `unroll`
+  // iterations.
+  PSB_CHECK(launch_iteration(ms, n, &launches));
+  int rest = iter - 1;
+  const bool graph = r.use_graph && rest >= 2;
   if (!graph) {
-    for (int it = 0; it < iter; it++) PSB_CHECK(launch_iteration(ms, n, &launches));
+    for (int it = 0; it < rest; it++) PSB_CHECK(launch_iteration(ms, n, &launches));
   } else {
-    const int unroll = std::min(iter, kUnroll);
+    const int unroll = std::min(rest, kUnroll);
     std::string key = graph_key(ms, n, unroll);
     cudaGraphExec_t exec = nullptr;
-    int64_t per_graph = 0;
     auto it = r.graphs.find(key);
     // Kernel arguments (tensor maps, pointers) are baked into the graph;
-    // they only change when grids are freed, which drops all graphs.
-    if (it != r.graphs.end()) {
-      exec = it->second;
-    }
-    {
-      // Count launches of one iteration without launching (dry count).
-      int64_t c = 0;
-      for (int i = 0; i < n; i++) c += ms[i]->color == 2 ? 2 : 1;
-      per_graph = c * unroll;
-    }
+    // they only change when grids or maps are freed or the tuning changes,
+    // which drops all graphs.
+    if (it != r.graphs.end()) exec = it->second;
+    int64_t per_iter = 0;
+    for (int i = 0; i < n; i++) per_iter += ms[i]->color == 2 ? 2 : 1;
     if (!exec) {
       cudaGraph_t g;
       PSB_TRY(cudaStreamBeginCapture(r.stream, cudaStreamCaptureModeThreadLocal));
@@ -250,22 +250,25 @@ static psb_status run_maps(MapImpl **ms, int n, int iter) {
       psb_status st = PSB_OK;
       for (int u = 0; u < unroll && st == PSB_OK; u++) st = launch_iteration(ms, n, &dummy);
       cudaError_t e = cudaStreamEndCapture(r.stream, &g);
-      if (st != PSB_OK) {
+      if (st != PSB_OK || e != cudaSuccess) {
         if (e == cudaSuccess) cudaGraphDestroy(g);
-        return set_status(st);
+        cudaGetLastError();  // do not leave a capture error for later calls
+        return st != PSB_OK ? set_status(st) : cuda_status(e, "cudaStreamEndCapture");
       }
-      if (e != cudaSuccess) return cuda_status(e, "cudaStreamEndCapture");
       e = cudaGraphInstantiate(&exec, g, 0);
       cudaGraphDestroy(g);
-      if (e != cudaSuccess) return cuda_status(e, "cudaGraphInstantiate");
+      if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_status(e, "cudaGraphInstantiate");
+      }
       r.graphs[key] = exec;
     }
-    const int reps = iter / unroll;
+    const int reps = rest / unroll;
     for (int k = 0; k < reps; k++) {
       PSB_TRY(cudaGraphLaunch(exec, r.stream));
-      launches += per_graph;
+      launches += per_iter * unroll;
     }
-    for (int k = 0; k < iter % unroll; k++) PSB_CHECK(launch_iteration(ms, n, &launches));
+    for (int k = 0; k < rest % unroll; k++) PSB_CHECK(launch_iteration(ms, n, &launches));
   }
   PSB_TRY(cudaEventRecord(r.ev_stop, r.stream));
   legacy_join_out();

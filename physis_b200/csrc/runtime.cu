@@ -38,6 +38,9 @@ psb_status set_status(psb_status s) {
 
 psb_status cuda_status(cudaError_t e, const char *what) {
   if (__ps_trace) fprintf(__ps_trace, "physis_b200: %s: %s\n", what, cudaGetErrorString(e));
+  // Clear a non-sticky error so it is not reported again by a later call.
+  cudaGetLastError();
+  snprintf(rt().last_error, sizeof(rt().last_error), "%s: %s", what, cudaGetErrorString(e));
   if (e == cudaErrorMemoryAllocation) return set_status(PSB_ERR_NOMEM);
   return set_status(PSB_ERR_CUDA);
 }

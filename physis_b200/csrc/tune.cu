@@ -36,17 +36,17 @@ psb_tune_config default_config(int kernel, int type, const int *n) {
   c.t_depth = 1;
   if (kernel == PSB_KERNEL_HIMENO19) {
     c.tile_x = 64;
-    c.tile_y = 4;
-    c.z_chunk = 64;
-    c.stages = 8;
-  } else {
-    c.tile_x = type == PS_DOUBLE ? 32 : 64;
     c.tile_y = 8;
-    c.z_chunk = 64;
+    c.z_chunk = 32;
+    c.stages = 6;
+  } else {
+    c.tile_x = 32;
+    c.tile_y = 16;
+    c.z_chunk = 16;
     c.stages = 6;
   }
   // Small grids: shorter chunks keep enough CTAs in flight.
-  if (n[2] < 2 * c.z_chunk) c.z_chunk = std::max(8, n[2] / 4);
+  if (n[2] < 2 * c.z_chunk) c.z_chunk = std::max(4, n[2] / 4);
   return c;
 }
 
@@ -252,9 +252,9 @@ psb_status psb_autotune(int kernel_id, int type, const PSIndex *dims, int force,
   const bool him = kernel_id == PSB_KERNEL_HIMENO19;
   std::vector<int> txs = type == PS_DOUBLE ? std::vector<int>{16, 32, 64}
                                            : std::vector<int>{32, 64, 128};
-  std::vector<int> tys = him ? std::vector<int>{2, 4, 8} : std::vector<int>{4, 8, 16};
+  std::vector<int> tys = him ? std::vector<int>{4, 8, 16} : std::vector<int>{4, 8, 16, 32};
   std::vector<int> zcs = {16, 32, 64, 128};
-  std::vector<int> sts = him ? std::vector<int>{6, 8, 12} : std::vector<int>{4, 6, 8};
+  std::vector<int> sts = {4, 6, 8};
   for (int tx : txs)
     for (int ty : tys)
       for (int zc : zcs)
