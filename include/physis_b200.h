@@ -445,6 +445,28 @@ psb_status psb_himeno_residual_history(PSStencil map, double *out, int n);
 /* Reduction of a domain of a grid, FP64 result for every element type. */
 psb_status psb_reduce(__PSGrid *g, int op, const __PSDomain *dom, double *result);
 
+/* Allocation-free reduction (no counterpart in the reference). For callers
+ * that cannot call cudaMalloc -- a host framework that owns all device memory
+ * through its own allocator and budget, or a latency-critical loop where an
+ * allocation would synchronise the device -- this reduces a strided device
+ * array with the same kernel and order as psb_reduce but keeps its scratch in
+ * a fixed static device array of PSB_NOALLOC_SCRATCH_BYTES (held by every GPU
+ * that loads the library until exit). It calls no allocator.
+ *   data    device pointer to element (0,0,0) of the array
+ *   type    PS_FLOAT, PS_DOUBLE, PS_INT or PS_LONG; op a PSReduceOp
+ *   extent  nx, ny, nz, each in [1, PSB_NOALLOC_MAX_EXTENT] (else PSB_ERR_INVALID)
+ *   stride  elements between rows (>= nx) and between planes (>= stride[0]*ny)
+ *   stream  a cudaStream_t, or NULL for the legacy default stream
+ *   result  host pointer; the call returns once it is written (FP64 value)
+ * The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current: make it before any stream
+ * capture. All calls share the array and it keeps the last call's contents;
+ * calls that overlap on the GPU race. */
+#define PSB_NOALLOC_SCRATCH_BYTES 19200
+#define PSB_NOALLOC_MAX_EXTENT 2147483647LL
+psb_status psb_reduce_noalloc(const void *data, int type, int op, const int64_t *extent,
+                              const int64_t *stride, void *stream, double *result);
+
 /* Timing of the last psb_stencil_run / PSStencilRun: device time (CUDA
  * events on the runtime stream) and the number of kernel launches it
  * issued. */

@@ -15,6 +15,8 @@
 // Scratch (partials, ticket, result) lives in a runtime-owned buffer that is
 // allocated once.
 #include <cfloat>
+#include <cstdio>
+#include <mutex>
 
 #include "device.cuh"
 
@@ -169,4 +171,119 @@ psb_status reduce_view(const GridView &v, int type, int op, const Dom3 &dom, dou
   return PSB_OK;
 }
 
+// ===========================================================================
+// Allocation-free reduction entry point.
+//
+// Some callers cannot call cudaMalloc: a host framework that owns every byte
+// of device memory through its own allocator (and counts it against a
+// budget), or a latency-critical loop where a cudaMalloc/cudaFree would
+// synchronise the device. psb_reduce_noalloc serves them: the same k_reduce
+// kernel as psb_reduce, with its per-CTA partials, ticket and result kept in
+// the fixed, file-scope device array below instead of a runtime allocation.
+//
+//  * The array is kNoallocScratchBytes (19,200 bytes); every GPU that loads
+//    this library holds it until the process exits.
+//  * Host code cannot use the array's name as a device address, so on the
+//    first call on each device (with that device current) the address is
+//    fetched once with cudaGetSymbolAddress and cached. That first call
+//    should therefore come before any stream capture.
+//  * Every call shares the array and the array keeps the last call's
+//    contents: the ticket is cleared before each launch, and calls that
+//    overlap on the GPU (other streams, other host threads) race on it.
+//  * The launch never uses more CTAs than the array has partial slots, so
+//    the array does not bound the input; extents are bounded by the
+//    kernel's 32-bit indices (PSB_NOALLOC_MAX_EXTENT per dimension) and
+//    larger ones are rejected.
+// ===========================================================================
 }  // namespace psb
+
+namespace {
+constexpr size_t kNoallocScratchBytes = sizeof(psb::RAcc) * psb::kReduceMaxBlocks + 256;
+static_assert(kNoallocScratchBytes == PSB_NOALLOC_SCRATCH_BYTES,
+              "PSB_NOALLOC_SCRATCH_BYTES must describe the static scratch array");
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocScratchBytes];
+
+constexpr int kNoallocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_addr[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (set up once).
+cudaError_t noalloc_scratch(void **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kNoallocMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return cudaSuccess;
+}
+}  // namespace
+
+extern "C" psb_status psb_reduce_noalloc(const void *data, int type, int op,
+                                         const int64_t *extent, const int64_t *stride,
+                                         void *stream, double *result) {
+  using namespace psb;
+  if (!data || !extent || !stride || !result || op < PS_MAX || op > PS_PROD ||
+      (type != PS_FLOAT && type != PS_DOUBLE && type != PS_INT && type != PS_LONG)) {
+    fprintf(stderr, "psb_reduce_noalloc: invalid argument\n");
+    return set_status(PSB_ERR_INVALID);
+  }
+  for (int i = 0; i < 3; i++) {
+    if (extent[i] < 1 || extent[i] > PSB_NOALLOC_MAX_EXTENT) {
+      fprintf(stderr,
+              "psb_reduce_noalloc: extent[%d] = %lld is outside [1, %lld], the largest "
+              "extent this entry point reduces\n",
+              i, (long long)extent[i], (long long)PSB_NOALLOC_MAX_EXTENT);
+      return set_status(PSB_ERR_INVALID);
+    }
+  }
+  if (stride[0] < extent[0] || stride[1] < stride[0] * extent[1]) {
+    fprintf(stderr, "psb_reduce_noalloc: strides must not overlap rows or planes\n");
+    return set_status(PSB_ERR_INVALID);
+  }
+  void *scratch = nullptr;
+  cudaError_t e = noalloc_scratch(&scratch);
+  if (e != cudaSuccess) return cuda_status(e, "psb_reduce_noalloc: cudaGetSymbolAddress");
+  cudaStream_t s = (cudaStream_t)stream;
+  ReduceScratch sc;
+  sc.partials = (RAcc *)scratch;
+  sc.ticket = (unsigned *)((char *)scratch + sizeof(RAcc) * kReduceMaxBlocks);
+  sc.result = (double *)((char *)scratch + sizeof(RAcc) * kReduceMaxBlocks + 128);
+  GridView v;
+  v.origin = const_cast<void *>(data);
+  v.sy = stride[0];
+  v.sz = stride[1];
+  v.n[0] = (int)extent[0];
+  v.n[1] = (int)extent[1];
+  v.n[2] = (int)extent[2];
+  v.type = type;
+  v.halo = 0;
+  Dom3 d;
+  for (int i = 0; i < 3; i++) {
+    d.lo[i] = 0;
+    d.hi[i] = (int)extent[i];
+  }
+  const int64_t rows = extent[1] * extent[2];
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 7) / 8, kReduceMaxBlocks));
+  // The ticket must start at zero; the array keeps whatever the last call left.
+  e = cudaMemsetAsync(sc.ticket, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return cuda_status(e, "psb_reduce_noalloc: clear ticket");
+  switch (type) {
+    case PS_FLOAT: k_reduce<float><<<blocks, 256, 0, s>>>(v, d, op, sc); break;
+    case PS_DOUBLE: k_reduce<double><<<blocks, 256, 0, s>>>(v, d, op, sc); break;
+    case PS_INT: k_reduce<int32_t><<<blocks, 256, 0, s>>>(v, d, op, sc); break;
+    default: k_reduce<int64_t><<<blocks, 256, 0, s>>>(v, d, op, sc); break;
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_status(e, "psb_reduce_noalloc: launch");
+  e = cudaMemcpyAsync(result, sc.result, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return cuda_status(e, "psb_reduce_noalloc: result");
+  return PSB_OK;
+}
