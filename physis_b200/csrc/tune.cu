@@ -12,6 +12,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <dlfcn.h>
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -57,12 +58,23 @@ static std::string cache_path() {
   return std::string(h ? h : "/tmp") + "/.cache/physis_b200_tune.json";
 }
 
-static void load_cache() {
+// The tuned configurations measured on B200 ship next to the library
+// (physis_b200/tune_b200.json); a user cache entry for the same key wins.
+static std::string shipped_path() {
+  Dl_info info;
+  if (!dladdr((void *)&shipped_path, &info) || !info.dli_fname) return "";
+  std::string so = info.dli_fname;  // .../physis_b200/lib/libphysis_rt_b200.so
+  size_t a = so.find_last_of('/');
+  if (a == std::string::npos) return "";
+  std::string libdir = so.substr(0, a);
+  size_t b = libdir.find_last_of('/');
+  if (b == std::string::npos) return "";
+  return libdir.substr(0, b) + "/tune_b200.json";
+}
+
+static void parse_cache_file(const std::string &path) {
   Runtime &r = rt();
-  if (r.tune_loaded) return;
-  r.tune_loaded = true;
-  r.tune_path = cache_path();
-  FILE *f = fopen(r.tune_path.c_str(), "r");
+  FILE *f = fopen(path.c_str(), "r");
   if (!f) return;
   char line[512];
   while (fgets(line, sizeof(line), f)) {
@@ -78,6 +90,16 @@ static void load_cache() {
     if (got >= 11) r.tune[k] = c;
   }
   fclose(f);
+}
+
+static void load_cache() {
+  Runtime &r = rt();
+  if (r.tune_loaded) return;
+  r.tune_loaded = true;
+  r.tune_path = cache_path();
+  std::string shipped = shipped_path();
+  if (!shipped.empty()) parse_cache_file(shipped);
+  parse_cache_file(r.tune_path);
 }
 
 static void save_cache() {
