@@ -506,6 +506,15 @@ psb_status psb_batch_add(psb_batch *b, int kernel_id, __PSGrid *const *grids, in
 psb_status psb_batch_run(psb_batch *b, int mode);
 psb_status psb_batch_stats(psb_batch *b, double *device_ms, int64_t *launches,
                            int64_t *lattice_updates);
+/* Stop a member early once its relative residual is <= tol, checked every
+ * check_every steps (7-point: |u_{n+1}-u_n|_2 / |u_{n+1}|_2; Himeno:
+ * sqrt(gosa_n / gosa_0)); modes 0 and 1 only. */
+psb_status psb_batch_set_stop(psb_batch *b, int member, double tol, int check_every);
+/* Steps a member completed in the last run, its last residual (as defined
+ * above, -1 if never checked) and which of its two grids holds the result
+ * (0 or 1). */
+psb_status psb_batch_member_result(psb_batch *b, int member, int *steps_done, double *residual,
+                                   int *result_grid);
 psb_status psb_batch_free(psb_batch *b);
 
 /* ------------------------------------------------------------------------ */

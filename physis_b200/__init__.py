@@ -181,6 +181,10 @@ def _load():
         "psb_batch_stats": (S, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_double),
                                 ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
         "psb_batch_free": (S, [ctypes.c_void_p]),
+        "psb_batch_set_stop": (S, [ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int]),
+        "psb_batch_member_result": (S, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                        ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_int)]),
         "psb_server_create": (S, [ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
         "psb_server_submit": (S, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]),
         "psb_server_cancel": (S, [ctypes.c_void_p, ctypes.c_int64]),
@@ -523,3 +527,51 @@ class GenericStencil:
               "psb_generic_register")
         self.kernel_id = kid.value
         _generic_arity[self.kernel_id] = len(grids)
+
+
+# ---------------------------------------------------------------------------
+# Batching
+# ---------------------------------------------------------------------------
+BATCH_PERSISTENT, BATCH_GRAPH, BATCH_PLAIN_LOOP, BATCH_TUNED_LOOP = 0, 1, 2, 3
+
+
+class Batch:
+    """Many independent solves advanced together (psb_batch_*)."""
+
+    def __init__(self):
+        p = ctypes.c_void_p()
+        check(lib.psb_batch_create(ctypes.byref(p)), "psb_batch_create")
+        self.ptr = p
+        self.members = []
+
+    def add(self, kernel, grids, params, steps, tol=0.0, check_every=0):
+        gp = (ctypes.c_void_p * len(grids))(*[g.ptr.value for g in grids])
+        pp = (ctypes.c_double * max(1, len(params)))(*[float(v) for v in params])
+        m = ctypes.c_int()
+        check(lib.psb_batch_add(self.ptr, kernel, gp, len(grids), pp, len(params), steps,
+                                ctypes.byref(m)), "psb_batch_add")
+        if tol > 0 or check_every > 0:
+            check(lib.psb_batch_set_stop(self.ptr, m.value, tol, check_every), "psb_batch_set_stop")
+        self.members.append(list(grids))
+        return m.value
+
+    def run(self, mode=BATCH_PERSISTENT):
+        check(lib.psb_batch_run(self.ptr, mode), "psb_batch_run")
+
+    def stats(self):
+        ms, n, lups = ctypes.c_double(), ctypes.c_int64(), ctypes.c_int64()
+        check(lib.psb_batch_stats(self.ptr, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(lups)),
+              "psb_batch_stats")
+        return {"device_ms": ms.value, "launches": n.value, "lattice_updates": lups.value}
+
+    def result(self, member):
+        """(steps done, residual, grid holding the result)."""
+        st, res, which = ctypes.c_int(), ctypes.c_double(), ctypes.c_int()
+        check(lib.psb_batch_member_result(self.ptr, member, ctypes.byref(st), ctypes.byref(res),
+                                          ctypes.byref(which)), "psb_batch_member_result")
+        return st.value, res.value, self.members[member][which.value]
+
+    def free(self):
+        if self.ptr:
+            check(lib.psb_batch_free(self.ptr), "psb_batch_free")
+            self.ptr = ctypes.c_void_p()

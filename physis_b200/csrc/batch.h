@@ -1,0 +1,32 @@
+// Host-side batch member record shared by the batching and serving code.
+#pragma once
+
+#include <vector>
+
+#include "internal.h"
+
+namespace psb {
+
+struct BatchMemberHost {
+  int kind = 0;            // 0 diffusion clamped, 1 diffusion periodic, 2 Himeno
+  int kernel_id = 0;       // PSB_KERNEL_*
+  GridImpl *grids[14] = {};
+  int ngrids = 0;
+  double params[PSB_MAX_PARAMS] = {};
+  int nparams = 0;
+  int steps = 0;           // total steps of the solve
+  int check_every = 0;     // residual check interval (0: none)
+  double tol = 0.0;        // relative residual tolerance (0: run all steps)
+  int64_t points = 0;      // lattice updates per step
+};
+
+}  // namespace psb
+
+struct psb_batch;
+
+namespace psb {
+psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std::vector<int> &step0);
+psb_status batch_launch_persistent(psb_batch *b, cudaStream_t s, int64_t *launches);
+psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches);
+psb_status batch_add_member(psb_batch *b, const BatchMemberHost &m);
+}  // namespace psb

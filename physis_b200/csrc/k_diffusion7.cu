@@ -22,122 +22,9 @@
 // resident halo of a pitched grid, which every writer keeps current.
 #include <algorithm>
 
-#include "device.cuh"
+#include "k_diffusion7.cuh"
 
 namespace psb {
-
-template <typename T>
-struct C7 {
-  T ce, cw, cn, cs, ct, cb, cc;
-};
-
-template <typename T>
-__device__ __forceinline__ T diff7_point(const C7<T> &k, T c, T w, T e, T n, T s, T b, T t) {
-  T v = xmul(k.cc, c);
-  v = xadd(v, xmul(k.cw, w));
-  v = xadd(v, xmul(k.ce, e));
-  v = xadd(v, xmul(k.cs, s));
-  v = xadd(v, xmul(k.cn, n));
-  v = xadd(v, xmul(k.cb, b));
-  v = xadd(v, xmul(k.ct, t));
-  return v;
-}
-
-// Four (float) or two (double) consecutive x points of one row. c/n/s/b/t
-// are the 16-byte vectors of the points' own column in the planes/rows
-// around them; wl/er are the scalars left and right of the vector. The w
-// and e neighbours of a point are its vector's own elements shifted by one,
-// so the products cw*w and ce*e come from cw*c and ce*c of the neighbouring
-// lanes plus one scalar product each at the ends. The float form computes
-// products of natural element pairs with the packed sm_100 f32x2 multiply
-// (every lane an IEEE round-to-nearest product) and sums them with scalar
-// round-to-nearest adds in the reference order. The adds stay scalar on
-// purpose: a packed add that consumes a packed product is fused into a
-// packed FMA by the compiler even when both carry an explicit .rn, which
-// would change the rounding; a scalar add of a packed product is not.
-// xfix marks clamped x faces inside the vector: bit 4 = the first point is
-// x = 0 (its w is c), bit v = point v is x = nx-1 (its e is c).
-template <typename T>
-struct K7 {
-  C7<T> s;
-};
-template <>
-struct K7<float> {
-  C7<float> s;
-  float2 ce, cw, cn, cs, ct, cb, cc;
-};
-
-template <typename T>
-__device__ __forceinline__ K7<T> make_k7(const C7<T> &c) {
-  K7<T> k;
-  k.s = c;
-  if constexpr (sizeof(T) == 4) {
-    k.ce = make_float2(c.ce, c.ce);
-    k.cw = make_float2(c.cw, c.cw);
-    k.cn = make_float2(c.cn, c.cn);
-    k.cs = make_float2(c.cs, c.cs);
-    k.ct = make_float2(c.ct, c.ct);
-    k.cb = make_float2(c.cb, c.cb);
-    k.cc = make_float2(c.cc, c.cc);
-  }
-  return k;
-}
-
-__device__ __forceinline__ void mul4(float2 k, const Vec16<float> &x, float *p) {
-  const float2 lo = __fmul2_rn(k, make_float2(x.v[0], x.v[1]));
-  const float2 hi = __fmul2_rn(k, make_float2(x.v[2], x.v[3]));
-  p[0] = lo.x;
-  p[1] = lo.y;
-  p[2] = hi.x;
-  p[3] = hi.y;
-}
-
-template <typename T>
-__device__ __forceinline__ Vec16<T> diff7_row(const K7<T> &k, const Vec16<T> &c, T wl, T er,
-                                              const Vec16<T> &n, const Vec16<T> &s,
-                                              const Vec16<T> &b, const Vec16<T> &t,
-                                              unsigned xfix) {
-  constexpr int V = Vec16<T>::N;
-  T pcc[V], pcw[V], pce[V], ps[V], pn[V], pb[V], pt[V];
-  if constexpr (sizeof(T) == 4) {
-    mul4(k.cc, c, pcc);
-    mul4(k.cw, c, pcw);
-    mul4(k.ce, c, pce);
-    mul4(k.cs, s, ps);
-    mul4(k.cn, n, pn);
-    mul4(k.cb, b, pb);
-    mul4(k.ct, t, pt);
-  } else {
-#pragma unroll
-    for (int v = 0; v < V; v++) {
-      pcc[v] = xmul(k.s.cc, c.v[v]);
-      pcw[v] = xmul(k.s.cw, c.v[v]);
-      pce[v] = xmul(k.s.ce, c.v[v]);
-      ps[v] = xmul(k.s.cs, s.v[v]);
-      pn[v] = xmul(k.s.cn, n.v[v]);
-      pb[v] = xmul(k.s.cb, b.v[v]);
-      pt[v] = xmul(k.s.ct, t.v[v]);
-    }
-  }
-  T pw[V], pe[V];
-  pw[0] = xmul(k.s.cw, wl);
-#pragma unroll
-  for (int v = 1; v < V; v++) pw[v] = pcw[v - 1];
-#pragma unroll
-  for (int v = 0; v < V - 1; v++) pe[v] = pce[v + 1];
-  pe[V - 1] = xmul(k.s.ce, er);
-  if (xfix) {
-    if (xfix & 16u) pw[0] = pcw[0];
-#pragma unroll
-    for (int v = 0; v < V; v++)
-      if (xfix & (1u << v)) pe[v] = pce[v];
-  }
-  Vec16<T> r;
-#pragma unroll
-  for (int v = 0; v < V; v++)
-    r.v[v] = xadd(xadd(xadd(xadd(xadd(xadd(pcc[v], pw[v]), pe[v]), ps[v]), pn[v]), pb[v]), pt[v]);
-  return r;
-}
 
 // --------------------------------------------------------------------------
 // Plain kernel
@@ -177,253 +64,21 @@ __global__ void __launch_bounds__(256) k_diff7_plain(GridView in, GridView out, 
   }
 }
 
-// --------------------------------------------------------------------------
-// TMA z-streaming kernel, warp-specialised
-//
-// One producer warp streams input planes (box (TX+2V) x (TY+2) x 1) into a
-// ring of S shared-memory stages with TMA; `full[s]` completes when a plane
-// has landed, `empty[s]` when every consumer warp has finished with it.
-// Consumer warps never meet at a CTA-wide barrier: each waits on the plane
-// it needs and releases the one it is done with. Each consumer thread owns
-// V consecutive x points (16 bytes) of VY rows; z neighbours stay in
-// registers. Faces are resolved with selects only on threads/planes that
-// touch a face; all other points take a select-free path.
-// --------------------------------------------------------------------------
-struct TmaGeom {
-  int ax0, ay0, az0;      // tensor-map coordinates of logical (0,0,0)
-  int tiles_x, tiles_y;   // tiles over the domain
-  int zchunk;             // planes per CTA
-  int stages;             // ring depth
-  int bx, by;             // box (elements)
-  int stage_bytes;        // bytes between stages (128-aligned)
-  int x_base;             // x of the first tile (domain lo rounded down)
-  int tx_threads;         // consumer threads along x (TX / V)
-  int ty_threads;         // consumer thread rows (TY / VY)
-};
-
-constexpr int kVY = 2;
-
 template <typename T, bool PERIODIC>
 __global__ void __launch_bounds__(544) k_diff7_tma(const __grid_constant__ CUtensorMap tin,
                                                    GridView out, int nx, int ny, int nz, Dom3 d,
                                                    C7<T> k, TmaGeom geo, int images, int *err) {
-  constexpr int V = 16 / sizeof(T);
-  constexpr int VY = kVY;
   extern __shared__ __align__(128) unsigned char smem_raw[];
   // TMA destinations must be 128-byte aligned: align the base explicitly
   // (128 spare bytes are allocated for this).
   unsigned char *smem = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-  uint64_t *empty = full + 32;
-  unsigned char *ring = smem + 512;
-
-  const int S = geo.stages;
-  const int nct = geo.tx_threads * geo.ty_threads;  // consumer threads
-  const int ncw = nct >> 5;                          // consumer warps
-  const int TX = geo.tx_threads * V, TY = geo.ty_threads * VY;
   int b = blockIdx.x;
   const int tile_x = b % geo.tiles_x;
   b /= geo.tiles_x;
   const int tile_y = b % geo.tiles_y;
   const int zc = b / geo.tiles_y;
-  const int x0 = geo.x_base + tile_x * TX;
-  const int y0 = d.lo[1] + tile_y * TY;
-  const int zb = d.lo[2] + zc * geo.zchunk;
-  const int ze = min(zb + geo.zchunk, d.hi[2]);
-  const int nzl = ze - zb;  // output planes
-  const int np = nzl + 2;   // input planes zb-1 .. ze
-  const int tid = threadIdx.x;
-
-  if (tid == 0) {
-    for (int i = 0; i < S; i++) {
-      mbar_init(&full[i], 1);
-      mbar_init(&empty[i], ncw);
-    }
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  if (tid >= nct) {
-    // ---------------- producer warp ----------------
-    if (tid != nct) return;
-    tma_prefetch_desc(&tin);
-    const uint32_t bytes = (uint32_t)(geo.bx * geo.by * sizeof(T));
-    int slot = 0, round = 0, issued = 0;
-    bool ok = true;
-    for (int j = 0; j < np; j++) {
-      if (round > 0 && !mbar_wait_bounded(&empty[slot], (round - 1) & 1)) {
-        ok = false;
-        break;
-      }
-      mbar_arrive_expect_tx(&full[slot], bytes);
-      tma_load_3d(ring + slot * geo.stage_bytes, &tin, &full[slot], x0 - V + geo.ax0,
-                  y0 - 1 + geo.ay0, zb - 1 + j + geo.az0);
-      issued++;
-      if (++slot == S) {
-        slot = 0;
-        round++;
-      }
-    }
-    if (!ok) {
-      atomicExch(err, 1);
-      // Let the copies already issued land before the CTA can leave.
-      for (int j = 0; j < issued; j++) {
-        long long t0 = clock64();
-        while (!mbar_try_wait(&full[j % S], (j / S) & 1) && clock64() - t0 < 200000000LL) {
-        }
-      }
-    }
-    return;
-  }
-
-  // ---------------- consumer warps ----------------
-  const int tx = tid % geo.tx_threads, ty = tid / geo.tx_threads;
-  const int lane = tid & 31;
-  const int BX = geo.bx;
-  const int xg0 = x0 + tx * V;
-  const int yg0 = y0 + ty * VY;
-  const int rc0 = (ty * VY + 1) * BX + V + tx * V;  // smem offset of (x0, row 0)
-  // Clamped x faces inside this thread's vector (see diff7_row).
-  unsigned xfix = 0;
-  if (!PERIODIC) {
-    if (xg0 == 0) xfix |= 16u;
-#pragma unroll
-    for (int v = 0; v < V; v++)
-      if (xg0 + v == nx - 1) xfix |= 1u << v;
-  }
-  bool yedge = false;
-#pragma unroll
-  for (int r = 0; r < VY; r++) yedge = yedge || yg0 + r == 0 || yg0 + r == ny - 1;
-  yedge = !PERIODIC && yedge;
-  bool row_in[VY];
-#pragma unroll
-  for (int r = 0; r < VY; r++) row_in[r] = yg0 + r >= d.lo[1] && yg0 + r < d.hi[1];
-  const bool xvec = xg0 >= d.lo[0] && xg0 + V <= d.hi[0];
-  const K7<T> kk = make_k7(k);
-
-  // Every lane waits (the wait gives it visibility of the TMA data); the
-  // outcome is made warp-uniform so a timeout never splits a warp.
-  auto wait_plane = [&](int slot, int round) -> bool {
-    bool ok = mbar_wait_bounded(&full[slot], round & 1);
-    return __all_sync(0xffffffffu, ok);
-  };
-  auto release = [&](int slot) {
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[slot]);
-  };
-  auto plane_ptr = [&](int slot) -> const T * {
-    return reinterpret_cast<const T *>(ring + slot * geo.stage_bytes);
-  };
-
-  T *o = (T *)out.origin;
-  T *dst0 = o + (int64_t)xg0 + (int64_t)yg0 * out.sy + (int64_t)zb * out.sz;
-  int s_z = 1 % S;          // slot of the plane of z
-  int s_t = 1 % S, r_t = 0;  // slot / round of the plane of z+1 (advanced before use)
-  if (S == 1) r_t = 1;
-  int z = zb;
-
-  // One z step: b = plane z-1 (registers), c = plane z (registers), t is
-  // loaded from the plane of z+1. Returns false on a timeout.
-  auto step = [&](Vec16<T>(&vb)[VY], Vec16<T>(&vc)[VY], Vec16<T>(&vt)[VY]) -> bool {
-    if (++s_t == S) {
-      s_t = 0;
-      r_t++;
-    }
-    if (!wait_plane(s_t, r_t)) return false;
-    const T *pz = plane_ptr(s_z);
-    const T *pt = plane_ptr(s_t);
-#pragma unroll
-    for (int r = 0; r < VY; r++) vt[r] = lds16(pt + rc0 + r * BX);
-    const Vec16<T> vn = lds16(pz + rc0 - BX);
-    const Vec16<T> vs = lds16(pz + rc0 + VY * BX);
-    T wl[VY], er[VY];
-#pragma unroll
-    for (int r = 0; r < VY; r++) {
-      wl[r] = pz[rc0 + r * BX - 1];
-      er[r] = pz[rc0 + r * BX + V];
-    }
-    release(s_z);  // this warp is done with the plane of z
-    const bool zedge = !PERIODIC && (z == 0 || z == nz - 1);
-    Vec16<T> res[VY];
-    if (!(yedge || zedge)) {
-#pragma unroll
-      for (int r = 0; r < VY; r++)
-        res[r] = diff7_row(kk, vc[r], wl[r], er[r], r == 0 ? vn : vc[r - 1],
-                           r == VY - 1 ? vs : vc[r + 1], vb[r], vt[r], xfix);
-    } else {
-#pragma unroll
-      for (int r = 0; r < VY; r++) {
-        const Vec16<T> &nv = r == 0 ? vn : vc[r - 1];
-        const Vec16<T> &sv = r == VY - 1 ? vs : vc[r + 1];
-        const int y = yg0 + r;
-#pragma unroll
-        for (int v = 0; v < V; v++) {
-          const int x = xg0 + v;
-          T c = vc[r].v[v];
-          T w = v == 0 ? wl[r] : vc[r].v[v - 1];
-          T e = v == V - 1 ? er[r] : vc[r].v[v + 1];
-          T n = nv.v[v], s = sv.v[v], bb = vb[r].v[v], t = vt[r].v[v];
-          if (x == 0) w = c;
-          if (x == nx - 1) e = c;
-          if (y == 0) n = c;
-          if (y == ny - 1) s = c;
-          if (z == 0) bb = c;
-          if (z == nz - 1) t = c;
-          res[r].v[v] = diff7_point(k, c, w, e, n, s, bb, t);
-        }
-      }
-    }
-#pragma unroll
-    for (int r = 0; r < VY; r++) {
-      if (!row_in[r]) continue;
-      T *dst = dst0 + r * out.sy;
-      if (xvec) {
-        stg16(dst, res[r]);
-      } else {
-#pragma unroll
-        for (int v = 0; v < V; v++)
-          if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) dst[v] = res[r].v[v];
-      }
-      if (PERIODIC && images) {
-#pragma unroll
-        for (int v = 0; v < V; v++)
-          if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0])
-            store_periodic_images(o, out.sy, out.sz, out.n, out.halo, xg0 + v, yg0 + r, z,
-                                  res[r].v[v]);
-      }
-    }
-    dst0 += out.sz;
-    s_z = s_t;
-    z++;
-    return true;
-  };
-
-  // Prologue: planes 0 (z-1) and 1 (z).
-  Vec16<T> A[VY], B[VY], C[VY];
-  bool bad = !wait_plane(0, 0);
-  bad = bad || !wait_plane(1 % S, 1 / S);
-  if (!bad) {
-    const T *p0 = plane_ptr(0), *p1 = plane_ptr(1 % S);
-#pragma unroll
-    for (int r = 0; r < VY; r++) {
-      A[r] = lds16(p0 + rc0 + r * BX);
-      B[r] = lds16(p1 + rc0 + r * BX);
-    }
-    release(0);
-    // Three steps per trip rotate the register roles (b, c, t) without moves.
-    int jj = 0;
-    for (; jj + 3 <= nzl; jj += 3) {
-      if (!step(A, B, C) || !step(B, C, A) || !step(C, A, B)) {
-        bad = true;
-        break;
-      }
-    }
-    if (!bad && jj < nzl) {
-      bad = !step(A, B, C);
-      if (!bad && jj + 1 < nzl) bad = !step(B, C, A);
-    }
-  }
-  if (bad && lane == 0) atomicExch(err, 1);
+  diff7_tile<T, PERIODIC, false>(&tin, out, nx, ny, nz, d, k, geo, tile_x, tile_y, zc, images,
+                                 err, smem, nullptr);
 }
 
 // --------------------------------------------------------------------------

@@ -1,0 +1,149 @@
+"""Batched solves (psb_batch_*): many uneven grids in one persistent launch,
+per-step graph launches, and the per-grid loops. Every member's result must
+equal the oracle bit for bit in every mode, alone or in the mix."""
+import numpy as np
+import pytest
+
+import physis_b200 as ps
+from oracle import oracle
+from tests import gpu_util as U
+
+COEF = [0.1, 0.1, 0.1, 0.1, 0.1, 0.1, 0.4]
+
+# (kind, (nx, ny, nz), steps)
+MEMBERS = [
+    ("diff", (64, 64, 64), 6),
+    ("diffp", (32, 32, 32), 7),
+    ("him", (33, 33, 65), 4),
+    ("diff", (33, 17, 40), 3),
+    ("diffp", (48, 20, 9), 10),
+    ("him", (20, 9, 70), 5),
+    ("diff", (100, 7, 5), 1),
+    ("him", (65, 12, 4), 2),
+    ("diffp", (70, 66, 33), 12),
+]
+
+
+def _inputs(kind, dims, seed):
+    nx, ny, nz = dims
+    if kind == "him":
+        return U.himeno_inputs((nz, ny, nx), seed)
+    return np.random.default_rng(seed).random((nz, ny, nx), dtype=np.float32), None
+
+
+def _want(kind, data, steps):
+    f, coef = data
+    if kind == "him":
+        return oracle.himeno(f, coef, 0.8, steps)[0]
+    return oracle.diffusion7(f, steps, np.asarray(COEF, np.float32), periodic=kind == "diffp")
+
+
+class Members:
+    def __init__(self, spec):
+        self.spec = spec
+        self.data = [_inputs(k, d, 100 + i) for i, (k, d, _) in enumerate(spec)]
+        self.grids = []
+        for (kind, dims, _), (f, coef) in zip(spec, self.data):
+            n = 14 if kind == "him" else 2
+            gs = [ps.grid_new(ps.PS_FLOAT, dims) for _ in range(n)]
+            self.grids.append(gs)
+        self.load()
+
+    def load(self):
+        for (kind, dims, _), (f, coef), gs in zip(self.spec, self.data, self.grids):
+            ps.PSGridCopyin(gs[0], f)
+            ps.PSGridCopyin(gs[1], f)
+            if kind == "him":
+                for i in range(12):
+                    ps.PSGridCopyin(gs[2 + i], coef[i])
+
+    def batch(self, stop=None):
+        b = ps.Batch()
+        for i, ((kind, dims, steps), gs) in enumerate(zip(self.spec, self.grids)):
+            k = {"diff": ps.DIFFUSION7, "diffp": ps.DIFFUSION7_PERIODIC, "him": ps.HIMENO19}[kind]
+            params = [0.8] if kind == "him" else COEF
+            tol, every = stop(i) if stop else (0.0, 0)
+            b.add(k, gs, params, steps, tol=tol, check_every=every)
+        return b
+
+    def free(self):
+        for gs in self.grids:
+            for g in gs:
+                ps.PSGridFree(g)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 1, 2, 3])
+def test_batch_members_bit_exact(mode):
+    M = Members(MEMBERS)
+    try:
+        b = M.batch()
+        b.run(mode)
+        st = b.stats()
+        assert st["lattice_updates"] > 0 and st["launches"] >= 1
+        if mode == 0:
+            assert st["launches"] == 1
+        for i, (kind, dims, steps) in enumerate(MEMBERS):
+            done, _, g = b.result(i)
+            assert done == steps
+            got = ps.PSGridCopyout(g)
+            assert U.bits_equal(got, _want(kind, M.data[i], steps)), (mode, i, kind, dims)
+        b.free()
+    finally:
+        M.free()
+
+
+@pytest.mark.gpu
+def test_batch_rerun_is_repeatable():
+    """Running the same batch twice from the same inputs gives the same bits."""
+    M = Members(MEMBERS[:5])
+    try:
+        b = M.batch()
+        b.run(0)
+        first = [ps.PSGridCopyout(b.result(i)[2]) for i in range(5)]
+        M.load()
+        b.run(0)
+        second = [ps.PSGridCopyout(b.result(i)[2]) for i in range(5)]
+        assert all(U.bits_equal(a, c) for a, c in zip(first, second))
+        b.free()
+    finally:
+        M.free()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_convergence_same_alone_and_in_mix(mode):
+    """Members stop at their residual tolerance; the stop step and the field
+    are the same whether a member runs alone or in the mix."""
+    spec = [("diff", (40, 40, 40), 200), ("him", (33, 33, 33), 120), ("diffp", (24, 24, 24), 150),
+            ("diff", (64, 30, 20), 90)]
+    stop = lambda i: ((2e-3, 5), (0.4, 4), (3e-3, 3), (1e-2, 2))[i]
+    M = Members(spec)
+    try:
+        b = M.batch(stop)
+        b.run(mode)
+        mixed = []
+        for i in range(len(spec)):
+            done, res, g = b.result(i)
+            mixed.append((done, res, ps.PSGridCopyout(g)))
+        b.free()
+        for i, (kind, dims, steps) in enumerate(spec):
+            done = mixed[i][0]
+            assert 0 < done <= steps
+            # the field after `done` steps is the oracle's field after `done` steps
+            assert U.bits_equal(mixed[i][2], _want(kind, M.data[i], done)), (i, done)
+        # each member alone
+        for i in range(len(spec)):
+            M.load()
+            alone = Members.__new__(Members)
+            alone.spec = [spec[i]]
+            alone.data = [M.data[i]]
+            alone.grids = [M.grids[i]]
+            b1 = alone.batch(lambda _j: stop(i))
+            b1.run(mode)
+            done, res, g = b1.result(0)
+            assert done == mixed[i][0] and res == mixed[i][1]
+            assert U.bits_equal(ps.PSGridCopyout(g), mixed[i][2])
+            b1.free()
+    finally:
+        M.free()
