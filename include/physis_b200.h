@@ -402,6 +402,13 @@ psb_status psb_grid_copyout_async(__PSGrid *g, void *dst);
 psb_status psb_sync(void);
 psb_status psb_host_alloc(size_t bytes, void **ptr);
 psb_status psb_host_free(void *ptr);
+/* Fill a grid's interior on the device with a seeded synthetic field (no
+ * counterpart in the reference; used by benchmarks and tests). Element i =
+ * x + nx*(y + ny*z) gets h = splitmix64(seed*0x9E3779B97F4A7C15 + i) and
+ * kind 0: lo + (hi-lo) * (h >> 40) * 2^-24; kind 1: lo; kind 2: 1 inside and
+ * 0 on the faces; kind 3: (z/(nz-1))^2 -- computed in double, rounded once.
+ * Asynchronous on the runtime stream. */
+psb_status psb_grid_fill(__PSGrid *g, int kind, uint64_t seed, double lo, double hi);
 /* Copy one grid's interior into another grid of the same shape and type. */
 psb_status psb_grid_copy(__PSGrid *dst, const __PSGrid *src);
 

@@ -152,6 +152,7 @@ def _load():
         "psb_host_alloc": (S, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
         "psb_host_free": (S, [ctypes.c_void_p]),
         "psb_grid_copy": (S, [G, G]),
+        "psb_grid_fill": (S, [G, ctypes.c_int, ctypes.c_uint64, ctypes.c_double, ctypes.c_double]),
         "psb_generic_register": (S, [ctypes.POINTER(GenericStencilStruct), ctypes.POINTER(ctypes.c_int)]),
         "psb_stencil_map": (S, [ctypes.c_int, ctypes.POINTER(PSDomain), ctypes.POINTER(G), ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
@@ -307,6 +308,39 @@ def PSGridFree(g):
     if g.ptr:
         lib.PSGridFree(g.ptr)
         g.ptr = ctypes.c_void_p()
+
+
+FILL_UNIFORM, FILL_CONST, FILL_BND, FILL_ZPROFILE = 0, 1, 2, 3
+
+
+def grid_fill(g, kind, seed=0, lo=0.0, hi=1.0):
+    """Seeded synthetic field generated on the device (psb_grid_fill)."""
+    check(lib.psb_grid_fill(g.ptr, kind, seed, lo, hi), "psb_grid_fill")
+
+
+def fill_reference(dims, kind, seed=0, lo=0.0, hi=1.0, dtype=np.float32):
+    """Host restatement of psb_grid_fill (for checks): array of shape (nz, ny, nx)."""
+    nx, ny, nz = dims
+    i = np.arange(nx * ny * nz, dtype=np.uint64)
+    if kind == FILL_UNIFORM:
+        with np.errstate(over="ignore"):
+            x = np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15) + i + np.uint64(0x9E3779B97F4A7C15)
+            x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+            x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+            x = x ^ (x >> np.uint64(31))
+        v = lo + (hi - lo) * ((x >> np.uint64(40)).astype(np.float64) * (1.0 / 16777216.0))
+    elif kind == FILL_CONST:
+        v = np.full(i.shape, lo, dtype=np.float64)
+    elif kind == FILL_BND:
+        z, r = np.divmod(i.astype(np.int64), nx * ny)
+        y, x = np.divmod(r, nx)
+        face = (x == 0) | (y == 0) | (z == 0) | (x == nx - 1) | (y == ny - 1) | (z == nz - 1)
+        v = np.where(face, 0.0, 1.0)
+    else:
+        z = i.astype(np.int64) // (nx * ny)
+        t = z / (nz - 1) if nz > 1 else np.zeros_like(z, dtype=np.float64)
+        v = t * t
+    return v.astype(dtype).reshape(nz, ny, nx)
 
 
 def PSGridDim(g, d):

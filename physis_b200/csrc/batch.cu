@@ -131,7 +131,9 @@ __device__ void cta_sum2(double a, double b, double *scr, double *oa, double *ob
 
 // One item: tile t of local step s of member m. All threads of the CTA call
 // it. Returns false if a bounded wait gave up.
-__device__ bool batch_item(const BMember &M, int s, int t, unsigned char *smem, int *err) {
+template <int GROUP>
+__device__ __forceinline__ bool batch_item(const BMember &M, int s, int t, unsigned char *smem,
+                                           int *err) {
   const int par = (M.step0 + s) & 1;
   const int gstep = M.step0 + s;
   const bool check = M.check_every > 0 &&
@@ -153,7 +155,7 @@ __device__ bool batch_item(const BMember &M, int s, int t, unsigned char *smem, 
   if (!skip) {
     if (threadIdx.x == kBTx * kBTy)  // producer: order generic acquire before TMA reads
       asm volatile("fence.proxy.async.global;" ::: "memory");
-    if (M.kind == BK_HIMENO) {
+    if constexpr (GROUP == 1) {
       double g = 0;
       himeno_tile(M.tmap[par], (float *)M.buf[par ^ 1].origin, M.cf, M.sy, M.sz, M.dom, M.omega,
                   M.hg, tile_x, tile_y, zc, err, smem, &g, &bad);
@@ -246,8 +248,14 @@ __device__ __forceinline__ void inval_barriers(unsigned char *smem) {
   }
 }
 
-// Mode 0: one persistent launch over the whole work list.
-__global__ void __launch_bounds__(kBThreads, 3) k_batch_persistent(BatchDev B) {
+// Mode 0: one persistent launch per stencil kind over that kind's work list
+// (a kernel per kind keeps each at the register budget of its single-grid
+// kernel; the two lists are independent).
+// Diffusion items (four instantiations of the tile: clamped/periodic, with or
+// without residual terms) get the register budget of 3 CTAs per SM, Himeno
+// items that of 4.
+template <int GROUP>
+__global__ void __launch_bounds__(kBThreads, GROUP == 0 ? 3 : 4) k_batch_persistent(BatchDev B) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char *smem = aligned_smem(smem_raw);
   __shared__ long long item_s;
@@ -285,8 +293,7 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_persistent(BatchDev B) {
     }
     __syncthreads();
     if (item_s >= B.total_items || stop_s) break;
-    const BMember &M = B.members[m_s];
-    if (!batch_item(M, s_s, t_s, smem, B.err)) {
+    if (!batch_item<GROUP>(B.members[m_s], s_s, t_s, smem, B.err)) {
       __syncthreads();
       break;
     }
@@ -296,82 +303,86 @@ __global__ void __launch_bounds__(kBThreads, 3) k_batch_persistent(BatchDev B) {
   }
 }
 
-// Mode 1: one launch per step; blockIdx.x enumerates the tiles of the
-// members still running at step s.
-__global__ void __launch_bounds__(kBThreads, 3) k_batch_step(BatchDev B, int s) {
+// Mode 1: one launch per step and kind; blockIdx.x enumerates the tiles of
+// that kind's members still running at step s.
+template <int GROUP>
+__global__ void __launch_bounds__(kBThreads, GROUP == 0 ? 3 : 4) k_batch_step(BatchDev B, int s) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char *smem = aligned_smem(smem_raw);
   const int64_t local = blockIdx.x;
   const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
   const int m = B.order[k];
   const int t = (int)(local - B.tile_prefix[k]);
-  batch_item(B.members[m], s, t, smem, B.err);
+  batch_item<GROUP>(B.members[m], s, t, smem, B.err);
 }
 
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
 
-static size_t batch_smem_bytes(TmaGeom dg, HimenoGeom hg) {
-  size_t d = 512 + (size_t)dg.stages * dg.stage_bytes;
-  size_t h = 768 + (size_t)hg.stages * hg.stage_bytes;
-  return 128 + std::max(d, h);
-}
-
 }  // namespace psb
 
 using namespace psb;
 
-struct psb_batch {
-  std::vector<BatchMemberHost> hm;
-  // device state
-  BMember *d_members = nullptr;
+// Work list of one kernel kind (group 0: diffusion members, 1: Himeno).
+struct BatchGroup {
+  std::vector<int> order;               // member ids of this group, by steps (descending)
+  std::vector<int64_t> tile_prefix, step_offset;
+  int max_steps = 0;
+  int64_t total_items = 0;
   int *d_order = nullptr;
   int64_t *d_tile_prefix = nullptr;
   int64_t *d_step_offset = nullptr;
   unsigned long long *d_cursor = nullptr;
+  int blocks_persistent = 0;
+};
+
+struct psb_batch {
+  std::vector<BatchMemberHost> hm;
+  BMember *d_members = nullptr;
   CUtensorMap *d_tmaps = nullptr;
   double *d_partials = nullptr;
   unsigned *d_done = nullptr;
   int *d_stop = nullptr;
   double *d_res = nullptr;
   std::vector<BMember> members;
-  std::vector<int> order;
-  std::vector<int64_t> tile_prefix, step_offset;
-  int max_steps = 0;
-  int64_t total_items = 0;
+  BatchGroup grp[2];
   bool built = false;
   cudaGraphExec_t graph = nullptr;
+  cudaStream_t side = nullptr;       // second stream of the per-step graph
+  cudaEvent_t fork = nullptr, join = nullptr;
   double last_ms = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // batch timing (apart from PSStencilRun's)
   int64_t last_launches = 0;
   int64_t last_lups = 0;
-  int blocks_persistent = 0;
 };
 
 namespace psb {
+
+static int member_group(int kind) { return kind == BK_HIMENO ? 1 : 0; }
 
 static void batch_release_device(psb_batch *b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   b->graph = nullptr;
   cudaFree(b->d_members);
-  cudaFree(b->d_order);
-  cudaFree(b->d_tile_prefix);
-  cudaFree(b->d_step_offset);
-  cudaFree(b->d_cursor);
   cudaFree(b->d_tmaps);
   cudaFree(b->d_partials);
   cudaFree(b->d_done);
   cudaFree(b->d_stop);
   cudaFree(b->d_res);
   b->d_members = nullptr;
-  b->d_order = nullptr;
-  b->d_tile_prefix = b->d_step_offset = nullptr;
-  b->d_cursor = nullptr;
   b->d_tmaps = nullptr;
   b->d_partials = nullptr;
   b->d_done = nullptr;
   b->d_stop = nullptr;
   b->d_res = nullptr;
+  for (auto &g : b->grp) {
+    cudaFree(g.d_order);
+    cudaFree(g.d_tile_prefix);
+    cudaFree(g.d_step_offset);
+    cudaFree(g.d_cursor);
+    g = BatchGroup();
+  }
   b->built = false;
 }
 
@@ -415,14 +426,20 @@ static HimenoGeom batch_hgeom(const GridImpl *g) {
   return geo;
 }
 
-// Build the device work list and member descriptors for one launch in which
+static size_t batch_smem(int group) {
+  const int dstage = ((kBTx * 4 + 8) * (kBTy * kVY + 2) * 4 + 127) / 128 * 128;
+  const int hstage = ((kBTx * 4 + 8) * (kBTy + 2) * 4 + 127) / 128 * 128;
+  return group == 0 ? 128 + 512 + (size_t)kBStages * dstage : 128 + 768 + (size_t)kBStages * hstage;
+}
+
+// Build the device work lists and member descriptors for one launch in which
 // member i runs steps[i] steps starting at its global step step0[i].
 psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std::vector<int> &step0) {
   Runtime &r = rt();
   const int n = (int)b->hm.size();
   batch_release_device(b);
   b->members.assign(n, BMember());
-  std::vector<CUtensorMap> tmaps(2 * n);
+  std::vector<CUtensorMap> tmaps(2 * std::max(1, n));
   int64_t partial_slots = 0;
   for (int i = 0; i < n; i++) {
     const BatchMemberHost &h = b->hm[i];
@@ -439,6 +456,7 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     M.buf[1] = g1->view();
     M.sy = g0->sy;
     M.sz = g0->sz;
+    const CUtensorMap *a = nullptr, *c = nullptr;
     if (h.kind == BK_HIMENO) {
       M.hg = batch_hgeom(g0);
       for (int k = 0; k < 3; k++) {
@@ -450,11 +468,8 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
       M.nzc = (g0->pub.dim[2] - 2 + M.hg.zchunk - 1) / M.hg.zchunk;
       M.omega = (float)h.params[0];
       for (int k = 0; k < 12; k++) M.cf.f[k] = (const float *)h.grids[2 + k]->view().origin;
-      const CUtensorMap *a = nullptr, *c = nullptr;
       PSB_CHECK(get_tmap(g0, M.hg.bx, M.hg.by, &a));
       PSB_CHECK(get_tmap(g1, M.hg.bx, M.hg.by, &c));
-      tmaps[2 * i] = *a;
-      tmaps[2 * i + 1] = *c;
     } else {
       M.dg = batch_dgeom(g0);
       for (int k = 0; k < 3; k++) {
@@ -471,35 +486,17 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
       M.k7.ct = (float)h.params[4];
       M.k7.cb = (float)h.params[5];
       M.k7.cc = (float)h.params[6];
-      const CUtensorMap *a = nullptr, *c = nullptr;
       PSB_CHECK(get_tmap(g0, M.dg.bx, M.dg.by, &a));
       PSB_CHECK(get_tmap(g1, M.dg.bx, M.dg.by, &c));
-      tmaps[2 * i] = *a;
-      tmaps[2 * i + 1] = *c;
     }
+    tmaps[2 * i] = *a;
+    tmaps[2 * i + 1] = *c;
     M.ntiles = M.tiles_x * M.tiles_y * M.nzc;
     partial_slots += 4 * (int64_t)M.ntiles;
   }
-  // Order members by steps (descending): the members still running at step
-  // s are then a prefix of the order.
-  b->order.resize(n);
-  std::iota(b->order.begin(), b->order.end(), 0);
-  std::stable_sort(b->order.begin(), b->order.end(),
-                   [&](int x, int y) { return steps[x] > steps[y]; });
-  b->tile_prefix.assign(n + 1, 0);
-  for (int i = 0; i < n; i++)
-    b->tile_prefix[i + 1] = b->tile_prefix[i] + b->members[b->order[i]].ntiles;
-  b->max_steps = n ? steps[b->order[0]] : 0;
-  b->step_offset.assign(b->max_steps + 1, 0);
-  int active = n;
-  for (int s = 0; s < b->max_steps; s++) {
-    while (active > 0 && steps[b->order[active - 1]] <= s) active--;
-    b->step_offset[s + 1] = b->step_offset[s] + b->tile_prefix[active];
-  }
-  b->total_items = b->max_steps ? b->step_offset[b->max_steps] : 0;
-  // Device arrays.
-  PSB_TRY(cudaMalloc(&b->d_tmaps, sizeof(CUtensorMap) * std::max(1, 2 * n)));
-  PSB_TRY(cudaMemcpy(b->d_tmaps, tmaps.data(), sizeof(CUtensorMap) * 2 * n, cudaMemcpyHostToDevice));
+  PSB_TRY(cudaMalloc(&b->d_tmaps, sizeof(CUtensorMap) * tmaps.size()));
+  PSB_TRY(cudaMemcpy(b->d_tmaps, tmaps.data(), sizeof(CUtensorMap) * tmaps.size(),
+                     cudaMemcpyHostToDevice));
   PSB_TRY(cudaMalloc(&b->d_partials, sizeof(double) * std::max<int64_t>(1, partial_slots)));
   PSB_TRY(cudaMalloc(&b->d_done, sizeof(unsigned) * std::max(1, n)));
   PSB_TRY(cudaMalloc(&b->d_stop, sizeof(int) * std::max(1, n)));
@@ -518,31 +515,55 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
   }
   PSB_TRY(cudaMalloc(&b->d_members, sizeof(BMember) * std::max(1, n)));
   PSB_TRY(cudaMemcpy(b->d_members, b->members.data(), sizeof(BMember) * n, cudaMemcpyHostToDevice));
-  PSB_TRY(cudaMalloc(&b->d_order, sizeof(int) * std::max(1, n)));
-  PSB_TRY(cudaMemcpy(b->d_order, b->order.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-  PSB_TRY(cudaMalloc(&b->d_tile_prefix, sizeof(int64_t) * (n + 1)));
-  PSB_TRY(cudaMemcpy(b->d_tile_prefix, b->tile_prefix.data(), sizeof(int64_t) * (n + 1),
-                     cudaMemcpyHostToDevice));
-  PSB_TRY(cudaMalloc(&b->d_step_offset, sizeof(int64_t) * (b->max_steps + 1)));
-  PSB_TRY(cudaMemcpy(b->d_step_offset, b->step_offset.data(), sizeof(int64_t) * (b->max_steps + 1),
-                     cudaMemcpyHostToDevice));
-  PSB_TRY(cudaMalloc(&b->d_cursor, sizeof(unsigned long long)));
-  // Kernel attributes and the persistent grid size.
-  TmaGeom dg;
-  HimenoGeom hg;
-  memset(&dg, 0, sizeof(dg));
-  memset(&hg, 0, sizeof(hg));
-  dg.stages = hg.stages = kBStages;
-  dg.stage_bytes = ((kBTx * 4 + 8) * (kBTy * kVY + 2) * 4 + 127) / 128 * 128;
-  hg.stage_bytes = ((kBTx * 4 + 8) * (kBTy + 2) * 4 + 127) / 128 * 128;
-  const size_t smem = batch_smem_bytes(dg, hg);
-  PSB_TRY(cudaFuncSetAttribute(k_batch_persistent, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               cudaSharedmemCarveoutMaxShared));
-  PSB_TRY(cudaFuncSetAttribute(k_batch_step, cudaFuncAttributePreferredSharedMemoryCarveout,
-                               cudaSharedmemCarveoutMaxShared));
-  int per_sm = 0;
-  PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent, kBThreads, smem));
-  b->blocks_persistent = std::max(1, per_sm) * r.sm_count;
+  // One work list per kernel kind. Members are ordered by steps
+  // (descending), so the members still running at step s are a prefix.
+  for (int gi = 0; gi < 2; gi++) {
+    BatchGroup &G = b->grp[gi];
+    for (int i = 0; i < n; i++)
+      if (member_group(b->hm[i].kind) == gi) G.order.push_back(i);
+    std::stable_sort(G.order.begin(), G.order.end(),
+                     [&](int x, int y) { return steps[x] > steps[y]; });
+    const int gn = (int)G.order.size();
+    G.tile_prefix.assign(gn + 1, 0);
+    for (int i = 0; i < gn; i++)
+      G.tile_prefix[i + 1] = G.tile_prefix[i] + b->members[G.order[i]].ntiles;
+    G.max_steps = gn ? steps[G.order[0]] : 0;
+    G.step_offset.assign(G.max_steps + 1, 0);
+    int active = gn;
+    for (int st = 0; st < G.max_steps; st++) {
+      while (active > 0 && steps[G.order[active - 1]] <= st) active--;
+      G.step_offset[st + 1] = G.step_offset[st] + G.tile_prefix[active];
+    }
+    G.total_items = G.max_steps ? G.step_offset[G.max_steps] : 0;
+    PSB_TRY(cudaMalloc(&G.d_order, sizeof(int) * std::max(1, gn)));
+    if (gn) PSB_TRY(cudaMemcpy(G.d_order, G.order.data(), sizeof(int) * gn, cudaMemcpyHostToDevice));
+    PSB_TRY(cudaMalloc(&G.d_tile_prefix, sizeof(int64_t) * (gn + 1)));
+    PSB_TRY(cudaMemcpy(G.d_tile_prefix, G.tile_prefix.data(), sizeof(int64_t) * (gn + 1),
+                       cudaMemcpyHostToDevice));
+    PSB_TRY(cudaMalloc(&G.d_step_offset, sizeof(int64_t) * (G.max_steps + 1)));
+    PSB_TRY(cudaMemcpy(G.d_step_offset, G.step_offset.data(), sizeof(int64_t) * (G.max_steps + 1),
+                       cudaMemcpyHostToDevice));
+    PSB_TRY(cudaMalloc(&G.d_cursor, sizeof(unsigned long long)));
+    int per_sm = 0;
+    if (gi == 0) {
+      PSB_TRY(cudaFuncSetAttribute(k_batch_persistent<0>,
+                                   cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
+      PSB_TRY(cudaFuncSetAttribute(k_batch_step<0>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
+      PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent<0>,
+                                                            kBThreads, batch_smem(0)));
+    } else {
+      PSB_TRY(cudaFuncSetAttribute(k_batch_persistent<1>,
+                                   cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
+      PSB_TRY(cudaFuncSetAttribute(k_batch_step<1>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                   cudaSharedmemCarveoutMaxShared));
+      PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent<1>,
+                                                            kBThreads, batch_smem(1)));
+    }
+    G.blocks_persistent = std::max(1, per_sm) * r.sm_count;
+  }
   b->built = true;
   return PSB_OK;
 }
@@ -551,60 +572,72 @@ psb_status batch_reset_counters(psb_batch *b, cudaStream_t s) {
   const int n = (int)b->hm.size();
   PSB_TRY(cudaMemsetAsync(b->d_done, 0, sizeof(unsigned) * std::max(1, n), s));
   PSB_TRY(cudaMemsetAsync(b->d_stop, 0xff, sizeof(int) * std::max(1, n), s));
-  PSB_TRY(cudaMemsetAsync(b->d_cursor, 0, sizeof(unsigned long long), s));
+  for (auto &g : b->grp) PSB_TRY(cudaMemsetAsync(g.d_cursor, 0, sizeof(unsigned long long), s));
   return PSB_OK;
 }
 
-static BatchDev batch_dev(psb_batch *b) {
+static BatchDev batch_dev(psb_batch *b, int gi) {
+  const BatchGroup &G = b->grp[gi];
   BatchDev B;
-  B.nmembers = (int)b->hm.size();
+  B.nmembers = (int)G.order.size();
   B.members = b->d_members;
-  B.order = b->d_order;
-  B.tile_prefix = b->d_tile_prefix;
-  B.step_offset = b->d_step_offset;
-  B.max_steps = b->max_steps;
-  B.total_items = b->total_items;
-  B.cursor = b->d_cursor;
+  B.order = G.d_order;
+  B.tile_prefix = G.d_tile_prefix;
+  B.step_offset = G.d_step_offset;
+  B.max_steps = G.max_steps;
+  B.total_items = G.total_items;
+  B.cursor = G.d_cursor;
   B.err = rt().d_error;
   return B;
 }
 
-static size_t batch_smem() {
-  TmaGeom dg;
-  HimenoGeom hg;
-  dg.stages = hg.stages = kBStages;
-  dg.stage_bytes = ((kBTx * 4 + 8) * (kBTy * kVY + 2) * 4 + 127) / 128 * 128;
-  hg.stage_bytes = ((kBTx * 4 + 8) * (kBTy + 2) * 4 + 127) / 128 * 128;
-  return batch_smem_bytes(dg, hg);
-}
-
 psb_status batch_launch_persistent(psb_batch *b, cudaStream_t s, int64_t *launches) {
-  if (!b->total_items) return PSB_OK;
   PSB_CHECK(batch_reset_counters(b, s));
-  const int blocks = (int)std::min<int64_t>(b->blocks_persistent, b->total_items);
-  k_batch_persistent<<<blocks, kBThreads, batch_smem(), s>>>(batch_dev(b));
-  (*launches)++;
-  cudaError_t e = cudaGetLastError();
-  if (e != cudaSuccess) return cuda_status(e, "k_batch_persistent");
+  for (int gi = 0; gi < 2; gi++) {
+    const BatchGroup &G = b->grp[gi];
+    if (!G.total_items) continue;
+    const int blocks = (int)std::min<int64_t>(G.blocks_persistent, G.total_items);
+    if (gi == 0)
+      k_batch_persistent<0><<<blocks, kBThreads, batch_smem(0), s>>>(batch_dev(b, 0));
+    else
+      k_batch_persistent<1><<<blocks, kBThreads, batch_smem(1), s>>>(batch_dev(b, 1));
+    (*launches)++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_status(e, "k_batch_persistent");
+  }
   return PSB_OK;
 }
 
-// Per-step launches (mode 1): recorded once into a graph (counters reset
-// inside it) and replayed.
+// Per-step launches (mode 1): both kinds' step sequences, on two streams
+// forked and joined inside one CUDA graph, recorded once and replayed.
 psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches) {
-  if (!b->total_items) return PSB_OK;
-  const int n = (int)b->hm.size();
   if (!b->graph) {
+    if (!b->side) {
+      PSB_TRY(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+      PSB_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+      PSB_TRY(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming));
+    }
     cudaGraph_t g;
     PSB_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     psb_status st = batch_reset_counters(b, s);
-    int active = n;
-    const BatchDev B = batch_dev(b);
-    for (int step = 0; step < b->max_steps && st == PSB_OK; step++) {
-      while (active > 0 && b->members[b->order[active - 1]].steps <= step) active--;
-      const int64_t blocks = b->tile_prefix[active];
-      k_batch_step<<<(unsigned)blocks, kBThreads, batch_smem(), s>>>(B, step);
+    cudaEventRecord(b->fork, s);
+    cudaStreamWaitEvent(b->side, b->fork, 0);
+    for (int gi = 0; gi < 2 && st == PSB_OK; gi++) {
+      const BatchGroup &G = b->grp[gi];
+      cudaStream_t ss = gi == 0 ? s : b->side;
+      const BatchDev B = batch_dev(b, gi);
+      int active = (int)G.order.size();
+      for (int step = 0; step < G.max_steps; step++) {
+        while (active > 0 && b->members[G.order[active - 1]].steps <= step) active--;
+        const unsigned blocks = (unsigned)G.tile_prefix[active];
+        if (gi == 0)
+          k_batch_step<0><<<blocks, kBThreads, batch_smem(0), ss>>>(B, step);
+        else
+          k_batch_step<1><<<blocks, kBThreads, batch_smem(1), ss>>>(B, step);
+      }
     }
+    cudaEventRecord(b->join, b->side);
+    cudaStreamWaitEvent(s, b->join, 0);
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (st != PSB_OK || e != cudaSuccess) {
       if (e == cudaSuccess) cudaGraphDestroy(g);
@@ -616,7 +649,7 @@ psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches) {
     if (e != cudaSuccess) return cuda_status(e, "batch graph instantiate");
   }
   PSB_TRY(cudaGraphLaunch(b->graph, s));
-  *launches += b->max_steps;
+  *launches += b->grp[0].max_steps + b->grp[1].max_steps;
   return PSB_OK;
 }
 
@@ -684,6 +717,8 @@ psb_status psb_batch_create(psb_batch **b) {
   if (!b) return set_status(PSB_ERR_INVALID);
   PSB_CHECK(ensure_init());
   *b = new psb_batch();
+  PSB_TRY(cudaEventCreate(&(*b)->ev0));
+  PSB_TRY(cudaEventCreate(&(*b)->ev1));
   return PSB_OK;
 }
 
@@ -745,7 +780,7 @@ psb_status psb_batch_run(psb_batch *b, int mode) {
       PSB_CHECK(batch_prepare(b, steps, step0));
     }
   }
-  PSB_TRY(cudaEventRecord(r.ev_start, r.stream));
+  PSB_TRY(cudaEventRecord(b->ev0, r.stream));
   psb_status st;
   switch (mode) {
     case 0: st = batch_launch_persistent(b, r.stream, &launches); break;
@@ -755,11 +790,11 @@ psb_status psb_batch_run(psb_batch *b, int mode) {
     default: return set_status(PSB_ERR_INVALID);
   }
   if (st != PSB_OK) return set_status(st);
-  PSB_TRY(cudaEventRecord(r.ev_stop, r.stream));
+  PSB_TRY(cudaEventRecord(b->ev1, r.stream));
   legacy_join_out();
-  PSB_TRY(cudaEventSynchronize(r.ev_stop));
+  PSB_TRY(cudaEventSynchronize(b->ev1));
   float ms = 0;
-  PSB_TRY(cudaEventElapsedTime(&ms, r.ev_start, r.ev_stop));
+  PSB_TRY(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
   b->last_ms = ms;
   b->last_launches = launches;
   int64_t lups = 0;
@@ -825,6 +860,11 @@ psb_status psb_batch_free(psb_batch *b) {
   if (!b) return set_status(PSB_ERR_INVALID);
   cudaStreamSynchronize(rt().stream);
   batch_release_device(b);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->side) cudaStreamDestroy(b->side);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->join) cudaEventDestroy(b->join);
   delete b;
   return PSB_OK;
 }

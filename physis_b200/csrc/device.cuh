@@ -158,36 +158,21 @@ __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
 
-// ---------------------------------------------------------------------------
-// Periodic halo images. A pitched grid keeps `halo` ghost cells around the
-// interior; for periodic reads, ghost cell q must hold the value of the
-// interior cell ((q + n) % n) per axis. A kernel that writes interior point
-// p therefore also writes every ghost cell whose wrapped position is p.
-// ---------------------------------------------------------------------------
-
-__device__ __forceinline__ int wrap_images(int x, int n, int h, int *out) {
-  int k = 0;
-  out[k++] = x;
-  if (x >= n - h && x - n >= -h) out[k++] = x - n;
-  if (x < h && x + n < n + h) out[k++] = x + n;
-  return k;
-}
-
+// Face images for the 7-point stencil: it only reads the six face
+// neighbours, so the halo cells it needs are the depth-1 faces (x = -1 and
+// x = n at interior y, z, and likewise for y and z). A writer of interior
+// point (x, y, z) keeps them periodic by storing its value at the face image
+// of each axis where it lies on the opposite face.
 template <typename T>
-__device__ __forceinline__ void store_periodic_images(T *origin, int64_t sy, int64_t sz,
-                                                      const int *n, int h, int x, int y, int z,
-                                                      T v) {
-  if (x >= h && x < n[0] - h && y >= h && y < n[1] - h && z >= h && z < n[2] - h) return;
-  int ix[3], iy[3], iz[3];
-  int kx = wrap_images(x, n[0], h, ix);
-  int ky = wrap_images(y, n[1], h, iy);
-  int kz = wrap_images(z, n[2], h, iz);
-  for (int c = 0; c < kz; c++)
-    for (int b = 0; b < ky; b++)
-      for (int a = 0; a < kx; a++) {
-        if (a == 0 && b == 0 && c == 0) continue;
-        origin[(int64_t)ix[a] + iy[b] * sy + iz[c] * sz] = v;
-      }
+__device__ __forceinline__ void store_face_images(T *origin, int64_t sy, int64_t sz, const int *n,
+                                                  int x, int y, int z, T v) {
+  const int64_t c = (int64_t)x + y * sy + z * sz;
+  if (x == 0) origin[c + n[0]] = v;
+  if (x == n[0] - 1) origin[c - n[0]] = v;
+  if (y == 0) origin[c + n[1] * sy] = v;
+  if (y == n[1] - 1) origin[c - n[1] * sy] = v;
+  if (z == 0) origin[c + n[2] * sz] = v;
+  if (z == n[2] - 1) origin[c - n[2] * sz] = v;
 }
 
 }  // namespace psb

@@ -59,8 +59,7 @@ __global__ void __launch_bounds__(256) k_diff7_plain(GridView in, GridView out, 
     }
     T v = diff7_point(k, c, w, e, n, s, b, t);
     o[x + y * out.sy + z * out.sz] = v;
-    if (PERIODIC && images)
-      store_periodic_images(o, out.sy, out.sz, out.n, out.halo, x, y, z, v);
+    if (PERIODIC && images) store_face_images(o, out.sy, out.sz, out.n, x, y, z, v);
   }
 }
 

@@ -157,11 +157,14 @@ struct TileAcc {
 // memory (barriers + ring). With ACC the consumer threads add their points'
 // convergence terms to *acc.
 template <typename T, bool PERIODIC, bool ACC>
-__device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridView &out, int nx,
-                                           int ny, int nz, const Dom3 &d, const C7<T> &k,
-                                           const TmaGeom &geo, int tile_x, int tile_y, int zc,
+__device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridView out, int nx,
+                                           int ny, int nz, const Dom3 d, const C7<T> k,
+                                           const TmaGeom geo, int tile_x, int tile_y, int zc,
                                            int images, int *err, unsigned char *smem,
                                            TileAcc *acc) {
+  // The descriptors arrive by value so that they live in registers: callers
+  // may pass fields of a table in global memory, and references into it
+  // would be reloaded after every store of the hot loop.
   constexpr int V = 16 / sizeof(T);
   constexpr int VY = kVY;
   uint64_t *full = reinterpret_cast<uint64_t *>(smem);
@@ -344,11 +347,16 @@ __device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridVie
           if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) dst[v] = res[r].v[v];
       }
       if (PERIODIC && images) {
+        // Only threads on a face have images to write: x faces touch the
+        // first or last element of a vector, y/z faces whole rows/planes.
+        const int y = yg0 + r;
+        const bool yz = y == 0 || y == out.n[1] - 1 || z == 0 || z == out.n[2] - 1;
+        if (yz || xg0 == 0 || xg0 + V - 1 >= out.n[0] - 1) {
 #pragma unroll
-        for (int v = 0; v < V; v++)
-          if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0])
-            store_periodic_images(o, out.sy, out.sz, out.n, out.halo, xg0 + v, yg0 + r, z,
-                                  res[r].v[v]);
+          for (int v = 0; v < V; v++)
+            if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0])
+              store_face_images(o, out.sy, out.sz, out.n, xg0 + v, y, z, res[r].v[v]);
+        }
       }
     }
     dst0 += out.sz;

@@ -59,8 +59,8 @@ __device__ __forceinline__ void consumer_bar(int nct) {
 // following consumer barrier (the consumer threads), false in the producer
 // warp. A timeout sets *bad_out.
 __device__ __forceinline__ bool himeno_tile(const CUtensorMap *tin, float *pout,
-                                            const HimenoCoef &cf, int64_t sy, int64_t sz,
-                                            const Dom3 &d, float omega, const HimenoGeom &geo,
+                                            const HimenoCoef cf, int64_t sy, int64_t sz,
+                                            const Dom3 d, float omega, const HimenoGeom geo,
                                             int tile_x, int tile_y, int zc, int *err,
                                             unsigned char *smem, double *acc_out,
                                             bool *bad_out) {

@@ -13,6 +13,7 @@
 #include <sys/time.h>
 #include <time.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 
@@ -352,7 +353,13 @@ psb_status get_tmap(GridImpl *g, int bx, int by, const CUtensorMap **out) {
   CUtensorMap m;
   int E = g->pub.elm_size;
   CUtensorMapDataType dt = E == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
-  cuuint64_t dims[3] = {(cuuint64_t)g->pitch, (cuuint64_t)g->rows, (cuuint64_t)g->planes};
+  // The x extent ends at the right halo, not at the padded pitch: box columns
+  // past it are out of bounds, so TMA fills them instead of reading padding
+  // from DRAM (this matters for narrow grids, whose rows are mostly padding).
+  const int64_t xext = g->layout == PSB_LAYOUT_PITCHED
+                           ? std::min<int64_t>(g->pitch, (int64_t)g->pad_left + g->pub.dim[0] + g->halo)
+                           : g->pitch;
+  cuuint64_t dims[3] = {(cuuint64_t)xext, (cuuint64_t)g->rows, (cuuint64_t)g->planes};
   cuuint64_t strides[2] = {(cuuint64_t)(g->sy * E), (cuuint64_t)(g->sz * E)};
   cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
   cuuint32_t estr[3] = {1, 1, 1};

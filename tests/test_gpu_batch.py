@@ -82,7 +82,7 @@ def test_batch_members_bit_exact(mode):
         st = b.stats()
         assert st["lattice_updates"] > 0 and st["launches"] >= 1
         if mode == 0:
-            assert st["launches"] == 1
+            assert st["launches"] <= 2  # one persistent launch per stencil kind
         for i, (kind, dims, steps) in enumerate(MEMBERS):
             done, _, g = b.result(i)
             assert done == steps
@@ -147,3 +147,18 @@ def test_batch_convergence_same_alone_and_in_mix(mode):
             b1.free()
     finally:
         M.free()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kind", [ps.FILL_UNIFORM, ps.FILL_CONST, ps.FILL_BND, ps.FILL_ZPROFILE])
+def test_grid_fill_matches_host_restatement(kind):
+    dims = (37, 20, 11)
+    for layout in (ps.LAYOUT_PITCHED, ps.LAYOUT_DENSE):
+        g = ps.grid_new(ps.PS_FLOAT, dims, layout)
+        try:
+            ps.grid_fill(g, kind, 77, -0.5, 2.0)
+            got = ps.PSGridCopyout(g)
+            want = ps.fill_reference(dims, kind, 77, -0.5, 2.0)
+            assert U.bits_equal(got, want)
+        finally:
+            ps.PSGridFree(g)
