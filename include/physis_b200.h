@@ -528,38 +528,66 @@ psb_status psb_batch_free(psb_batch *b);
 /* Group 2d: serving -- continuous batching of solve requests                */
 /* ------------------------------------------------------------------------ */
 
+/* A server owns a worker thread that admits queued requests in arrival
+ * order while the device-memory budget and the slot limit allow, keeps each
+ * admitted request's grids resident on the device until it finishes, and
+ * advances all admitted requests together in rounds of the persistent
+ * batched kernel (group 2c); requests that arrive while a round runs join at
+ * the next round boundary. A request finishes when its relative residual
+ * (as for psb_batch_set_stop) is <= tol at a check, or after max_steps.
+ * Results do not depend on what else is being served: each request's
+ * arithmetic and residual sums are those of serving it alone.
+ * mode PSB_SERVE_BATCHED: the above. PSB_SERVE_FIFO: the baseline -- one
+ * request at a time in arrival order, one plain-kernel launch per step and
+ * a separate residual pass at each check (the reference's loop shape). */
 typedef struct psb_server psb_server;
+enum { PSB_SERVE_BATCHED = 0, PSB_SERVE_FIFO = 1 };
 typedef struct {
   int kernel_id;          /* PSB_KERNEL_DIFFUSION7(_PERIODIC) or PSB_KERNEL_HIMENO19 */
   PSIndex dims[3];
-  int max_steps;          /* stop after this many steps */
+  int max_steps;          /* stop after this many steps (>= 1) */
   double tol;             /* stop when the relative residual is <= tol (0: never) */
-  int check_every;        /* residual check interval in steps */
-  const float *init;      /* host initial field (nx*ny*nz), copied at submit */
-  const float *coef;      /* Himeno: 12 coefficient fields + bnd + wrk1,
-                             14*nx*ny*nz floats in the grid order of
-                             PSB_KERNEL_HIMENO19 minus the two p grids; NULL
-                             for diffusion */
-  double params[PSB_MAX_PARAMS];
+  int check_every;        /* residual check interval in steps (>= 1 when tol > 0) */
+  const float *init;      /* host initial field (nx*ny*nz floats: u, or Himeno p),
+                             or NULL to generate it on the device from seed */
+  const float *coef;      /* Himeno: 12*nx*ny*nz floats, the fields a0 a1 a2 a3
+                             b0 b1 b2 c0 c1 c2 bnd wrk1 one after another, or NULL
+                             to generate them from seed; unused for diffusion */
+  float *out;             /* host buffer for the final field (nx*ny*nz), or NULL */
+  uint64_t seed;          /* seed of the generated fields */
+  double params[PSB_MAX_PARAMS];  /* kernel parameters as for psb_stencil_map */
   int nparams;
 } psb_request;
+/* Fields generated from seed s (psb_grid_fill kinds): diffusion u uniform in
+ * [0,1) with seed s; Himeno p = (z/(nz-1))^2, a0..a2, c0..c2 uniform in
+ * [0.9,1.1), a3 in [0.95/6,1.05/6), b0..b2 in [-0.01,0.01) with seeds
+ * s*16+1 .. s*16+10 in field order, bnd 1 inside and 0 on the faces, wrk1 0. */
 typedef struct {
   int64_t id;
-  psb_status status;
+  psb_status status;      /* PSB_OK, PSB_ERR_CANCELLED or the failure */
   int steps_done;
-  double residual;
-  double submit_s, start_s, finish_s;  /* host monotonic clock, seconds */
+  double residual;        /* last relative residual, -1 if never checked */
+  double submit_s, start_s, finish_s;  /* host steady clock, seconds */
 } psb_result;
+/* max_slots: requests on the device at once (0: no limit). */
 psb_status psb_server_create(size_t mem_budget_bytes, int max_slots, int mode,
                              psb_server **s);
+/* Queue a request. init, coef and out must stay valid until the request
+ * completes (psb_server_wait returned it). A request whose grids alone
+ * exceed the budget is refused with PSB_ERR_NOMEM. */
 psb_status psb_server_submit(psb_server *s, const psb_request *req, int64_t *id);
+/* Cancel a queued or running request; it completes with PSB_ERR_CANCELLED
+ * (a running one at its next round boundary). */
 psb_status psb_server_cancel(psb_server *s, int64_t id);
-/* Wait for request id (id < 0: any), copy its final field to out (may be
- * NULL) and its record to *res. timeout_s < 0 waits forever. */
-psb_status psb_server_wait(psb_server *s, int64_t id, float *out, double timeout_s,
-                           psb_result *res);
+/* Wait for request id (id < 0: the earliest completed one not yet returned)
+ * and return its record; each request is returned once. timeout_s < 0 waits
+ * forever; PSB_ERR_TIMEOUT if it did not complete in time. */
+psb_status psb_server_wait(psb_server *s, int64_t id, double timeout_s, psb_result *res);
+/* Bytes a request needs on the device (its resident grids). */
+psb_status psb_server_request_bytes(const psb_request *req, size_t *bytes);
 psb_status psb_server_stats(psb_server *s, int64_t *completed, int64_t *rounds,
-                            int64_t *launches, size_t *peak_bytes);
+                            int64_t *launches, size_t *peak_bytes, double *device_ms);
+/* Finish every queued and running request, then stop the worker. */
 psb_status psb_server_destroy(psb_server *s);
 
 #ifdef __cplusplus

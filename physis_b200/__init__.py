@@ -99,14 +99,16 @@ class TuneConfig(ctypes.Structure):
 
 
 class Request(ctypes.Structure):
+    """psb_request."""
     _fields_ = [("kernel_id", ctypes.c_int), ("dims", ctypes.c_int32 * 3),
                 ("max_steps", ctypes.c_int), ("tol", ctypes.c_double),
                 ("check_every", ctypes.c_int), ("init", ctypes.c_void_p),
-                ("coef", ctypes.c_void_p), ("params", ctypes.c_double * PSB_MAX_PARAMS),
-                ("nparams", ctypes.c_int)]
+                ("coef", ctypes.c_void_p), ("out", ctypes.c_void_p), ("seed", ctypes.c_uint64),
+                ("params", ctypes.c_double * PSB_MAX_PARAMS), ("nparams", ctypes.c_int)]
 
 
 class Result(ctypes.Structure):
+    """psb_result."""
     _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int), ("steps_done", ctypes.c_int),
                 ("residual", ctypes.c_double), ("submit_s", ctypes.c_double),
                 ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double)]
@@ -189,10 +191,12 @@ def _load():
         "psb_server_create": (S, [ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
         "psb_server_submit": (S, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]),
         "psb_server_cancel": (S, [ctypes.c_void_p, ctypes.c_int64]),
-        "psb_server_wait": (S, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_double,
+        "psb_server_wait": (S, [ctypes.c_void_p, ctypes.c_int64, ctypes.c_double,
                                 ctypes.POINTER(Result)]),
+        "psb_server_request_bytes": (S, [ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_size_t)]),
         "psb_server_stats": (S, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
-                                 ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_size_t)]),
+                                 ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_size_t),
+                                 ctypes.POINTER(ctypes.c_double)]),
         "psb_server_destroy": (S, [ctypes.c_void_p]),
     }
     for name, (res, args) in sigs.items():
@@ -609,3 +613,96 @@ class Batch:
         if self.ptr:
             check(lib.psb_batch_free(self.ptr), "psb_batch_free")
             self.ptr = ctypes.c_void_p()
+
+
+# ---------------------------------------------------------------------------
+# Serving
+# ---------------------------------------------------------------------------
+SERVE_BATCHED = 0
+SERVE_FIFO = 1
+
+
+def _host_ptr(a, n, what):
+    """Address of a C-contiguous float32 array of n elements (None -> NULL)."""
+    if a is None:
+        return None
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous
+            and a.size == n):
+        raise ValueError("%s: need a C-contiguous float32 array of %d elements" % (what, n))
+    return a.ctypes.data
+
+
+class Server:
+    """Continuous-batching solve server (psb_server_*).
+
+    Arrays passed to submit (init, coef, out) must stay alive until wait()
+    has returned that request; the object keeps references to them until
+    then."""
+
+    def __init__(self, budget_bytes, max_slots=0, mode=SERVE_BATCHED):
+        p = ctypes.c_void_p()
+        check(lib.psb_server_create(int(budget_bytes), int(max_slots), int(mode), ctypes.byref(p)),
+              "psb_server_create")
+        self.ptr = p
+        self._keep = {}
+
+    @staticmethod
+    def request(kernel, dims, params, max_steps, tol=0.0, check_every=0, init=None, coef=None,
+                out=None, seed=0):
+        q = Request()
+        q.kernel_id = int(kernel)
+        for k in range(3):
+            q.dims[k] = int(dims[k])
+        q.max_steps = int(max_steps)
+        q.tol = float(tol)
+        q.check_every = int(check_every)
+        n = int(dims[0]) * int(dims[1]) * int(dims[2])
+        q.init = _host_ptr(init, n, "init")
+        q.coef = _host_ptr(coef, 12 * n, "coef")
+        q.out = _host_ptr(out, n, "out")
+        q.seed = int(seed)
+        for i, v in enumerate(params):
+            q.params[i] = float(v)
+        q.nparams = len(params)
+        return q
+
+    @staticmethod
+    def request_bytes(q):
+        b = ctypes.c_size_t()
+        check(lib.psb_server_request_bytes(ctypes.byref(q), ctypes.byref(b)), "psb_server_request_bytes")
+        return b.value
+
+    def submit(self, kernel, dims, params, max_steps, tol=0.0, check_every=0, init=None,
+               coef=None, out=None, seed=0):
+        q = self.request(kernel, dims, params, max_steps, tol, check_every, init, coef, out, seed)
+        i = ctypes.c_int64()
+        check(lib.psb_server_submit(self.ptr, ctypes.byref(q), ctypes.byref(i)), "psb_server_submit")
+        self._keep[i.value] = (init, coef, out)
+        return i.value
+
+    def cancel(self, rid):
+        check(lib.psb_server_cancel(self.ptr, int(rid)), "psb_server_cancel")
+
+    def wait(self, rid=-1, timeout=-1.0):
+        """Record of request rid (-1: the next completed one) as a dict."""
+        r = Result()
+        check(lib.psb_server_wait(self.ptr, int(rid), float(timeout), ctypes.byref(r)),
+              "psb_server_wait")
+        self._keep.pop(r.id, None)
+        return {"id": r.id, "status": r.status, "steps_done": r.steps_done,
+                "residual": r.residual, "submit_s": r.submit_s, "start_s": r.start_s,
+                "finish_s": r.finish_s}
+
+    def stats(self):
+        c, rd, la = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()
+        pk, ms = ctypes.c_size_t(), ctypes.c_double()
+        check(lib.psb_server_stats(self.ptr, ctypes.byref(c), ctypes.byref(rd), ctypes.byref(la),
+                                   ctypes.byref(pk), ctypes.byref(ms)), "psb_server_stats")
+        return {"completed": c.value, "rounds": rd.value, "launches": la.value,
+                "peak_bytes": pk.value, "device_ms": ms.value}
+
+    def destroy(self):
+        if self.ptr:
+            check(lib.psb_server_destroy(self.ptr), "psb_server_destroy")
+            self.ptr = ctypes.c_void_p()
+            self._keep.clear()

@@ -39,8 +39,6 @@
 
 namespace psb {
 
-enum { BK_DIFF7 = 0, BK_DIFF7P = 1, BK_HIMENO = 2 };
-
 // Fixed tile shape of batched items: 64 points wide, 128 consumer threads.
 constexpr int kBTx = 16;       // consumer threads along x (x 4 floats = 64 points)
 constexpr int kBTy = 8;        // consumer thread rows
@@ -334,17 +332,21 @@ struct BatchGroup {
   int64_t *d_tile_prefix = nullptr;
   int64_t *d_step_offset = nullptr;
   unsigned long long *d_cursor = nullptr;
+  size_t cap_order = 0, cap_tile_prefix = 0, cap_step_offset = 0;
   int blocks_persistent = 0;
 };
 
 struct psb_batch {
   std::vector<BatchMemberHost> hm;
+  std::vector<double> res_init;  // 4 per member, uploaded by batch_prepare when set
   BMember *d_members = nullptr;
   CUtensorMap *d_tmaps = nullptr;
   double *d_partials = nullptr;
   unsigned *d_done = nullptr;
   int *d_stop = nullptr;
   double *d_res = nullptr;
+  size_t cap_members = 0, cap_tmaps = 0, cap_partials = 0, cap_done = 0, cap_stop = 0,
+         cap_res = 0;  // bytes allocated (device buffers are reused while they fit)
   std::vector<BMember> members;
   BatchGroup grp[2];
   bool built = false;
@@ -361,9 +363,15 @@ namespace psb {
 
 static int member_group(int kind) { return kind == BK_HIMENO ? 1 : 0; }
 
-static void batch_release_device(psb_batch *b) {
+// The work lists and descriptors no longer match the members.
+static void batch_invalidate(psb_batch *b) {
   if (b->graph) cudaGraphExecDestroy(b->graph);
   b->graph = nullptr;
+  b->built = false;
+}
+
+static void batch_release_device(psb_batch *b) {
+  batch_invalidate(b);
   cudaFree(b->d_members);
   cudaFree(b->d_tmaps);
   cudaFree(b->d_partials);
@@ -376,6 +384,7 @@ static void batch_release_device(psb_batch *b) {
   b->d_done = nullptr;
   b->d_stop = nullptr;
   b->d_res = nullptr;
+  b->cap_members = b->cap_tmaps = b->cap_partials = b->cap_done = b->cap_stop = b->cap_res = 0;
   for (auto &g : b->grp) {
     cudaFree(g.d_order);
     cudaFree(g.d_tile_prefix);
@@ -383,7 +392,21 @@ static void batch_release_device(psb_batch *b) {
     cudaFree(g.d_cursor);
     g = BatchGroup();
   }
-  b->built = false;
+}
+
+// Make *p hold at least `bytes` (grown by half again when it must grow, so
+// a server's changing member list rarely reallocates).
+template <typename T>
+static psb_status dev_reserve(T **p, size_t *cap, size_t bytes) {
+  bytes = std::max<size_t>(bytes, 16);
+  if (bytes <= *cap) return PSB_OK;
+  const size_t want = std::max(bytes, *cap + *cap / 2);
+  cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  PSB_TRY(cudaMalloc((void **)p, want));
+  *cap = want;
+  return PSB_OK;
 }
 
 static TmaGeom batch_dgeom(const GridImpl *g) {
@@ -437,7 +460,7 @@ static size_t batch_smem(int group) {
 psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std::vector<int> &step0) {
   Runtime &r = rt();
   const int n = (int)b->hm.size();
-  batch_release_device(b);
+  batch_invalidate(b);
   b->members.assign(n, BMember());
   std::vector<CUtensorMap> tmaps(2 * std::max(1, n));
   int64_t partial_slots = 0;
@@ -494,14 +517,18 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     M.ntiles = M.tiles_x * M.tiles_y * M.nzc;
     partial_slots += 4 * (int64_t)M.ntiles;
   }
-  PSB_TRY(cudaMalloc(&b->d_tmaps, sizeof(CUtensorMap) * tmaps.size()));
+  PSB_CHECK(dev_reserve(&b->d_tmaps, &b->cap_tmaps, sizeof(CUtensorMap) * tmaps.size()));
   PSB_TRY(cudaMemcpy(b->d_tmaps, tmaps.data(), sizeof(CUtensorMap) * tmaps.size(),
                      cudaMemcpyHostToDevice));
-  PSB_TRY(cudaMalloc(&b->d_partials, sizeof(double) * std::max<int64_t>(1, partial_slots)));
-  PSB_TRY(cudaMalloc(&b->d_done, sizeof(unsigned) * std::max(1, n)));
-  PSB_TRY(cudaMalloc(&b->d_stop, sizeof(int) * std::max(1, n)));
-  PSB_TRY(cudaMalloc(&b->d_res, sizeof(double) * 4 * std::max(1, n)));
-  PSB_TRY(cudaMemset(b->d_res, 0, sizeof(double) * 4 * std::max(1, n)));
+  PSB_CHECK(dev_reserve(&b->d_partials, &b->cap_partials,
+                        sizeof(double) * std::max<int64_t>(1, partial_slots)));
+  PSB_CHECK(dev_reserve(&b->d_done, &b->cap_done, sizeof(unsigned) * std::max(1, n)));
+  PSB_CHECK(dev_reserve(&b->d_stop, &b->cap_stop, sizeof(int) * std::max(1, n)));
+  PSB_CHECK(dev_reserve(&b->d_res, &b->cap_res, sizeof(double) * 4 * std::max(1, n)));
+  if ((int)b->res_init.size() == 4 * n && n > 0)
+    PSB_TRY(cudaMemcpy(b->d_res, b->res_init.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice));
+  else
+    PSB_TRY(cudaMemset(b->d_res, 0, sizeof(double) * 4 * std::max(1, n)));
   int64_t off = 0;
   for (int i = 0; i < n; i++) {
     BMember &M = b->members[i];
@@ -513,12 +540,13 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     M.stop = b->d_stop + i;
     M.res = b->d_res + 4 * i;
   }
-  PSB_TRY(cudaMalloc(&b->d_members, sizeof(BMember) * std::max(1, n)));
+  PSB_CHECK(dev_reserve(&b->d_members, &b->cap_members, sizeof(BMember) * std::max(1, n)));
   PSB_TRY(cudaMemcpy(b->d_members, b->members.data(), sizeof(BMember) * n, cudaMemcpyHostToDevice));
   // One work list per kernel kind. Members are ordered by steps
   // (descending), so the members still running at step s are a prefix.
   for (int gi = 0; gi < 2; gi++) {
     BatchGroup &G = b->grp[gi];
+    G.order.clear();
     for (int i = 0; i < n; i++)
       if (member_group(b->hm[i].kind) == gi) G.order.push_back(i);
     std::stable_sort(G.order.begin(), G.order.end(),
@@ -535,15 +563,16 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
       G.step_offset[st + 1] = G.step_offset[st] + G.tile_prefix[active];
     }
     G.total_items = G.max_steps ? G.step_offset[G.max_steps] : 0;
-    PSB_TRY(cudaMalloc(&G.d_order, sizeof(int) * std::max(1, gn)));
+    PSB_CHECK(dev_reserve(&G.d_order, &G.cap_order, sizeof(int) * std::max(1, gn)));
     if (gn) PSB_TRY(cudaMemcpy(G.d_order, G.order.data(), sizeof(int) * gn, cudaMemcpyHostToDevice));
-    PSB_TRY(cudaMalloc(&G.d_tile_prefix, sizeof(int64_t) * (gn + 1)));
+    PSB_CHECK(dev_reserve(&G.d_tile_prefix, &G.cap_tile_prefix, sizeof(int64_t) * (gn + 1)));
     PSB_TRY(cudaMemcpy(G.d_tile_prefix, G.tile_prefix.data(), sizeof(int64_t) * (gn + 1),
                        cudaMemcpyHostToDevice));
-    PSB_TRY(cudaMalloc(&G.d_step_offset, sizeof(int64_t) * (G.max_steps + 1)));
+    PSB_CHECK(dev_reserve(&G.d_step_offset, &G.cap_step_offset,
+                          sizeof(int64_t) * (G.max_steps + 1)));
     PSB_TRY(cudaMemcpy(G.d_step_offset, G.step_offset.data(), sizeof(int64_t) * (G.max_steps + 1),
                        cudaMemcpyHostToDevice));
-    PSB_TRY(cudaMalloc(&G.d_cursor, sizeof(unsigned long long)));
+    if (!G.d_cursor) PSB_TRY(cudaMalloc(&G.d_cursor, sizeof(unsigned long long)));
     int per_sm = 0;
     if (gi == 0) {
       PSB_TRY(cudaFuncSetAttribute(k_batch_persistent<0>,
@@ -565,6 +594,18 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     G.blocks_persistent = std::max(1, per_sm) * r.sm_count;
   }
   b->built = true;
+  return PSB_OK;
+}
+
+// After a run: per member, local steps completed when it converged (-1 if
+// it did not) and its residual state (4 doubles).
+psb_status batch_read_state(psb_batch *b, std::vector<int> &stop, std::vector<double> &res) {
+  const int n = (int)b->hm.size();
+  stop.assign(n, -1);
+  res.assign(4 * n, 0.0);
+  if (!b->built || n == 0) return PSB_OK;
+  PSB_TRY(cudaMemcpy(stop.data(), b->d_stop, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  PSB_TRY(cudaMemcpy(res.data(), b->d_res, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost));
   return PSB_OK;
 }
 
@@ -660,9 +701,34 @@ psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches) {
 // ===========================================================================
 namespace psb {
 
+psb_batch *batch_new() {
+  psb_batch *b = new psb_batch();
+  cudaEventCreate(&b->ev0);
+  cudaEventCreate(&b->ev1);
+  return b;
+}
+
+void batch_set_members(psb_batch *b, const std::vector<BatchMemberHost> &m,
+                       const std::vector<double> &res_init) {
+  batch_invalidate(b);
+  b->hm = m;
+  b->res_init = res_init;
+}
+
+void batch_delete(psb_batch *b) {
+  if (!b) return;
+  batch_release_device(b);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  if (b->side) cudaStreamDestroy(b->side);
+  if (b->fork) cudaEventDestroy(b->fork);
+  if (b->join) cudaEventDestroy(b->join);
+  delete b;
+}
+
 psb_status batch_add_member(psb_batch *b, const BatchMemberHost &m) {
   b->hm.push_back(m);
-  batch_release_device(b);
+  batch_invalidate(b);
   return PSB_OK;
 }
 
@@ -832,7 +898,7 @@ psb_status psb_batch_set_stop(psb_batch *b, int member, double tol, int check_ev
     return set_status(PSB_ERR_INVALID);
   b->hm[member].tol = tol;
   b->hm[member].check_every = check_every;
-  batch_release_device(b);
+  batch_invalidate(b);
   return PSB_OK;
 }
 

@@ -7,6 +7,8 @@
 
 namespace psb {
 
+enum { BK_DIFF7 = 0, BK_DIFF7P = 1, BK_HIMENO = 2 };
+
 struct BatchMemberHost {
   int kind = 0;            // 0 diffusion clamped, 1 diffusion periodic, 2 Himeno
   int kernel_id = 0;       // PSB_KERNEL_*
@@ -29,4 +31,10 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
 psb_status batch_launch_persistent(psb_batch *b, cudaStream_t s, int64_t *launches);
 psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches);
 psb_status batch_add_member(psb_batch *b, const BatchMemberHost &m);
+psb_status batch_read_state(psb_batch *b, std::vector<int> &stop, std::vector<double> &res);
+// Server access to a batch's member list (replaced every round).
+psb_batch *batch_new();
+void batch_set_members(psb_batch *b, const std::vector<BatchMemberHost> &m,
+                       const std::vector<double> &res_init);
+void batch_delete(psb_batch *b);
 }  // namespace psb

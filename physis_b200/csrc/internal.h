@@ -163,6 +163,15 @@ psb_status launch_map(MapImpl &m, int color, int64_t *launches);
 psb_status prepare_ghosts(MapImpl &m);
 psb_status launch_halo_fill(GridImpl *g, int mode, cudaStream_t s);
 
+// Pitched 3-D grids in a stream-ordered memory pool (serving): allocation and
+// zero fill on stream s, free after the work queued on s.
+size_t grid_pitched_bytes(int elm_size, const int *dims);
+psb_status grid_alloc_pool(int type, const int *dims, cudaMemPool_t pool, cudaStream_t s,
+                           GridImpl **out);
+void grid_free_pool(GridImpl *g, cudaStream_t s);
+psb_status grid_copy_in_on(GridImpl *g, const void *src, cudaStream_t s);
+psb_status grid_copy_out_on(GridImpl *g, void *dst, cudaStream_t s);
+
 // Kernel launchers implemented in the .cu files.
 psb_status diffusion7_launch(MapImpl &m, const psb_tune_config &cfg, cudaStream_t s,
                              int64_t *launches);

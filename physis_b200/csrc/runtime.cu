@@ -170,17 +170,11 @@ static void set_dev_struct(GridImpl *g, void *p0) {
   g->pub.dev = (__PSGrid_dev *)&g->dev;
 }
 
-// Allocate a grid. Dense: exactly the reference layout. Pitched: x rows are
-// padded to 128 bytes with one 128-byte line (at least PSB_HALO cells) left
-// of logical x = 0, and PSB_HALO halo rows/planes around y and z.
-static psb_status grid_alloc(int type, int elm_size, int nd, const int *dims, int layout,
-                             GridImpl **out) {
-  *out = nullptr;
-  if (nd < 1 || nd > 3) return set_status(PSB_ERR_INVALID);
-  for (int i = 0; i < nd; i++)
-    if (dims[i] <= 0) return set_status(PSB_ERR_INVALID);
-  if (elm_size <= 0) return set_status(PSB_ERR_INVALID);
-  PSB_CHECK(ensure_init());
+// Describe a grid (layout and strides; no allocation). Dense: exactly the
+// reference layout. Pitched: x rows are padded to 128 bytes with one
+// 128-byte line (at least PSB_HALO cells) left of logical x = 0, and
+// PSB_HALO halo rows/planes around y and z.
+static GridImpl *grid_describe(int type, int elm_size, int nd, const int *dims, int layout) {
   GridImpl *g = new GridImpl();
   g->pub.elm_size = elm_size;
   g->pub.num_dims = nd;
@@ -211,6 +205,26 @@ static psb_status grid_alloc(int type, int elm_size, int nd, const int *dims, in
     g->origin_off = 0;
   }
   g->alloc_bytes = (size_t)g->pitch * g->rows * g->planes * elm_size;
+  return g;
+}
+
+// Point a described grid at its allocation; a zero-filled grid has a
+// consistent halo for every boundary mode (the interior is zero too).
+static void grid_attach(GridImpl *g) {
+  g->ghost_valid = g->layout == PSB_LAYOUT_PITCHED ? PSB_BOUNDARY_PERIODIC : PSB_BOUNDARY_NONE;
+  g->pub.p0 = (char *)g->alloc + g->origin_off * g->pub.elm_size;
+  set_dev_struct(g, g->pub.p0);
+}
+
+static psb_status grid_alloc(int type, int elm_size, int nd, const int *dims, int layout,
+                             GridImpl **out) {
+  *out = nullptr;
+  if (nd < 1 || nd > 3) return set_status(PSB_ERR_INVALID);
+  for (int i = 0; i < nd; i++)
+    if (dims[i] <= 0) return set_status(PSB_ERR_INVALID);
+  if (elm_size <= 0) return set_status(PSB_ERR_INVALID);
+  PSB_CHECK(ensure_init());
+  GridImpl *g = grid_describe(type, elm_size, nd, dims, layout);
   cudaError_t e = cudaMalloc(&g->alloc, g->alloc_bytes);
   if (e != cudaSuccess) {
     delete g;
@@ -224,12 +238,70 @@ static psb_status grid_alloc(int type, int elm_size, int nd, const int *dims, in
     delete g;
     return cuda_status(e, "cudaMemset(grid)");
   }
-  // A zero-filled grid has a consistent halo for every mode only if the
-  // interior is zero too, which it is.
-  g->ghost_valid = g->layout == PSB_LAYOUT_PITCHED ? PSB_BOUNDARY_PERIODIC : PSB_BOUNDARY_NONE;
-  g->pub.p0 = (char *)g->alloc + g->origin_off * elm_size;
-  set_dev_struct(g, g->pub.p0);
+  grid_attach(g);
   *out = g;
+  return PSB_OK;
+}
+
+size_t grid_pitched_bytes(int elm_size, const int *dims) {
+  GridImpl *g = grid_describe(PS_FLOAT, elm_size, 3, dims, PSB_LAYOUT_PITCHED);
+  const size_t b = g->alloc_bytes;
+  delete g;
+  return b;
+}
+
+psb_status grid_alloc_pool(int type, const int *dims, cudaMemPool_t pool, cudaStream_t s,
+                           GridImpl **out) {
+  *out = nullptr;
+  for (int i = 0; i < 3; i++)
+    if (dims[i] <= 0) return set_status(PSB_ERR_INVALID);
+  GridImpl *g = grid_describe(type, type_size(type), 3, dims, PSB_LAYOUT_PITCHED);
+  cudaError_t e = cudaMallocFromPoolAsync(&g->alloc, g->alloc_bytes, pool, s);
+  if (e == cudaSuccess) e = cudaMemsetAsync(g->alloc, 0, g->alloc_bytes, s);
+  if (e != cudaSuccess) {
+    if (g->alloc) cudaFreeAsync(g->alloc, s);
+    delete g;
+    cudaGetLastError();
+    return cuda_status(e, "cudaMallocFromPoolAsync(grid)");
+  }
+  grid_attach(g);
+  *out = g;
+  return PSB_OK;
+}
+
+void grid_free_pool(GridImpl *g, cudaStream_t s) {
+  if (!g) return;
+  if (g->alloc) cudaFreeAsync(g->alloc, s);
+  g->magic = 0;
+  delete g;
+}
+
+psb_status grid_copy_in_on(GridImpl *g, const void *src, cudaStream_t s) {
+  const int E = g->pub.elm_size;
+  cudaMemcpy3DParms p;
+  memset(&p, 0, sizeof(p));
+  const int nx = g->pub.dim[0], ny = g->pub.dim[1], nz = g->pub.dim[2];
+  p.srcPtr = make_cudaPitchedPtr((void *)src, (size_t)nx * E, nx, ny);
+  p.dstPtr = make_cudaPitchedPtr(g->alloc, (size_t)g->pitch * E, g->pitch, g->rows);
+  p.dstPos = make_cudaPos((size_t)g->pad_left * E, g->halo, g->halo);
+  p.extent = make_cudaExtent((size_t)nx * E, ny, nz);
+  p.kind = cudaMemcpyHostToDevice;
+  PSB_TRY(cudaMemcpy3DAsync(&p, s));
+  g->ghost_valid = PSB_BOUNDARY_NONE;
+  return PSB_OK;
+}
+
+psb_status grid_copy_out_on(GridImpl *g, void *dst, cudaStream_t s) {
+  const int E = g->pub.elm_size;
+  cudaMemcpy3DParms p;
+  memset(&p, 0, sizeof(p));
+  const int nx = g->pub.dim[0], ny = g->pub.dim[1], nz = g->pub.dim[2];
+  p.srcPtr = make_cudaPitchedPtr(g->alloc, (size_t)g->pitch * E, g->pitch, g->rows);
+  p.srcPos = make_cudaPos((size_t)g->pad_left * E, g->halo, g->halo);
+  p.dstPtr = make_cudaPitchedPtr(dst, (size_t)nx * E, nx, ny);
+  p.extent = make_cudaExtent((size_t)nx * E, ny, nz);
+  p.kind = cudaMemcpyDeviceToHost;
+  PSB_TRY(cudaMemcpy3DAsync(&p, s));
   return PSB_OK;
 }
 

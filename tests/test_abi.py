@@ -3,6 +3,7 @@
 import ctypes
 import os
 import re
+import subprocess
 
 import pytest
 
@@ -72,6 +73,34 @@ def test_struct_layouts_match_reference_abi():
     assert ctypes.sizeof(ps.PSGridStruct) == 48
     assert ps.PSGridStruct.num_elms.offset == 32 and ps.PSGridStruct.dev.offset == 40
     assert ctypes.sizeof(ps.PSDomain) == 48
+
+
+def test_ctypes_structs_match_header(tmp_path):
+    """Sizes and field offsets of the ctypes mirrors equal the C header's."""
+    import physis_b200 as ps
+    structs = {"psb_request": ps.Request, "psb_result": ps.Result,
+               "psb_tune_config": ps.TuneConfig, "psb_generic_stencil": ps.GenericStencilStruct}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "physis_b200.h"',
+             'int main(void) {']
+    for cname, cls in structs.items():
+        lines.append('printf("%s sizeof %%zu\\n", sizeof(%s));' % (cname, cname))
+        for f in cls._fields_:
+            lines.append('printf("%s %s %%zu\\n", offsetof(%s, %s));' % (cname, f[0], cname, f[0]))
+    lines += ['return 0;', '}']
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
+                   check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                               text=True).stdout.splitlines():
+        c, f, v = line.split()
+        got[(c, f)] = int(v)
+    for cname, cls in structs.items():
+        assert got[(cname, "sizeof")] == ctypes.sizeof(cls), cname
+        for f in cls._fields_:
+            assert got[(cname, f[0])] == getattr(cls, f[0]).offset, (cname, f[0])
 
 
 def test_domain_constructors_need_no_gpu():
