@@ -156,44 +156,52 @@ class ClockSampler:
 # Our arm
 # ---------------------------------------------------------------------------
 class Dist:
+    """One process per GPU (torchrun env): barriers and max/sum over ranks.
+    NCCL on GPU hosts; gloo where no GPU is visible (host-side tests)."""
+
     def __init__(self, gpus):
         self.world = int(os.environ.get("WORLD_SIZE", "1"))
         self.rank = int(os.environ.get("RANK", "0"))
         self.local = int(os.environ.get("LOCAL_RANK", "0"))
         self.pg = None
+        self.device = "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                    device_id=torch.device("cuda", self.local))
+            timeout = datetime.timedelta(seconds=300)
+            if torch.cuda.is_available():
+                torch.cuda.set_device(self.local)
+                self.device = "cuda"
+                dist.init_process_group("nccl", timeout=timeout,
+                                        device_id=torch.device("cuda", self.local))
+            else:
+                dist.init_process_group("gloo", timeout=timeout)
             self.pg = dist
 
     def barrier(self):
         if self.pg:
             self.pg.barrier()
 
-    def max(self, v):
+    def _reduce(self, v, op):
         if not self.pg:
             return v
         import torch
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
+        self.pg.all_reduce(t, op=op)
         return float(t.item())
 
+    def max(self, v):
+        return self._reduce(v, self.pg.ReduceOp.MAX if self.pg else None)
+
     def sum(self, v):
-        if not self.pg:
-            return v
-        import torch
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
-        return float(t.item())
+        return self._reduce(v, self.pg.ReduceOp.SUM if self.pg else None)
 
     def close(self):
         if self.pg:
             self.pg.destroy_process_group()
+            self.pg = None
 
 
 def load_traffic(kernel_name):
@@ -399,18 +407,17 @@ def run_ours(args):
 # Reference arm
 # ---------------------------------------------------------------------------
 def _ref_worker(args):
-    wl, dims, dt_name, count, seed = args
+    kind, dims, dt_name, count, seed = args
     sys.path.insert(0, ROOT)
     from oracle import oracle
     dt = np.dtype(dt_name)
-    k = WORKLOADS[wl][0]
-    if k == "himeno":
+    if kind == "himeno":
         p, coef = himeno_fields(dims, seed)
         _, secs = oracle.ref_himeno(p, coef, 0.8, count)
         nx, ny, nz = dims
         return (nx - 2) * (ny - 2) * (nz - 2) * count, secs
     f = c2_field(dims, dt, seed)
-    _, secs = oracle.ref_diffusion7(f, count, np.asarray(COEF, dt))
+    _, secs = oracle.ref_diffusion7(f, count, np.asarray(COEF, dt), periodic=kind == "diffusion7p")
     return dims[0] * dims[1] * dims[2] * count, secs
 
 
@@ -723,6 +730,20 @@ def c5_cpu_baseline(trace, steps_done):
                       % (rate_d / 1e9, rate_h / 1e9)}
 
 
+def _ref_rate(pool, procs, kind, dims, dt, count, reps, warm):
+    """Aggregate rate of the reference CPU target: `procs` processes, each
+    running its own solve of `count` steps; lattice updates / slowest loop."""
+    vals = []
+    for i in range(warm + reps):
+        jobs = [(kind, dims, np.dtype(dt).name, count, 1000 + j) for j in range(procs)]
+        res = pool.map(_ref_worker, jobs)
+        if i >= warm:
+            vals.append((sum(r[0] for r in res), max(r[1] for r in res)))
+    pts = sum(v[0] for v in vals)
+    loop_s = sum(v[1] for v in vals)
+    return pts / loop_s, loop_s / len(vals)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -741,39 +762,65 @@ def run_reference(args):
         avail = os.sysconf("SC_AVPHYS_PAGES") * os.sysconf("SC_PAGE_SIZE")
     except Exception:
         avail = 16 << 30
+    ctx = mp.get_context("spawn")
+    common = {"n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+              "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+              "data": "synthetic", "impl": "reference"}
+    if kname in ("batch", "serve"):
+        # Independent solves: sample each stencil's rate on all host cores and
+        # apply it to the workload's lattice updates.
+        sd, sh = (128, 128, 128), (129, 129, 129)
+        per = 14 * int(np.prod(sh)) * 4
+        procs = max(1, min(ncpu, int(avail * 0.6 // per), args.ref_procs))
+        dkind = "diffusion7p" if kname == "batch" else "diffusion7"
+        with ctx.Pool(procs) as pool:
+            rate_d, _ = _ref_rate(pool, procs, dkind, sd, np.float32, 10, max(1, args.steps // 3), 1)
+            rate_h, _ = _ref_rate(pool, procs, "himeno", sh, np.float32, 4, max(1, args.steps // 3), 1)
+        if kname == "batch":
+            members = c4_members(count=args.members)
+            lu_d = sum(d[0] * d[1] * d[2] * st for k, d, st in members if k == "diffp")
+            lu_h = sum((d[0] - 2) * (d[1] - 2) * (d[2] - 2) * st for k, d, st in members if k == "him")
+            secs = lu_d / rate_d + lu_h / rate_h
+            value, unit, metric = (lu_d + lu_h) / secs / 1e9, "GLUPS", "lattice_updates_per_s_c4"
+            per_step = secs
+            what = "the batch's %d members at their step counts" % len(members)
+        else:
+            trace = c5_trace(count=args.c5_requests)
+            secs = sum(c5_points(k, side) * C5_MAX_STEPS / (rate_h if k == "him" else rate_d)
+                       for _, k, side, _ in trace)
+            value, unit, metric = len(trace) / secs, "solves/s", "served_solves_per_s_c5"
+            per_step = secs / len(trace)
+            what = ("the trace's %d requests at %d steps each (the reference has no residual "
+                    "stop)" % (len(trace), C5_MAX_STEPS))
+        sample = ("rates of %s 128^3 x 10 steps (%.2f GLUPS) and Himeno 129^3 x 4 sweeps "
+                  "(%.2f GLUPS), each on %d processes at once, applied to %s"
+                  % (dkind, rate_d / 1e9, rate_h / 1e9, procs, what))
+        line = dict(common, metric=metric, value=value, unit=unit, ms_per_step=per_step * 1e3,
+                    dtype="f32", config={"workload": describe(wl),
+                                         "parallelism": "%d host processes" % procs},
+                    cpu_baseline={"value": value, "unit": unit, "cores": procs,
+                                  "kind": "reference", "sample": sample},
+                    e2e={"value": value, "unit": unit, "h2d_bytes_per_step": 0,
+                         "d2h_bytes_per_step": 0})
+        print(json.dumps(line), flush=True)
+        return
     per = (14 if kname == "himeno" else 3) * int(np.prod(dims)) * np.dtype(dt).itemsize
     procs = max(1, min(ncpu, int(avail * 0.6 // per), args.ref_procs))
-    count = 2 if kname != "himeno" else 2
-    ctx = mp.get_context("spawn")
-    vals = []
+    count = 2
     with ctx.Pool(procs) as pool:
-        for i in range(args.warmup + args.steps):
-            jobs = [(wl, dims, np.dtype(dt).name, count, 1000 + j) for j in range(procs)]
-            t0 = time.perf_counter()
-            res = pool.map(_ref_worker, jobs)
-            wall = time.perf_counter() - t0
-            pts = sum(r[0] for r in res)
-            loop = max(r[1] for r in res)
-            if i >= args.warmup:
-                vals.append((pts, loop, wall))
-    pts = sum(v[0] for v in vals)
-    loop_s = sum(v[1] for v in vals)
-    value = pts / loop_s / 1e9
+        rate, loop_s = _ref_rate(pool, procs, kname, dims, dt, count, args.steps, args.warmup)
+    value = rate / 1e9
     sample = ("%d independent %dx%dx%d %s solves of %d %s each per step, one per process, "
               "run loop timed (copies excluded)" % (procs, dims[0], dims[1], dims[2],
                                                      np.dtype(dt).name, count,
                                                      "sweeps" if kname == "himeno" else "time steps"))
-    line = {
-        "metric": "lattice_updates_per_s_" + wl, "value": value, "unit": "GLUPS",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": loop_s / len(vals) * 1e3, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32" if dt == np.float32 else "f64", "data": "synthetic",
-        "config": {"workload": describe(wl), "parallelism": "%d host processes" % procs},
-        "impl": "reference",
-        "cpu_baseline": {"value": value, "unit": "GLUPS", "cores": procs, "kind": "reference",
-                         "sample": sample},
-        "e2e": {"value": value, "unit": "GLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    line = dict(common, metric="lattice_updates_per_s_" + wl, value=value, unit="GLUPS",
+                ms_per_step=loop_s * 1e3, dtype="f32" if dt == np.float32 else "f64",
+                config={"workload": describe(wl), "parallelism": "%d host processes" % procs},
+                cpu_baseline={"value": value, "unit": "GLUPS", "cores": procs, "kind": "reference",
+                              "sample": sample},
+                e2e={"value": value, "unit": "GLUPS", "h2d_bytes_per_step": 0,
+                     "d2h_bytes_per_step": 0})
     print(json.dumps(line), flush=True)
 
 

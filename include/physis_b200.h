@@ -569,7 +569,9 @@ typedef struct {
   double residual;        /* last relative residual, -1 if never checked */
   double submit_s, start_s, finish_s;  /* host steady clock, seconds */
 } psb_result;
-/* max_slots: requests on the device at once (0: no limit). */
+/* max_slots: requests advanced at once (0: no limit). The budget covers
+ * every resident grid, including those of finished requests whose results
+ * are still being copied out. */
 psb_status psb_server_create(size_t mem_budget_bytes, int max_slots, int mode,
                              psb_server **s);
 /* Queue a request. init, coef and out must stay valid until the request

@@ -4,7 +4,8 @@
 // or periodic, or a Himeno Jacobi relaxation, float) of `steps` steps, i.e.
 // what PSStencilRun(m(g0->g1), m(g1->g0), steps/2) does for one grid. The
 // work of all members is cut into items -- (member, step, tile) where a tile
-// is a 64-wide column of the member's domain over a z chunk -- and laid out in
+// is a 32-, 64- or 128-wide column of the member's domain (the shape that
+// fits its extent best) over a z chunk -- and laid out in
 // one device-side work list ordered by step, then member, then tile.
 //
 // Mode 0 (persistent): one launch with one CTA per resident slot. CTAs take
@@ -39,10 +40,10 @@
 
 namespace psb {
 
-// Fixed tile shape of batched items: 64 points wide, 128 consumer threads.
-constexpr int kBTx = 16;       // consumer threads along x (x 4 floats = 64 points)
-constexpr int kBTy = 8;        // consumer thread rows
-constexpr int kBThreads = kBTx * kBTy + 32;
+// Batched items run 128 consumer threads (tile shape per member) and one
+// producer warp.
+constexpr int kBConsumers = 128;
+constexpr int kBThreads = kBConsumers + 32;
 constexpr int kBStages = 6;
 
 struct BMember {
@@ -151,7 +152,7 @@ __device__ __forceinline__ bool batch_item(const BMember &M, int s, int t, unsig
   double a = 0, b = 0;
   bool bad = false;
   if (!skip) {
-    if (threadIdx.x == kBTx * kBTy)  // producer: order generic acquire before TMA reads
+    if (threadIdx.x == kBConsumers)  // producer: order generic acquire before TMA reads
       asm volatile("fence.proxy.async.global;" ::: "memory");
     if constexpr (GROUP == 1) {
       double g = 0;
@@ -409,11 +410,35 @@ static psb_status dev_reserve(T **p, size_t *cap, size_t bytes) {
   return PSB_OK;
 }
 
+// Tile shapes of batched items: 128 consumer threads as 8 x 16, 16 x 8 or
+// 32 x 4 (x threads of 4 floats each x rows); each member takes the shape
+// with the fewest tiles over its x-y extent (then the fewest box elements),
+// so small and narrow members waste few threads on partial tiles.
+constexpr int kBShapes[3][2] = {{8, 16}, {16, 8}, {32, 4}};
+
+static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int *ty_threads) {
+  int64_t best_tiles = -1, best_box = 0;
+  for (const auto &sh : kBShapes) {
+    const int TX = sh[0] * 4, TY = sh[1] * rows_per_thread;
+    const int64_t tiles = (int64_t)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
+    const int64_t box = tiles * (TX + 8) * (TY + 2);
+    if (best_tiles < 0 || tiles < best_tiles || (tiles == best_tiles && box < best_box)) {
+      best_tiles = tiles;
+      best_box = box;
+      *tx_threads = sh[0];
+      *ty_threads = sh[1];
+    }
+  }
+}
+
+static int stage_bytes_of(int tx_threads, int ty_threads, int rows_per_thread) {
+  return ((tx_threads * 4 + 8) * (ty_threads * rows_per_thread + 2) * 4 + 127) / 128 * 128;
+}
+
 static TmaGeom batch_dgeom(const GridImpl *g) {
   TmaGeom geo;
-  geo.tx_threads = kBTx;
-  geo.ty_threads = kBTy;
-  const int TX = kBTx * 4, TY = kBTy * kVY;
+  pick_shape(g->pub.dim[0], g->pub.dim[1], kVY, &geo.tx_threads, &geo.ty_threads);
+  const int TX = geo.tx_threads * 4, TY = geo.ty_threads * kVY;
   geo.bx = TX + 8;
   geo.by = TY + 2;
   geo.ax0 = g->pad_left;
@@ -424,35 +449,35 @@ static TmaGeom batch_dgeom(const GridImpl *g) {
   geo.tiles_y = (g->pub.dim[1] + TY - 1) / TY;
   geo.zchunk = 64;
   geo.stages = kBStages;
-  geo.stage_bytes = (geo.bx * geo.by * 4 + 127) / 128 * 128;
+  geo.stage_bytes = stage_bytes_of(geo.tx_threads, geo.ty_threads, kVY);
   return geo;
 }
 
 static HimenoGeom batch_hgeom(const GridImpl *g) {
   HimenoGeom geo;
-  geo.tx_threads = kBTx;
-  geo.ty_threads = kBTy;
-  const int TX = kBTx * 4, TY = kBTy;
+  // interior domain [1, n-1): tiles start at x = 0 (x_base), y = 1.
+  pick_shape(g->pub.dim[0] - 1, g->pub.dim[1] - 2, 1, &geo.tx_threads, &geo.ty_threads);
+  const int TX = geo.tx_threads * 4, TY = geo.ty_threads;
   geo.bx = TX + 8;
   geo.by = TY + 2;
   geo.ax0 = g->pad_left;
   geo.ay0 = g->halo;
   geo.az0 = g->halo;
   geo.x_base = 0;
-  // interior domain [1, n-1): tiles start at x = 0 (x_base), y = 1.
   geo.tiles_x = (g->pub.dim[0] - 1 + TX - 1) / TX;
   geo.tiles_y = (g->pub.dim[1] - 2 + TY - 1) / TY;
   geo.zchunk = 64;
   geo.stages = kBStages;
-  geo.stage_bytes = (geo.bx * geo.by * 4 + 127) / 128 * 128;
+  geo.stage_bytes = stage_bytes_of(geo.tx_threads, geo.ty_threads, 1);
   geo.nx = g->pub.dim[0];
   return geo;
 }
 
 static size_t batch_smem(int group) {
-  const int dstage = ((kBTx * 4 + 8) * (kBTy * kVY + 2) * 4 + 127) / 128 * 128;
-  const int hstage = ((kBTx * 4 + 8) * (kBTy + 2) * 4 + 127) / 128 * 128;
-  return group == 0 ? 128 + 512 + (size_t)kBStages * dstage : 128 + 768 + (size_t)kBStages * hstage;
+  int stage = 0;
+  for (const auto &sh : kBShapes)
+    stage = std::max(stage, stage_bytes_of(sh[0], sh[1], group == 0 ? kVY : 1));
+  return group == 0 ? 128 + 512 + (size_t)kBStages * stage : 128 + 768 + (size_t)kBStages * stage;
 }
 
 // Build the device work lists and member descriptors for one launch in which

@@ -514,7 +514,7 @@ psb_status psb_stencil_free(PSStencil s) {
   drop_graphs();
   if (m->d_partials) cudaFree(m->d_partials);
   if (m->d_ticket) cudaFree(m->d_ticket);
-  if (m->d_counter) cudaFree(m->d_counter);
+  // d_counter points into the d_ticket allocation.
   if (m->d_history) cudaFree(m->d_history);
   *m = MapImpl();
   return PSB_OK;

@@ -489,7 +489,7 @@ void PSFinalize(void) {
   for (auto &m : r.maps) {
     if (m.d_partials) cudaFree(m.d_partials);
     if (m.d_ticket) cudaFree(m.d_ticket);
-    if (m.d_counter) cudaFree(m.d_counter);
+    // d_counter points into the d_ticket allocation.
     if (m.d_history) cudaFree(m.d_history);
   }
   r.maps.clear();

@@ -145,7 +145,8 @@ def test_budget_and_slots():
     assert stats["peak_bytes"] >= one
     # Same results with one slot at a time.
     recs1, outs1, stats1 = _serve(reqs, slots=1)
-    assert stats1["peak_bytes"] == one
+    # One request advancing, at most one more whose result is being copied out.
+    assert one <= stats1["peak_bytes"] <= 2 * one
     for a, b in zip(outs, outs1):
         assert bits_equal(a, b)
     # A request larger than the whole budget is refused at submit.
