@@ -26,7 +26,8 @@ import os
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "libphysis_rt_b200.so")
+# PHYSIS_B200_LIB selects another build of the library (same ABI).
+LIB_PATH = os.environ.get("PHYSIS_B200_LIB") or os.path.join(_HERE, "lib", "libphysis_rt_b200.so")
 
 # ---------------------------------------------------------------------------
 # Constants (include/physis_b200.h)

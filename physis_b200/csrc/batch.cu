@@ -5,29 +5,34 @@
 // what PSStencilRun(m(g0->g1), m(g1->g0), steps/2) does for one grid. The
 // work of all members is cut into items -- (member, step, tile) where a tile
 // is a 32-, 64- or 128-wide column of the member's domain (the shape that
-// fits its extent best) over a z chunk -- and laid out in
-// one device-side work list ordered by step, then member, then tile.
+// fits its extent best) over a z chunk -- and laid out in one device-side
+// work list per stencil kind, ordered by step, then member, then tile.
 //
-// Mode 0 (persistent): one launch with one CTA per resident slot. CTAs take
-// items from the list with an atomic cursor; an item of step s of member m
-// waits until every tile of step s-1 of m is complete (a per-member counter,
-// acquire load, bounded wait). Because the list is ordered by step, every
-// dependency of an item is taken by a CTA before the item itself, so the
-// earliest unfinished item can always run: the launch needs no co-residency
-// guarantee and cannot deadlock. Small members no longer leave the GPU idle
-// between their steps and there are no launch gaps.
-// Mode 1 (graph): one launch per step over all members still running, the
-// sequence captured once in a CUDA graph and replayed.
+// Mode 0 (persistent): one launch per kind with one CTA per resident slot.
+// In each CTA a producer thread takes items from the list with an atomic
+// cursor, waits until the item's member has completed the previous step (a
+// per-member counter, acquire load, bounded wait), passes the item to the
+// consumer warps through a small descriptor queue in shared memory and
+// streams its input planes by TMA into a ring of stages. The ring is not
+// drained between items: the producer runs ahead into the next item's planes
+// while the consumers finish the current one, and consumer warps never meet
+// at a CTA-wide barrier, so a CTA moves from item to item without a bubble.
+// Because the list is ordered by step, every dependency of an item was taken
+// before the item itself and the earliest unfinished item can always run:
+// the launch needs no co-residency guarantee and cannot deadlock.
+// Mode 1 (graph): one launch per step and kind (one item per CTA) over all
+// members still running, the sequence captured once in a CUDA graph.
 // Mode 2 / 3: the per-grid loop -- each member alone, one launch per step,
 // with the plain kernel (the reference's shape) or the tuned TMA kernel.
 //
-// Each item runs the same tile functions as the single-grid kernels (TMA
-// plane ring, warp-specialised), so every member's result is bit-identical to
-// running it alone. Members may also measure a convergence residual every
-// `check_every` steps (7-point: |u_{n+1}-u_n|^2 and |u_{n+1}|^2; Himeno: the
-// sum of ss^2) and stop early: tiles write FP64 partials, and the CTA that
-// completes the last tile of a step combines them in tile order, decides, and
-// only then releases the member's next step, so the decision is deterministic.
+// Items run the same tile arithmetic as the single-grid kernels, so every
+// member's result is bit-identical to running it alone. Members may also
+// measure a convergence residual every `check_every` steps (7-point:
+// |u_{n+1}-u_n|^2 and |u_{n+1}|^2; Himeno: the sum of ss^2) and stop early:
+// each consumer warp writes an FP64 partial per item, and the warp that
+// completes the last unit of a step combines the partials in index order,
+// decides, and only then releases the member's next step, so the decision is
+// deterministic and independent of the rest of the batch.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -40,11 +45,41 @@
 
 namespace psb {
 
-// Batched items run 128 consumer threads (tile shape per member) and one
-// producer warp.
+// Batched items run 128 consumer threads (4 warps; tile shape per member)
+// and one producer warp.
 constexpr int kBConsumers = 128;
+constexpr int kBWarps = kBConsumers / 32;
 constexpr int kBThreads = kBConsumers + 32;
 constexpr int kBStages = 6;
+
+// Tile shapes of batched items: 128 consumer threads as 16 x 8, 32 x 4 or
+// 8 x 16 (x threads of 4 floats each x rows); kind_stage_bytes lists them
+// too. Ties go to the earlier shape.
+constexpr int kBShapes[3][2] = {{16, 8}, {32, 4}, {8, 16}};
+
+__host__ __device__ constexpr int stage_bytes_of(int tx_threads, int ty_threads,
+                                                 int rows_per_thread) {
+  return ((tx_threads * 4 + 8) * (ty_threads * rows_per_thread + 2) * 4 + 127) / 128 * 128;
+}
+
+__host__ __device__ constexpr int max3(int a, int b, int c) {
+  return a > b ? (a > c ? a : c) : (b > c ? b : c);
+}
+
+// One ring stride per kernel kind (the largest stage of its shapes): the
+// planes of differently shaped tiles follow each other through one ring.
+__host__ __device__ constexpr int kind_stage_bytes(int group) {
+  return max3(stage_bytes_of(16, 8, group == 0 ? kVY : 1),
+              stage_bytes_of(32, 4, group == 0 ? kVY : 1),
+              stage_bytes_of(8, 16, group == 0 ? kVY : 1));
+}
+
+// Shared memory of the batched kernel (bytes from the 128-aligned base):
+// ring barriers full[32] at 0 and empty[32] at 256, item queue barriers at
+// 512 (qfull) and 544 (qempty), item descriptors (kQ x 112 bytes) at 576,
+// stages from 1024.
+constexpr int kQ = 4;  // item descriptors in flight between producer and consumers
+constexpr int kSmemRing = 1024;
 
 struct BMember {
   int kind;
@@ -55,6 +90,7 @@ struct BMember {
   int check_every;  // 0: no checks
   double tol2;      // squared relative tolerance
   const CUtensorMap *tmap[2];
+  const CUtensorMap *tcoef;  // Himeno: 12 maps (box TX x TY) of the coefficient fields
   GridView buf[2];
   Dom3 dom;
   C7<float> k7;
@@ -63,8 +99,8 @@ struct BMember {
   int64_t sy, sz;
   TmaGeom dg;
   HimenoGeom hg;
-  double *partials;  // [2][ntiles][2]
-  unsigned *done;    // (ntiles + 1) units per step
+  double *partials;  // [2][ntiles][kBWarps][2]
+  unsigned *done;    // (ntiles * kBWarps + 1) units per step
   int *stop;         // local steps completed when converged, or -1
   double *res;       // [0] a or gosa, [1] b, [2] gosa of the first check, [3] check count
 };
@@ -80,6 +116,17 @@ struct BatchDev {
   unsigned long long *cursor;
   int *err;
 };
+
+// An item handed from the producer thread to the consumer warps. Himeno
+// items carry their member's coefficient field origins, which the consumers
+// read from shared memory on every plane instead of holding 12 pointers in
+// registers.
+struct ItemDesc {
+  int m, s, t, flags;
+  const float *cf[12];
+};
+enum { kItemEnd = 1, kItemSkip = 2 };
+static_assert(576 + kQ * sizeof(ItemDesc) <= kSmemRing, "item descriptors overlap the ring");
 
 __device__ __forceinline__ int upper_index(const int64_t *a, int n, int64_t v) {
   // largest i in [0, n) with a[i] <= v (a non-decreasing, a[0] = 0)
@@ -104,224 +151,312 @@ __device__ __forceinline__ int ld_acquire_int(const int *p) {
   return v;
 }
 
-// Sum of two doubles per thread over the CTA in a fixed order (thread 0).
-__device__ void cta_sum2(double a, double b, double *scr, double *oa, double *ob) {
-  for (int o = 16; o > 0; o >>= 1) {
-    a += __shfl_down_sync(0xffffffffu, a, o);
-    b += __shfl_down_sync(0xffffffffu, b, o);
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  __syncthreads();
-  if (lane == 0) {
-    scr[2 * warp] = a;
-    scr[2 * warp + 1] = b;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double sa = 0, sb = 0;
-    for (int w = 0; w < nw; w++) {
-      sa += scr[2 * w];
-      sb += scr[2 * w + 1];
+__device__ __forceinline__ unsigned step_unit(const BMember &M) {
+  return (unsigned)M.ntiles * kBWarps + 1u;
+}
+
+// Output column and planes of item (m, s, t).
+struct ItemGeom {
+  int x0, y0, zb, nzl;
+};
+
+template <int GROUP>
+__device__ __forceinline__ ItemGeom item_geom(const BMember &M, int t) {
+  const int tiles_x = GROUP == 0 ? M.dg.tiles_x : M.hg.tiles_x;
+  const int tiles_y = GROUP == 0 ? M.dg.tiles_y : M.hg.tiles_y;
+  const int zchunk = GROUP == 0 ? M.dg.zchunk : M.hg.zchunk;
+  const int tx_threads = GROUP == 0 ? M.dg.tx_threads : M.hg.tx_threads;
+  const int ty_threads = GROUP == 0 ? M.dg.ty_threads : M.hg.ty_threads;
+  const int x_base = GROUP == 0 ? M.dg.x_base : M.hg.x_base;
+  const int TX = tx_threads * 4, TY = ty_threads * (GROUP == 0 ? kVY : 1);
+  const int tile_x = t % tiles_x;
+  const int rest = t / tiles_x;
+  const int tile_y = rest % tiles_y;
+  const int zc = rest / tiles_y;
+  ItemGeom g;
+  g.x0 = x_base + tile_x * TX;
+  g.y0 = M.dom.lo[1] + tile_y * TY;
+  g.zb = M.dom.lo[2] + zc * zchunk;
+  g.nzl = min(g.zb + zchunk, M.dom.hi[2]) - g.zb;
+  return g;
+}
+
+// Producer thread: takes items (from the shared cursor, or item `blockIdx.x`
+// of `step` when step >= 0), waits until the item's member has completed
+// its previous step, hands the item to the consumers through the descriptor
+// queue and streams its input planes into the ring. It runs ahead of the
+// consumers by up to the ring's depth, across item boundaries.
+template <int GROUP>
+__device__ void batch_produce(const BatchDev &B, int step, const Ring &R, uint64_t *qfull,
+                              uint64_t *qempty, ItemDesc *desc) {
+  RingPos pos{0, 0};
+  bool ok = true;
+  for (uint32_t nq = 0;; nq++) {
+    long long item;
+    if (step >= 0)
+      item = nq == 0 ? (long long)B.step_offset[step] + blockIdx.x : (long long)B.total_items;
+    else
+      item = (long long)atomicAdd(B.cursor, 1ull);
+    int m = 0, s = 0, t = 0, flags = 0;
+    const BMember *M = nullptr;
+    if (item >= B.total_items || ld_acquire_int(B.err) != 0) {
+      flags = kItemEnd;
+    } else {
+      s = upper_index(B.step_offset, B.max_steps + 1, item);
+      const int64_t local = item - B.step_offset[s];
+      const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
+      m = B.order[k];
+      t = (int)(local - B.tile_prefix[k]);
+      M = &B.members[m];
+      // Every tile of step s-1 of this member, and its convergence decision.
+      const unsigned need = (unsigned)s * step_unit(*M);
+      if (ld_acquire(M->done) < need) {
+        const long long t0 = clock64();
+        unsigned sleep = 32;
+        while (ld_acquire(M->done) < need) {
+          if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) {
+            ok = false;
+            break;
+          }
+          __nanosleep(sleep);
+          if (sleep < 2048) sleep <<= 1;
+        }
+      }
+      if (!ok) {
+        flags = kItemEnd;
+      } else {
+        const int st = ld_acquire_int(M->stop);
+        if (st >= 0 && s >= st) flags = kItemSkip;
+      }
     }
-    *oa = sa;
-    *ob = sb;
+    const int q = nq % kQ;
+    if (nq >= kQ && !mbar_wait_bounded(&qempty[q], ((nq / kQ) - 1) & 1)) {
+      ok = false;
+      break;  // the consumers are stuck; their own bounded waits end them
+    }
+    desc[q].m = m;
+    desc[q].s = s;
+    desc[q].t = t;
+    desc[q].flags = flags;
+    if (GROUP == 1 && !(flags & (kItemEnd | kItemSkip)))
+      for (int i = 0; i < 12; i++) desc[q].cf[i] = M->cf.f[i];
+    mbar_arrive(&qfull[q]);  // release: the descriptor is visible to the consumers
+    if (flags & kItemEnd) break;
+    if (flags & kItemSkip) continue;
+    // The step's inputs were written by generic stores of other CTAs and
+    // acquired above; order that before the async-proxy (TMA) reads.
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    const int par = (M->step0 + s) & 1;
+    const ItemGeom g = item_geom<GROUP>(*M, t);
+    const int bx = GROUP == 0 ? M->dg.bx : M->hg.bx;
+    const int by = GROUP == 0 ? M->dg.by : M->hg.by;
+    const int ax0 = GROUP == 0 ? M->dg.ax0 : M->hg.ax0;
+    const int ay0 = GROUP == 0 ? M->dg.ay0 : M->hg.ay0;
+    const int az0 = GROUP == 0 ? M->dg.az0 : M->hg.az0;
+    if (GROUP == 0) {
+      if (!ring_produce(R, pos, M->tmap[par], (uint32_t)(bx * by * 4), g.x0 - 4 + ax0,
+                        g.y0 - 1 + ay0, g.zb - 1 + az0, g.nzl + 2)) {
+        ok = false;
+        break;
+      }
+    } else {
+      // Himeno: with each plane of p, bring the twelve coefficient planes of
+      // the same z into L2. The consumers load them one plane at a time
+      // (registers hold one plane's coefficients); coming from L2 instead of
+      // DRAM their latency no longer limits the sweep.
+      for (int j = 0; j < g.nzl + 2 && ok; j++) {
+        ok = ring_produce(R, pos, M->tmap[par], (uint32_t)(bx * by * 4), g.x0 - 4 + ax0,
+                          g.y0 - 1 + ay0, g.zb - 1 + j + az0, 1);
+        const int z = g.zb - 1 + j;
+        if (ok && z >= g.zb && z < g.zb + g.nzl)
+          for (int f = 0; f < 12; f++)
+            tma_prefetch_l2_3d(M->tcoef + f, g.x0 + ax0, g.y0 + ay0, z + az0);
+      }
+      if (!ok) break;
+    }
+  }
+  if (!ok) {
+    atomicExch(B.err, 1);
+    ring_drain(R, pos);
   }
 }
 
-// One item: tile t of local step s of member m. All threads of the CTA call
-// it. Returns false if a bounded wait gave up.
+// Completion of an item by one consumer warp: its FP64 residual partial
+// (when the step is checked), then one unit of the member's step counter.
+// The warp that completes the step's last unit combines the partials in
+// index order (deterministic: the same whatever else is in the batch),
+// decides convergence, and only then releases the member's next step.
 template <int GROUP>
-__device__ __forceinline__ bool batch_item(const BMember &M, int s, int t, unsigned char *smem,
-                                           int *err) {
+__device__ __forceinline__ void item_done(const BMember &M, int s, int t, int warp, int lane,
+                                          bool check, bool contrib, double a, double b) {
   const int par = (M.step0 + s) & 1;
   const int gstep = M.step0 + s;
-  const bool check = M.check_every > 0 &&
-                     ((gstep + 1) % M.check_every == 0 || (M.kind == BK_HIMENO && gstep == 0));
-  __shared__ int skip_s;
-  if (threadIdx.x == 0) {
-    const int st = ld_acquire_int(M.stop);
-    skip_s = st >= 0 && s >= st;
-  }
-  __syncthreads();
-  const bool skip = skip_s;
-  int tt = t;
-  const int tile_x = tt % M.tiles_x;
-  tt /= M.tiles_x;
-  const int tile_y = tt % M.tiles_y;
-  const int zc = tt / M.tiles_y;
-  double a = 0, b = 0;
-  bool bad = false;
-  if (!skip) {
-    if (threadIdx.x == kBConsumers)  // producer: order generic acquire before TMA reads
-      asm volatile("fence.proxy.async.global;" ::: "memory");
-    if constexpr (GROUP == 1) {
-      double g = 0;
-      himeno_tile(M.tmap[par], (float *)M.buf[par ^ 1].origin, M.cf, M.sy, M.sz, M.dom, M.omega,
-                  M.hg, tile_x, tile_y, zc, err, smem, &g, &bad);
-      a = g;
-    } else {
-      TileAcc acc{0, 0};
-      const int images = M.kind == BK_DIFF7P;
-      if (M.kind == BK_DIFF7P) {
-        if (check)
-          diff7_tile<float, true, true>(M.tmap[par], M.buf[par ^ 1], M.n[0], M.n[1], M.n[2], M.dom,
-                                        M.k7, M.dg, tile_x, tile_y, zc, images, err, smem, &acc);
-        else
-          diff7_tile<float, true, false>(M.tmap[par], M.buf[par ^ 1], M.n[0], M.n[1], M.n[2],
-                                         M.dom, M.k7, M.dg, tile_x, tile_y, zc, images, err, smem,
-                                         nullptr);
-      } else {
-        if (check)
-          diff7_tile<float, false, true>(M.tmap[par], M.buf[par ^ 1], M.n[0], M.n[1], M.n[2],
-                                         M.dom, M.k7, M.dg, tile_x, tile_y, zc, 0, err, smem,
-                                         &acc);
-        else
-          diff7_tile<float, false, false>(M.tmap[par], M.buf[par ^ 1], M.n[0], M.n[1], M.n[2],
-                                          M.dom, M.k7, M.dg, tile_x, tile_y, zc, 0, err, smem,
-                                          nullptr);
-      }
-      a = acc.a;
-      b = acc.b;
+  double *P = M.partials + (int64_t)par * M.ntiles * kBWarps * 2;
+  if (contrib) {
+    for (int o = 16; o > 0; o >>= 1) {
+      a += __shfl_down_sync(0xffffffffu, a, o);
+      b += __shfl_down_sync(0xffffffffu, b, o);
+    }
+    if (lane == 0) {
+      P[((int64_t)t * kBWarps + warp) * 2] = a;
+      P[((int64_t)t * kBWarps + warp) * 2 + 1] = b;
     }
   }
-  // Every thread is past the tile (the ring is idle): reuse the ring area.
-  double *scr = reinterpret_cast<double *>(smem + 512);
-  if (check && !skip) {
-    double sa, sb;
-    cta_sum2(a, b, scr, &sa, &sb);
-    if (threadIdx.x == 0) {
-      M.partials[(par * M.ntiles + t) * 2] = sa;
-      M.partials[(par * M.ntiles + t) * 2 + 1] = sb;
-    }
-  }
-  __shared__ int bad_any;
-  if (threadIdx.x == 0) bad_any = 0;
-  __syncthreads();
-  if (bad) atomicExch(&bad_any, 1);
-  __syncthreads();
-  if (threadIdx.x == 0 && !bad_any) {
+  __syncwarp();
+  unsigned last = 0;
+  if (lane == 0) {
     __threadfence();
-    const unsigned unit = (unsigned)M.ntiles + 1;
     const unsigned old = atomicAdd(M.done, 1u);
-    if (old + 1 == (unsigned)s * unit + (unsigned)M.ntiles) {
-      // Last tile of this step: decide convergence, then release the step.
-      if (check && !skip) {
-        __threadfence();
-        double sa = 0, sb = 0;
-        for (int i = 0; i < M.ntiles; i++) {
-          sa += __ldcg(&M.partials[(par * M.ntiles + i) * 2]);
-          sb += __ldcg(&M.partials[(par * M.ntiles + i) * 2 + 1]);
-        }
-        bool conv;
-        if (M.kind == BK_HIMENO) {
-          if (gstep == 0) M.res[2] = sa;
-          const double g0 = gstep == 0 ? sa : __ldcg(&M.res[2]);
-          conv = sa <= M.tol2 * g0;
-          M.res[1] = g0;
-        } else {
-          conv = sa <= M.tol2 * sb;
-          M.res[1] = sb;
-        }
-        M.res[0] = sa;
-        M.res[3] = (double)(gstep + 1);
-        if (conv && M.tol2 > 0) atomicExch(M.stop, s + 1);
+    last = old + 1 == (unsigned)s * step_unit(M) + (unsigned)M.ntiles * kBWarps;
+  }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return;
+  if (check && contrib) {
+    __threadfence();
+    const int n = M.ntiles * kBWarps;
+    double sa = 0, sb = 0;
+    for (int i = lane; i < n; i += 32) {
+      sa += __ldcg(&P[2 * i]);
+      sb += __ldcg(&P[2 * i + 1]);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      sa += __shfl_down_sync(0xffffffffu, sa, o);
+      sb += __shfl_down_sync(0xffffffffu, sb, o);
+    }
+    if (lane == 0) {
+      bool conv;
+      if (GROUP == 1) {
+        if (gstep == 0) M.res[2] = sa;
+        const double g0 = gstep == 0 ? sa : __ldcg(&M.res[2]);
+        conv = sa <= M.tol2 * g0;
+        M.res[1] = g0;
+      } else {
+        conv = sa <= M.tol2 * sb;
+        M.res[1] = sb;
       }
-      __threadfence();
-      atomicAdd(M.done, 1u);
+      M.res[0] = sa;
+      M.res[3] = (double)(gstep + 1);
+      if (conv && M.tol2 > 0) atomicExch(M.stop, s + 1);
     }
   }
-  return !bad_any;
+  if (lane == 0) {
+    __threadfence();
+    atomicAdd(M.done, 1u);
+  }
+}
+
+// Consumer warps: take item after item from the descriptor queue and run
+// the tile's computation from the ring. A descriptor slot is released when
+// the item is done (Himeno items read their coefficient origins from it).
+template <int GROUP>
+__device__ void batch_consume(const BatchDev &B, const Ring &R, uint64_t *qfull, uint64_t *qempty,
+                              const ItemDesc *desc) {
+  RingPos pos{0, 0};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (uint32_t nq = 0;; nq++) {
+    const int q = nq % kQ;
+    const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(&qfull[q], (nq / kQ) & 1));
+    if (!got) {
+      if (lane == 0) atomicExch(B.err, 1);
+      return;
+    }
+    const int dm = desc[q].m, ds = desc[q].s, dt = desc[q].t, dflags = desc[q].flags;
+    if (dflags & kItemEnd) {
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&qempty[q]);
+      return;
+    }
+    const BMember &M = B.members[dm];
+    const bool skip = (dflags & kItemSkip) != 0;
+    const int par = (M.step0 + ds) & 1;
+    const int gstep = M.step0 + ds;
+    const bool check = M.check_every > 0 &&
+                       ((gstep + 1) % M.check_every == 0 || (GROUP == 1 && gstep == 0));
+    double a = 0, b = 0;
+    if (!skip) {
+      const ItemGeom g = item_geom<GROUP>(M, dt);
+      bool ok;
+      if constexpr (GROUP == 1) {
+        const float *const *cf = desc[q].cf;
+        ok = himeno_consume(R, pos, (float *)M.buf[par ^ 1].origin,
+                            [&](int i) { return cf[i]; }, M.sy, M.sz, M.dom, M.omega, M.hg,
+                            g.x0, g.y0, g.zb, g.nzl, &a);
+      } else {
+        TileAcc acc{0, 0};
+        const GridView out = M.buf[par ^ 1];
+        if (M.kind == BK_DIFF7P) {
+          ok = check ? diff7_consume<float, true, true>(R, pos, out, M.n[0], M.n[1], M.n[2], M.dom,
+                                                        M.k7, M.dg, g.x0, g.y0, g.zb, g.nzl, 1,
+                                                        &acc)
+                     : diff7_consume<float, true, false>(R, pos, out, M.n[0], M.n[1], M.n[2],
+                                                         M.dom, M.k7, M.dg, g.x0, g.y0, g.zb,
+                                                         g.nzl, 1, nullptr);
+        } else {
+          ok = check ? diff7_consume<float, false, true>(R, pos, out, M.n[0], M.n[1], M.n[2],
+                                                         M.dom, M.k7, M.dg, g.x0, g.y0, g.zb,
+                                                         g.nzl, 0, &acc)
+                     : diff7_consume<float, false, false>(R, pos, out, M.n[0], M.n[1], M.n[2],
+                                                          M.dom, M.k7, M.dg, g.x0, g.y0, g.zb,
+                                                          g.nzl, 0, nullptr);
+        }
+        a = acc.a;
+        b = acc.b;
+      }
+      if (!ok) {
+        if (lane == 0) atomicExch(B.err, 1);
+        return;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&qempty[q]);
+    item_done<GROUP>(M, ds, dt, warp, lane, check, check && !skip, a, b);
+  }
 }
 
 __device__ __forceinline__ unsigned char *aligned_smem(unsigned char *raw) {
   return raw + ((128 - (smem_u32(raw) & 127)) & 127);
 }
 
-// Retire the ring's barriers between items (they are initialised again by
-// the next tile).
-__device__ __forceinline__ void inval_barriers(unsigned char *smem) {
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-  for (int i = 0; i < kBStages; i++) {
-    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[i])) : "memory");
-    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(&full[32 + i])) : "memory");
-  }
-}
-
-// Mode 0: one persistent launch per stencil kind over that kind's work list
-// (a kernel per kind keeps each at the register budget of its single-grid
-// kernel; the two lists are independent).
-// Diffusion items (four instantiations of the tile: clamped/periodic, with or
-// without residual terms) get the register budget of 3 CTAs per SM, Himeno
-// items that of 4.
+// The batched kernel of one stencil kind. step < 0: persistent -- each CTA
+// takes items from the kind's work list until it is exhausted (mode 0).
+// step >= 0: one item per CTA, item blockIdx.x of that step (mode 1, one
+// launch per step). Both kinds fit the register budget of 3 CTAs per SM
+// without spills.
+#ifndef PSB_BATCH_HIMENO_CTAS
+#define PSB_BATCH_HIMENO_CTAS 3
+#endif
 template <int GROUP>
-__global__ void __launch_bounds__(kBThreads, GROUP == 0 ? 3 : 4) k_batch_persistent(BatchDev B) {
+__global__ void __launch_bounds__(kBThreads, GROUP == 0 ? 3 : PSB_BATCH_HIMENO_CTAS)
+    k_batch(BatchDev B, int step) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char *smem = aligned_smem(smem_raw);
-  __shared__ long long item_s;
-  __shared__ int m_s, s_s, t_s, stop_s;
-  if (threadIdx.x == 0) stop_s = 0;
-  for (;;) {
-    if (threadIdx.x == 0) {
-      const long long item = (long long)atomicAdd(B.cursor, 1ull);
-      item_s = item;
-      if (item < B.total_items) {
-        const int s = upper_index(B.step_offset, B.max_steps + 1, item);
-        const int64_t local = item - B.step_offset[s];
-        const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
-        const int m = B.order[k];
-        m_s = m;
-        s_s = s;
-        t_s = (int)(local - B.tile_prefix[k]);
-        // Wait for every tile of step s-1 of this member (bounded).
-        const BMember &M = B.members[m];
-        const unsigned need = (unsigned)s * ((unsigned)M.ntiles + 1);
-        if (ld_acquire(M.done) < need) {
-          long long t0 = clock64();
-          unsigned sleep = 32;
-          while (ld_acquire(M.done) < need) {
-            if (ld_acquire_int((const int *)B.err) != 0 || clock64() - t0 > 4000000000LL) {
-              atomicExch(B.err, 1);
-              stop_s = 1;
-              break;
-            }
-            __nanosleep(sleep);
-            if (sleep < 2048) sleep <<= 1;
-          }
-        }
-      }
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  uint64_t *qfull = bars + 64, *qempty = bars + 68;
+  ItemDesc *desc = reinterpret_cast<ItemDesc *>(smem + 576);
+  const Ring R{bars, bars + 32, smem + kSmemRing, kBStages, kind_stage_bytes(GROUP)};
+  if (threadIdx.x == 0) {
+    ring_init(R, kBWarps);
+    for (int q = 0; q < kQ; q++) {
+      mbar_init(&qfull[q], 1);
+      mbar_init(&qempty[q], kBWarps);
     }
-    __syncthreads();
-    if (item_s >= B.total_items || stop_s) break;
-    if (!batch_item<GROUP>(B.members[m_s], s_s, t_s, smem, B.err)) {
-      __syncthreads();
-      break;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) inval_barriers(smem);
-    __syncthreads();
+    mbar_fence_init();
   }
+  __syncthreads();
+  if (threadIdx.x >= kBConsumers) {
+    if (threadIdx.x == kBConsumers) batch_produce<GROUP>(B, step, R, qfull, qempty, desc);
+    return;
+  }
+  batch_consume<GROUP>(B, R, qfull, qempty, desc);
 }
-
-// Mode 1: one launch per step and kind; blockIdx.x enumerates the tiles of
-// that kind's members still running at step s.
-template <int GROUP>
-__global__ void __launch_bounds__(kBThreads, GROUP == 0 ? 3 : 4) k_batch_step(BatchDev B, int s) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  unsigned char *smem = aligned_smem(smem_raw);
-  const int64_t local = blockIdx.x;
-  const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
-  const int m = B.order[k];
-  const int t = (int)(local - B.tile_prefix[k]);
-  batch_item<GROUP>(B.members[m], s, t, smem, B.err);
-}
-
-// ---------------------------------------------------------------------------
-// Host side
-// ---------------------------------------------------------------------------
 
 }  // namespace psb
 
 using namespace psb;
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
 
 // Work list of one kernel kind (group 0: diffusion members, 1: Himeno).
 struct BatchGroup {
@@ -410,12 +545,9 @@ static psb_status dev_reserve(T **p, size_t *cap, size_t bytes) {
   return PSB_OK;
 }
 
-// Tile shapes of batched items: 128 consumer threads as 8 x 16, 16 x 8 or
-// 32 x 4 (x threads of 4 floats each x rows); each member takes the shape
-// with the fewest tiles over its x-y extent (then the fewest box elements),
-// so small and narrow members waste few threads on partial tiles.
-constexpr int kBShapes[3][2] = {{8, 16}, {16, 8}, {32, 4}};
-
+// Each member takes the tile shape with the fewest tiles over its x-y
+// extent (then the fewest box elements), so small and narrow members waste
+// few threads on partial tiles.
 static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int *ty_threads) {
   int64_t best_tiles = -1, best_box = 0;
   for (const auto &sh : kBShapes) {
@@ -429,10 +561,6 @@ static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int
       *ty_threads = sh[1];
     }
   }
-}
-
-static int stage_bytes_of(int tx_threads, int ty_threads, int rows_per_thread) {
-  return ((tx_threads * 4 + 8) * (ty_threads * rows_per_thread + 2) * 4 + 127) / 128 * 128;
 }
 
 static TmaGeom batch_dgeom(const GridImpl *g) {
@@ -449,7 +577,7 @@ static TmaGeom batch_dgeom(const GridImpl *g) {
   geo.tiles_y = (g->pub.dim[1] + TY - 1) / TY;
   geo.zchunk = 64;
   geo.stages = kBStages;
-  geo.stage_bytes = stage_bytes_of(geo.tx_threads, geo.ty_threads, kVY);
+  geo.stage_bytes = kind_stage_bytes(0);
   return geo;
 }
 
@@ -468,16 +596,13 @@ static HimenoGeom batch_hgeom(const GridImpl *g) {
   geo.tiles_y = (g->pub.dim[1] - 2 + TY - 1) / TY;
   geo.zchunk = 64;
   geo.stages = kBStages;
-  geo.stage_bytes = stage_bytes_of(geo.tx_threads, geo.ty_threads, 1);
+  geo.stage_bytes = kind_stage_bytes(1);
   geo.nx = g->pub.dim[0];
   return geo;
 }
 
 static size_t batch_smem(int group) {
-  int stage = 0;
-  for (const auto &sh : kBShapes)
-    stage = std::max(stage, stage_bytes_of(sh[0], sh[1], group == 0 ? kVY : 1));
-  return group == 0 ? 128 + 512 + (size_t)kBStages * stage : 128 + 768 + (size_t)kBStages * stage;
+  return 128 + kSmemRing + (size_t)kBStages * kind_stage_bytes(group);
 }
 
 // Build the device work lists and member descriptors for one launch in which
@@ -488,6 +613,7 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
   batch_invalidate(b);
   b->members.assign(n, BMember());
   std::vector<CUtensorMap> tmaps(2 * std::max(1, n));
+  std::vector<int> coef_map(n, -1);  // index of a Himeno member's 12 coefficient maps
   int64_t partial_slots = 0;
   for (int i = 0; i < n; i++) {
     const BatchMemberHost &h = b->hm[i];
@@ -518,6 +644,12 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
       for (int k = 0; k < 12; k++) M.cf.f[k] = (const float *)h.grids[2 + k]->view().origin;
       PSB_CHECK(get_tmap(g0, M.hg.bx, M.hg.by, &a));
       PSB_CHECK(get_tmap(g1, M.hg.bx, M.hg.by, &c));
+      coef_map[i] = (int)tmaps.size();
+      for (int k = 0; k < 12; k++) {
+        const CUtensorMap *cm = nullptr;
+        PSB_CHECK(get_tmap(h.grids[2 + k], M.hg.tx_threads * 4, M.hg.ty_threads, &cm));
+        tmaps.push_back(*cm);
+      }
     } else {
       M.dg = batch_dgeom(g0);
       for (int k = 0; k < 3; k++) {
@@ -540,7 +672,7 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     tmaps[2 * i] = *a;
     tmaps[2 * i + 1] = *c;
     M.ntiles = M.tiles_x * M.tiles_y * M.nzc;
-    partial_slots += 4 * (int64_t)M.ntiles;
+    partial_slots += 2 * 2 * kBWarps * (int64_t)M.ntiles;
   }
   PSB_CHECK(dev_reserve(&b->d_tmaps, &b->cap_tmaps, sizeof(CUtensorMap) * tmaps.size()));
   PSB_TRY(cudaMemcpy(b->d_tmaps, tmaps.data(), sizeof(CUtensorMap) * tmaps.size(),
@@ -559,8 +691,9 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     BMember &M = b->members[i];
     M.tmap[0] = b->d_tmaps + 2 * i;
     M.tmap[1] = b->d_tmaps + 2 * i + 1;
+    M.tcoef = coef_map[i] >= 0 ? b->d_tmaps + coef_map[i] : nullptr;
     M.partials = b->d_partials + off;
-    off += 4 * (int64_t)M.ntiles;
+    off += 2 * 2 * kBWarps * (int64_t)M.ntiles;
     M.done = b->d_done + i;
     M.stop = b->d_stop + i;
     M.res = b->d_res + 4 * i;
@@ -600,21 +733,15 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     if (!G.d_cursor) PSB_TRY(cudaMalloc(&G.d_cursor, sizeof(unsigned long long)));
     int per_sm = 0;
     if (gi == 0) {
-      PSB_TRY(cudaFuncSetAttribute(k_batch_persistent<0>,
-                                   cudaFuncAttributePreferredSharedMemoryCarveout,
+      PSB_TRY(cudaFuncSetAttribute(k_batch<0>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
-      PSB_TRY(cudaFuncSetAttribute(k_batch_step<0>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                   cudaSharedmemCarveoutMaxShared));
-      PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent<0>,
-                                                            kBThreads, batch_smem(0)));
+      PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<0>, kBThreads,
+                                                            batch_smem(0)));
     } else {
-      PSB_TRY(cudaFuncSetAttribute(k_batch_persistent<1>,
-                                   cudaFuncAttributePreferredSharedMemoryCarveout,
+      PSB_TRY(cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
-      PSB_TRY(cudaFuncSetAttribute(k_batch_step<1>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                   cudaSharedmemCarveoutMaxShared));
-      PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_persistent<1>,
-                                                            kBThreads, batch_smem(1)));
+      PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<1>, kBThreads,
+                                                            batch_smem(1)));
     }
     G.blocks_persistent = std::max(1, per_sm) * r.sm_count;
   }
@@ -664,12 +791,12 @@ psb_status batch_launch_persistent(psb_batch *b, cudaStream_t s, int64_t *launch
     if (!G.total_items) continue;
     const int blocks = (int)std::min<int64_t>(G.blocks_persistent, G.total_items);
     if (gi == 0)
-      k_batch_persistent<0><<<blocks, kBThreads, batch_smem(0), s>>>(batch_dev(b, 0));
+      k_batch<0><<<blocks, kBThreads, batch_smem(0), s>>>(batch_dev(b, 0), -1);
     else
-      k_batch_persistent<1><<<blocks, kBThreads, batch_smem(1), s>>>(batch_dev(b, 1));
+      k_batch<1><<<blocks, kBThreads, batch_smem(1), s>>>(batch_dev(b, 1), -1);
     (*launches)++;
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e, "k_batch_persistent");
+    if (e != cudaSuccess) return cuda_status(e, "k_batch");
   }
   return PSB_OK;
 }
@@ -697,9 +824,9 @@ psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches) {
         while (active > 0 && b->members[G.order[active - 1]].steps <= step) active--;
         const unsigned blocks = (unsigned)G.tile_prefix[active];
         if (gi == 0)
-          k_batch_step<0><<<blocks, kBThreads, batch_smem(0), ss>>>(B, step);
+          k_batch<0><<<blocks, kBThreads, batch_smem(0), ss>>>(B, step);
         else
-          k_batch_step<1><<<blocks, kBThreads, batch_smem(1), ss>>>(B, step);
+          k_batch<1><<<blocks, kBThreads, batch_smem(1), ss>>>(B, step);
       }
     }
     cudaEventRecord(b->join, b->side);

@@ -154,6 +154,14 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
       : "memory");
 }
 
+// Bring one box of a tensor into L2 (no shared memory, no completion).
+__device__ __forceinline__ void tma_prefetch_l2_3d(const CUtensorMap *map, int x, int y, int z) {
+  asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
+
 __device__ __forceinline__ void tma_prefetch_desc(const CUtensorMap *map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }
@@ -173,6 +181,63 @@ __device__ __forceinline__ void store_face_images(T *origin, int64_t sy, int64_t
   if (y == n[1] - 1) origin[c - n[1] * sy] = v;
   if (z == 0) origin[c + n[2] * sz] = v;
   if (z == n[2] - 1) origin[c - n[2] * sz] = v;
+}
+
+// A ring of S shared-memory stages filled by TMA (one producer thread) and
+// drained by consumer warps. The position (slot, wrap count) is an explicit
+// value, so one ring can carry the planes of many tiles back to back.
+struct Ring {
+  uint64_t *full;       // S barriers, one producer arrival (+ the copy's bytes)
+  uint64_t *empty;      // S barriers, one arrival per consumer warp
+  unsigned char *base;  // stage 0
+  int S;
+  int stage_bytes;
+};
+
+struct RingPos {
+  int slot;
+  uint32_t round;  // times the ring wrapped before this position
+};
+
+__device__ __forceinline__ void ring_next(RingPos &p, int S) {
+  if (++p.slot == S) {
+    p.slot = 0;
+    p.round++;
+  }
+}
+
+__device__ __forceinline__ void ring_init(const Ring &R, int consumer_warps) {
+  for (int i = 0; i < R.S; i++) {
+    mbar_init(&R.full[i], 1);
+    mbar_init(&R.empty[i], consumer_warps);
+  }
+  mbar_fence_init();
+}
+
+// Producer: np planes, plane j from tensor coordinates (cx, cy, cz0 + j),
+// into the ring from position p on. False if a bounded wait gave up.
+__device__ __forceinline__ bool ring_produce(const Ring &R, RingPos &p, const CUtensorMap *tin,
+                                             uint32_t bytes, int cx, int cy, int cz0, int np) {
+  for (int j = 0; j < np; j++) {
+    if (p.round > 0 && !mbar_wait_bounded(&R.empty[p.slot], (p.round - 1) & 1)) return false;
+    mbar_arrive_expect_tx(&R.full[p.slot], bytes);
+    tma_load_3d(R.base + p.slot * R.stage_bytes, tin, &R.full[p.slot], cx, cy, cz0 + j);
+    ring_next(p, R.S);
+  }
+  return true;
+}
+
+// After a producer gave up: wait (bounded) until the last copy issued into
+// each slot before position `end` has landed, so none is in flight when the
+// CTA leaves.
+__device__ __forceinline__ void ring_drain(const Ring &R, RingPos end) {
+  for (int i = 0; i < R.S; i++) {
+    if (end.round == 0 && i >= end.slot) continue;
+    const uint32_t r = i < end.slot ? end.round : end.round - 1;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(&R.full[i], r & 1) && clock64() - t0 < 200000000LL) {
+    }
+  }
 }
 
 }  // namespace psb

@@ -120,16 +120,21 @@ __device__ __forceinline__ Vec16<T> diff7_row(const K7<T> &k, const Vec16<T> &c,
 }
 
 // --------------------------------------------------------------------------
-// TMA z-streaming kernel, warp-specialised
+// TMA z-streaming, warp-specialised
 //
-// One producer warp streams input planes (box (TX+2V) x (TY+2) x 1) into a
+// One producer thread streams input planes (box (TX+2V) x (TY+2) x 1) into a
 // ring of S shared-memory stages with TMA; `full[s]` completes when a plane
 // has landed, `empty[s]` when every consumer warp has finished with it.
 // Consumer warps never meet at a CTA-wide barrier: each waits on the plane
-// it needs and releases the one it is done with. Each consumer thread owns
-// V consecutive x points (16 bytes) of VY rows; z neighbours stay in
+// it needs and releases it when done. Each consumer thread owns V
+// consecutive x points (16 bytes) of VY rows; z neighbours stay in
 // registers. Faces are resolved with selects only on threads/planes that
 // touch a face; all other points take a select-free path.
+//
+// The ring position is an explicit value (Ring, RingPos in device.cuh), so
+// one ring can carry the planes of many tiles back to back: the single-grid
+// kernels run one tile per CTA, the batched persistent kernel streams tile
+// after tile through the same ring without draining it.
 // --------------------------------------------------------------------------
 struct TmaGeom {
   int ax0, ay0, az0;      // tensor-map coordinates of logical (0,0,0)
@@ -151,81 +156,22 @@ struct TileAcc {
   double a, b;
 };
 
-// One tile: the (TX x TY) column at (tile_x, tile_y) of the domain over z
-// chunk zc, read through tensor map `tin`, written to `out`. Called by every
-// thread of the CTA; `smem` is the CTA's 128-byte aligned dynamic shared
-// memory (barriers + ring). With ACC the consumer threads add their points'
-// convergence terms to *acc.
+// Consumer warps, one tile: planes zb-1 .. zb+nzl of the (TX x TY) column
+// at (x0, y0), starting at ring position p (advanced past all nzl + 2 planes,
+// every one of which is released). Output rows go to `out`; with PERIODIC
+// and `images`, every written face point also stores its image in the halo
+// (depth 1, one per face it lies on), which keeps the resident halo current
+// for the next periodic read. With ACC the convergence terms are added to
+// *acc. Returns false (warp-uniformly) if a bounded wait gave up.
 template <typename T, bool PERIODIC, bool ACC>
-__device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridView out, int nx,
-                                           int ny, int nz, const Dom3 d, const C7<T> k,
-                                           const TmaGeom geo, int tile_x, int tile_y, int zc,
-                                           int images, int *err, unsigned char *smem,
-                                           TileAcc *acc) {
-  // The descriptors arrive by value so that they live in registers: callers
-  // may pass fields of a table in global memory, and references into it
-  // would be reloaded after every store of the hot loop.
+__device__ __forceinline__ bool diff7_consume(const Ring &R, RingPos &p, const GridView out,
+                                              int nx, int ny, int nz, const Dom3 d,
+                                              const C7<T> k, const TmaGeom geo, int x0, int y0,
+                                              int zb, int nzl, int images, TileAcc *acc) {
   constexpr int V = 16 / sizeof(T);
   constexpr int VY = kVY;
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-  uint64_t *empty = full + 32;
-  unsigned char *ring = smem + 512;
-
-  const int S = geo.stages;
-  const int nct = geo.tx_threads * geo.ty_threads;  // consumer threads
-  const int ncw = nct >> 5;                          // consumer warps
-  const int TX = geo.tx_threads * V, TY = geo.ty_threads * VY;
-  const int x0 = geo.x_base + tile_x * TX;
-  const int y0 = d.lo[1] + tile_y * TY;
-  const int zb = d.lo[2] + zc * geo.zchunk;
-  const int ze = min(zb + geo.zchunk, d.hi[2]);
-  const int nzl = ze - zb;  // output planes
-  const int np = nzl + 2;   // input planes zb-1 .. ze
+  const int S = R.S;
   const int tid = threadIdx.x;
-
-  if (tid == 0) {
-    for (int i = 0; i < S; i++) {
-      mbar_init(&full[i], 1);
-      mbar_init(&empty[i], ncw);
-    }
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  if (tid >= nct) {
-    // ---------------- producer warp ----------------
-    if (tid != nct) return;
-    tma_prefetch_desc(tin);
-    const uint32_t bytes = (uint32_t)(geo.bx * geo.by * sizeof(T));
-    int slot = 0, round = 0, issued = 0;
-    bool ok = true;
-    for (int j = 0; j < np; j++) {
-      if (round > 0 && !mbar_wait_bounded(&empty[slot], (round - 1) & 1)) {
-        ok = false;
-        break;
-      }
-      mbar_arrive_expect_tx(&full[slot], bytes);
-      tma_load_3d(ring + slot * geo.stage_bytes, tin, &full[slot], x0 - V + geo.ax0,
-                  y0 - 1 + geo.ay0, zb - 1 + j + geo.az0);
-      issued++;
-      if (++slot == S) {
-        slot = 0;
-        round++;
-      }
-    }
-    if (!ok) {
-      atomicExch(err, 1);
-      // Let the copies already issued land before the CTA can leave.
-      for (int j = 0; j < issued; j++) {
-        long long t0 = clock64();
-        while (!mbar_try_wait(&full[j % S], (j / S) & 1) && clock64() - t0 < 200000000LL) {
-        }
-      }
-    }
-    return;
-  }
-
-  // ---------------- consumer warps ----------------
   const int tx = tid % geo.tx_threads, ty = tid / geo.tx_threads;
   const int lane = tid & 31;
   const int BX = geo.bx;
@@ -248,50 +194,61 @@ __device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridVie
 #pragma unroll
   for (int r = 0; r < VY; r++) row_in[r] = yg0 + r >= d.lo[1] && yg0 + r < d.hi[1];
   const bool xvec = xg0 >= d.lo[0] && xg0 + V <= d.hi[0];
+  // Periodic x-face images of this thread's vector: x = 0 goes to x = nx,
+  // x = nx-1 to x = -1.
+  const int vlast = nx - 1 - xg0;  // element of the vector at x = nx-1, if 0 <= vlast < V
+  const bool img_x0 = PERIODIC && xg0 == 0 && d.lo[0] <= 0;
+  const bool img_x1 = PERIODIC && vlast >= 0 && vlast < V && nx - 1 >= d.lo[0] && nx - 1 < d.hi[0];
   const K7<T> kk = make_k7(k);
 
   // Every lane waits (the wait gives it visibility of the TMA data); the
   // outcome is made warp-uniform so a timeout never splits a warp.
-  auto wait_plane = [&](int slot, int round) -> bool {
-    bool ok = mbar_wait_bounded(&full[slot], round & 1);
+  auto wait_plane = [&](const RingPos &q) -> bool {
+    bool ok = mbar_wait_bounded(&R.full[q.slot], q.round & 1);
     return __all_sync(0xffffffffu, ok);
   };
   auto release = [&](int slot) {
     __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[slot]);
+    if (lane == 0) mbar_arrive(&R.empty[slot]);
   };
   auto plane_ptr = [&](int slot) -> const T * {
-    return reinterpret_cast<const T *>(ring + slot * geo.stage_bytes);
+    return reinterpret_cast<const T *>(R.base + slot * R.stage_bytes);
+  };
+  auto store_vec = [&](T *dst, const Vec16<T> &v) {
+    if (xvec) {
+      stg16(dst, v);
+    } else {
+#pragma unroll
+      for (int e = 0; e < V; e++)
+        if (xg0 + e >= d.lo[0] && xg0 + e < d.hi[0]) dst[e] = v.v[e];
+    }
   };
 
   T *o = (T *)out.origin;
   T *dst0 = o + (int64_t)xg0 + (int64_t)yg0 * out.sy + (int64_t)zb * out.sz;
-  int s_z = 1 % S;          // slot of the plane of z
-  int s_t = 1 % S, r_t = 0;  // slot / round of the plane of z+1 (advanced before use)
-  if (S == 1) r_t = 1;
+  RingPos pz = p;  // plane of z (after the prologue)
+  ring_next(pz, S);
+  RingPos pt = pz;  // plane of z+1 (advanced before use)
   int z = zb;
 
   // One z step: b = plane z-1 (registers), c = plane z (registers), t is
   // loaded from the plane of z+1. Returns false on a timeout.
   auto step = [&](Vec16<T>(&vb)[VY], Vec16<T>(&vc)[VY], Vec16<T>(&vt)[VY]) -> bool {
-    if (++s_t == S) {
-      s_t = 0;
-      r_t++;
-    }
-    if (!wait_plane(s_t, r_t)) return false;
-    const T *pz = plane_ptr(s_z);
-    const T *pt = plane_ptr(s_t);
+    ring_next(pt, S);
+    if (!wait_plane(pt)) return false;
+    const T *pzp = plane_ptr(pz.slot);
+    const T *ptp = plane_ptr(pt.slot);
 #pragma unroll
-    for (int r = 0; r < VY; r++) vt[r] = lds16(pt + rc0 + r * BX);
-    const Vec16<T> vn = lds16(pz + rc0 - BX);
-    const Vec16<T> vs = lds16(pz + rc0 + VY * BX);
+    for (int r = 0; r < VY; r++) vt[r] = lds16(ptp + rc0 + r * BX);
+    const Vec16<T> vn = lds16(pzp + rc0 - BX);
+    const Vec16<T> vs = lds16(pzp + rc0 + VY * BX);
     T wl[VY], er[VY];
 #pragma unroll
     for (int r = 0; r < VY; r++) {
-      wl[r] = pz[rc0 + r * BX - 1];
-      er[r] = pz[rc0 + r * BX + V];
+      wl[r] = pzp[rc0 + r * BX - 1];
+      er[r] = pzp[rc0 + r * BX + V];
     }
-    release(s_z);  // this warp is done with the plane of z
+    release(pz.slot);  // this warp is done with the plane of z
     const bool zedge = !PERIODIC && (z == 0 || z == nz - 1);
     Vec16<T> res[VY];
     if (!(yedge || zedge)) {
@@ -339,44 +296,39 @@ __device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridVie
     for (int r = 0; r < VY; r++) {
       if (!row_in[r]) continue;
       T *dst = dst0 + r * out.sy;
-      if (xvec) {
-        stg16(dst, res[r]);
-      } else {
-#pragma unroll
-        for (int v = 0; v < V; v++)
-          if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) dst[v] = res[r].v[v];
-      }
+      store_vec(dst, res[r]);
       if (PERIODIC && images) {
-        // Only threads on a face have images to write: x faces touch the
-        // first or last element of a vector, y/z faces whole rows/planes.
         const int y = yg0 + r;
-        const bool yz = y == 0 || y == out.n[1] - 1 || z == 0 || z == out.n[2] - 1;
-        if (yz || xg0 == 0 || xg0 + V - 1 >= out.n[0] - 1) {
+        if (img_x0) dst[nx] = res[r].v[0];
+        if (img_x1) {
 #pragma unroll
           for (int v = 0; v < V; v++)
-            if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0])
-              store_face_images(o, out.sy, out.sz, out.n, xg0 + v, y, z, res[r].v[v]);
+            if (v == vlast) dst[v - nx] = res[r].v[v];
         }
+        if (y == 0) store_vec(dst + (int64_t)ny * out.sy, res[r]);
+        if (y == ny - 1) store_vec(dst - (int64_t)ny * out.sy, res[r]);
+        if (z == 0) store_vec(dst + (int64_t)nz * out.sz, res[r]);
+        if (z == nz - 1) store_vec(dst - (int64_t)nz * out.sz, res[r]);
       }
     }
     dst0 += out.sz;
-    s_z = s_t;
+    pz = pt;
     z++;
     return true;
   };
 
   // Prologue: planes 0 (z-1) and 1 (z).
   Vec16<T> A[VY], B[VY], C[VY];
-  bool bad = !wait_plane(0, 0);
-  bad = bad || !wait_plane(1 % S, 1 / S);
+  bool bad = !wait_plane(p);
+  bad = bad || !wait_plane(pz);
   if (!bad) {
-    const T *p0 = plane_ptr(0), *p1 = plane_ptr(1 % S);
+    const T *p0 = plane_ptr(p.slot), *p1 = plane_ptr(pz.slot);
 #pragma unroll
     for (int r = 0; r < VY; r++) {
       A[r] = lds16(p0 + rc0 + r * BX);
       B[r] = lds16(p1 + rc0 + r * BX);
     }
-    release(0);
+    release(p.slot);
     // Three steps per trip rotate the register roles (b, c, t) without moves.
     int jj = 0;
     for (; jj + 3 <= nzl; jj += 3) {
@@ -390,7 +342,57 @@ __device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridVie
       if (!bad && jj + 1 < nzl) bad = !step(B, C, A);
     }
   }
-  if (bad && lane == 0) atomicExch(err, 1);
+  if (bad) return false;
+  // The last plane (z+1 of the last output plane) was never a plane of z.
+  release(pt.slot);
+  p = pt;
+  ring_next(p, S);
+  return true;
+}
+
+// One tile as a whole CTA (single-grid kernels): the (TX x TY) column at
+// (tile_x, tile_y) of the domain over z chunk zc, read through tensor map
+// `tin`, written to `out`. Called by every thread of the CTA; `smem` is the
+// CTA's 128-byte aligned dynamic shared memory (barriers + ring).
+template <typename T, bool PERIODIC, bool ACC>
+__device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridView out, int nx,
+                                           int ny, int nz, const Dom3 d, const C7<T> k,
+                                           const TmaGeom geo, int tile_x, int tile_y, int zc,
+                                           int images, int *err, unsigned char *smem,
+                                           TileAcc *acc) {
+  // The descriptors arrive by value so that they live in registers: callers
+  // may pass fields of a table in global memory, and references into it
+  // would be reloaded after every store of the hot loop.
+  constexpr int V = 16 / sizeof(T);
+  const Ring R{reinterpret_cast<uint64_t *>(smem), reinterpret_cast<uint64_t *>(smem) + 32,
+               smem + 512, geo.stages, geo.stage_bytes};
+  const int nct = geo.tx_threads * geo.ty_threads;  // consumer threads
+  const int TX = geo.tx_threads * V, TY = geo.ty_threads * kVY;
+  const int x0 = geo.x_base + tile_x * TX;
+  const int y0 = d.lo[1] + tile_y * TY;
+  const int zb = d.lo[2] + zc * geo.zchunk;
+  const int nzl = min(zb + geo.zchunk, d.hi[2]) - zb;  // output planes
+  const int tid = threadIdx.x;
+
+  if (tid == 0) ring_init(R, nct >> 5);
+  __syncthreads();
+
+  RingPos pos{0, 0};
+  if (tid >= nct) {
+    if (tid != nct) return;
+    tma_prefetch_desc(tin);
+    const uint32_t bytes = (uint32_t)(geo.bx * geo.by * sizeof(T));
+    if (!ring_produce(R, pos, tin, bytes, x0 - V + geo.ax0, y0 - 1 + geo.ay0, zb - 1 + geo.az0,
+                      nzl + 2)) {
+      atomicExch(err, 1);
+      ring_drain(R, pos);
+    }
+    return;
+  }
+  if (!diff7_consume<T, PERIODIC, ACC>(R, pos, out, nx, ny, nz, d, k, geo, x0, y0, zb, nzl,
+                                       images, acc) &&
+      (tid & 31) == 0)
+    atomicExch(err, 1);
 }
 
 }  // namespace psb

@@ -52,76 +52,23 @@ __device__ __forceinline__ void consumer_bar(int nct) {
   asm volatile("bar.sync 1, %0;" ::"r"(nct) : "memory");
 }
 
-// One tile of a Himeno sweep: the (TX x TY) column at (tile_x, tile_y) over
-// z chunk zc. Called by every thread of the CTA; `smem` is the CTA's 128-byte
-// aligned dynamic shared memory. Consumer threads add sum(ss*ss) of their
-// points to *acc (FP64). Returns true in threads that must take part in a
-// following consumer barrier (the consumer threads), false in the producer
-// warp. A timeout sets *bad_out.
-__device__ __forceinline__ bool himeno_tile(const CUtensorMap *tin, float *pout,
-                                            const HimenoCoef cf, int64_t sy, int64_t sz,
-                                            const Dom3 d, float omega, const HimenoGeom geo,
-                                            int tile_x, int tile_y, int zc, int *err,
-                                            unsigned char *smem, double *acc_out,
-                                            bool *bad_out) {
+// Consumer warps, one tile of a Himeno sweep: planes zb-1 .. zb+nzl of p
+// around the (TX x TY) column at (x0, y0), from ring position p on (advanced
+// past all nzl + 2 planes, every one released). The twelve coefficient
+// fields are streamed from global memory with 16-byte loads issued before
+// the plane wait. Each consumer thread adds sum(ss*ss) of its points to *acc
+// (FP64). `coef(i)` gives the origin of coefficient field i; callers pass a
+// function that reads it where it is cheapest (a kernel parameter, or shared
+// memory, so 12 pointers need not occupy registers). Returns false
+// (warp-uniformly) if a bounded wait gave up.
+template <typename CoefFn>
+__device__ __forceinline__ bool himeno_consume(const Ring &R, RingPos &p, float *pout,
+                                               CoefFn coef, int64_t sy, int64_t sz,
+                                               const Dom3 d, float omega, const HimenoGeom geo,
+                                               int x0, int y0, int zb, int nzl, double *acc_out) {
   constexpr int V = 4;
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem);
-  uint64_t *empty = full + 32;
-  unsigned char *ring = smem + 768;
-
-  const int S = geo.stages;
-  const int nct = geo.tx_threads * geo.ty_threads;
-  const int ncw = nct >> 5;
-  const int TX = geo.tx_threads * V, TY = geo.ty_threads;
-  const int x0 = geo.x_base + tile_x * TX;
-  const int y0 = d.lo[1] + tile_y * TY;
-  const int zb = d.lo[2] + zc * geo.zchunk;
-  const int ze = min(zb + geo.zchunk, d.hi[2]);
-  const int nzl = ze - zb;
-  const int np = nzl + 2;
+  const int S = R.S;
   const int tid = threadIdx.x;
-
-  if (tid == 0) {
-    for (int i = 0; i < S; i++) {
-      mbar_init(&full[i], 1);
-      mbar_init(&empty[i], ncw);
-    }
-    mbar_fence_init();
-  }
-  __syncthreads();
-
-  if (tid >= nct) {
-    if (tid != nct) return false;
-    tma_prefetch_desc(tin);
-    const uint32_t bytes = (uint32_t)(geo.bx * geo.by * sizeof(float));
-    int slot = 0, round = 0, issued = 0;
-    bool ok = true;
-    for (int j = 0; j < np; j++) {
-      if (round > 0 && !mbar_wait_bounded(&empty[slot], (round - 1) & 1)) {
-        ok = false;
-        break;
-      }
-      mbar_arrive_expect_tx(&full[slot], bytes);
-      tma_load_3d(ring + slot * geo.stage_bytes, tin, &full[slot], x0 - V + geo.ax0,
-                  y0 - 1 + geo.ay0, zb - 1 + j + geo.az0);
-      issued++;
-      if (++slot == S) {
-        slot = 0;
-        round++;
-      }
-    }
-    if (!ok) {
-      atomicExch(err, 1);
-      for (int j = 0; j < issued; j++) {
-        long long t0 = clock64();
-        while (!mbar_try_wait(&full[j % S], (j / S) & 1) && clock64() - t0 < 200000000LL) {
-        }
-      }
-    }
-    return false;
-  }
-
-  // ---------------- consumers ----------------
   const int tx = tid % geo.tx_threads, ty = tid / geo.tx_threads;
   const int lane = tid & 31;
   const int BX = geo.bx;
@@ -131,44 +78,47 @@ __device__ __forceinline__ bool himeno_tile(const CUtensorMap *tin, float *pout,
   const bool row_in = yg >= d.lo[1] && yg < d.hi[1];
   const bool vec_ok = xg0 + V <= geo.nx;
   const bool xvec = xg0 >= d.lo[0] && xg0 + V <= d.hi[0];
-  auto wait_plane = [&](int slot, int round) -> bool {
-    bool ok = mbar_wait_bounded(&full[slot], round & 1);
+  auto wait_plane = [&](const RingPos &q) -> bool {
+    bool ok = mbar_wait_bounded(&R.full[q.slot], q.round & 1);
     return __all_sync(0xffffffffu, ok);
   };
+  auto release = [&](int slot) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&R.empty[slot]);
+  };
   auto plane_ptr = [&](int slot) -> const float * {
-    return reinterpret_cast<const float *>(ring + slot * geo.stage_bytes);
+    return reinterpret_cast<const float *>(R.base + slot * R.stage_bytes);
   };
   double acc = 0.0;
-  bool bad = !wait_plane(0, 0);
-  bad = bad || !wait_plane(1 % S, 1 / S);
-  int s_m = 0, s_c = 1 % S;        // slots of planes z-1 and z
-  int s_p = 1 % S, r_p = 0;        // slot / round of plane z+1 (advanced before use)
+  RingPos pm = p;  // plane z-1
+  RingPos pc = p;  // plane z
+  ring_next(pc, S);
+  RingPos pp = pc;  // plane z+1 (advanced before use)
+  bool bad = !wait_plane(pm);
+  bad = bad || !wait_plane(pc);
   int64_t off = (int64_t)xg0 + (int64_t)yg * sy + (int64_t)zb * sz;
   for (int jj = 0; jj < nzl && !bad; jj++) {
-    const int z = zb + jj;
     float co[12][V];
     if (row_in) {
 #pragma unroll
       for (int i = 0; i < 12; i++) {
+        const float *f = coef(i);
         if (vec_ok) {
-          Vec16<float> q = ldg16_stream(cf.f[i] + off);
+          Vec16<float> q = ldg16_stream(f + off);
 #pragma unroll
           for (int v = 0; v < V; v++) co[i][v] = q.v[v];
         } else {
 #pragma unroll
-          for (int v = 0; v < V; v++) co[i][v] = xg0 + v < geo.nx ? cf.f[i][off + v] : 0.f;
+          for (int v = 0; v < V; v++) co[i][v] = xg0 + v < geo.nx ? f[off + v] : 0.f;
         }
       }
     }
-    if (++s_p == S) {
-      s_p = 0;
-      r_p++;
-    }
-    if (!wait_plane(s_p, r_p)) {
+    ring_next(pp, S);
+    if (!wait_plane(pp)) {
       bad = true;
       break;
     }
-    const float *pm = plane_ptr(s_m), *pc = plane_ptr(s_c), *pp = plane_ptr(s_p);
+    const float *qm = plane_ptr(pm.slot), *qc = plane_ptr(pc.slot), *qp = plane_ptr(pp.slot);
     if (row_in) {
       float outv[V];
 #pragma unroll
@@ -178,10 +128,10 @@ __device__ __forceinline__ bool himeno_tile(const CUtensorMap *tin, float *pout,
 #pragma unroll
         for (int i = 0; i < 12; i++) c[i] = co[i][v];
         float ss;
-        outv[v] = himeno_point(c, pc[o], pc[o + 1], pc[o - 1], pc[o + BX], pc[o - BX], pp[o],
-                               pm[o], pp[o + BX], pp[o - BX], pm[o + BX], pm[o - BX],
-                               pc[o + 1 + BX], pc[o + 1 - BX], pc[o - 1 + BX], pc[o - 1 - BX],
-                               pp[o + 1], pm[o + 1], pp[o - 1], pm[o - 1], omega, &ss);
+        outv[v] = himeno_point(c, qc[o], qc[o + 1], qc[o - 1], qc[o + BX], qc[o - BX], qp[o],
+                               qm[o], qp[o + BX], qp[o - BX], qm[o + BX], qm[o - BX],
+                               qc[o + 1 + BX], qc[o + 1 - BX], qc[o - 1 + BX], qc[o - 1 - BX],
+                               qp[o + 1], qm[o + 1], qp[o - 1], qm[o - 1], omega, &ss);
         if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) acc += (double)ss * (double)ss;
       }
       float *dst = pout + off;
@@ -194,16 +144,63 @@ __device__ __forceinline__ bool himeno_tile(const CUtensorMap *tin, float *pout,
       }
     }
     // Plane z-1 is done for this warp.
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&empty[s_m]);
-    s_m = s_c;
-    s_c = s_p;
+    release(pm.slot);
+    pm = pc;
+    pc = pp;
     off += sz;
-    (void)z;
   }
-  if (bad && lane == 0) atomicExch(err, 1);
   *acc_out += acc;
-  *bad_out = bad;
+  if (bad) return false;
+  // The last two planes (z and z+1 of the last output plane).
+  release(pm.slot);
+  release(pc.slot);
+  p = pc;
+  ring_next(p, S);
+  return true;
+}
+
+// One tile of a Himeno sweep as a whole CTA (single-grid kernels): the
+// (TX x TY) column at (tile_x, tile_y) over z chunk zc. `smem` is the CTA's
+// 128-byte aligned dynamic shared memory. Consumer threads add sum(ss*ss) of
+// their points to *acc (FP64). Returns true in threads that must take part
+// in a following consumer barrier (the consumer threads), false in the
+// producer warp. A timeout sets *bad_out.
+__device__ __forceinline__ bool himeno_tile(const CUtensorMap *tin, float *pout,
+                                            const HimenoCoef cf, int64_t sy, int64_t sz,
+                                            const Dom3 d, float omega, const HimenoGeom geo,
+                                            int tile_x, int tile_y, int zc, int *err,
+                                            unsigned char *smem, double *acc_out,
+                                            bool *bad_out) {
+  constexpr int V = 4;
+  const Ring R{reinterpret_cast<uint64_t *>(smem), reinterpret_cast<uint64_t *>(smem) + 32,
+               smem + 768, geo.stages, geo.stage_bytes};
+  const int nct = geo.tx_threads * geo.ty_threads;
+  const int TX = geo.tx_threads * V, TY = geo.ty_threads;
+  const int x0 = geo.x_base + tile_x * TX;
+  const int y0 = d.lo[1] + tile_y * TY;
+  const int zb = d.lo[2] + zc * geo.zchunk;
+  const int nzl = min(zb + geo.zchunk, d.hi[2]) - zb;
+  const int tid = threadIdx.x;
+
+  if (tid == 0) ring_init(R, nct >> 5);
+  __syncthreads();
+
+  RingPos pos{0, 0};
+  if (tid >= nct) {
+    if (tid != nct) return false;
+    tma_prefetch_desc(tin);
+    const uint32_t bytes = (uint32_t)(geo.bx * geo.by * sizeof(float));
+    if (!ring_produce(R, pos, tin, bytes, x0 - V + geo.ax0, y0 - 1 + geo.ay0, zb - 1 + geo.az0,
+                      nzl + 2)) {
+      atomicExch(err, 1);
+      ring_drain(R, pos);
+    }
+    return false;
+  }
+  const bool ok = himeno_consume(R, pos, pout, [&](int i) { return cf.f[i]; }, sy, sz, d, omega,
+                                 geo, x0, y0, zb, nzl, acc_out);
+  if (!ok && (tid & 31) == 0) atomicExch(err, 1);
+  *bad_out = !ok;
   return true;
 }
 
