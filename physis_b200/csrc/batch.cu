@@ -470,6 +470,7 @@ struct BatchGroup {
   unsigned long long *d_cursor = nullptr;
   size_t cap_order = 0, cap_tile_prefix = 0, cap_step_offset = 0;
   int blocks_persistent = 0;
+  double work = 0;  // algorithmic bytes of the list (orders the concurrent launches)
 };
 
 struct psb_batch {
@@ -721,6 +722,9 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
       G.step_offset[st + 1] = G.step_offset[st] + G.tile_prefix[active];
     }
     G.total_items = G.max_steps ? G.step_offset[G.max_steps] : 0;
+    G.work = 0;
+    for (int i : G.order)
+      G.work += (double)b->hm[i].points * steps[i] * (gi == 1 ? 56.0 : 8.0);
     PSB_CHECK(dev_reserve(&G.d_order, &G.cap_order, sizeof(int) * std::max(1, gn)));
     if (gn) PSB_TRY(cudaMemcpy(G.d_order, G.order.data(), sizeof(int) * gn, cudaMemcpyHostToDevice));
     PSB_CHECK(dev_reserve(&G.d_tile_prefix, &G.cap_tile_prefix, sizeof(int64_t) * (gn + 1)));
@@ -784,19 +788,45 @@ static BatchDev batch_dev(psb_batch *b, int gi) {
   return B;
 }
 
+static psb_status batch_side_stream(psb_batch *b) {
+  if (!b->side) {
+    PSB_TRY(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+    PSB_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    PSB_TRY(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming));
+  }
+  return PSB_OK;
+}
+
+// Mode 0: the two kinds' persistent launches run concurrently, the one with
+// more work launched first on `s`, the other on a side stream; the second
+// launch's CTAs take slots as the first one's retire, so each fills the
+// other's tail.
 psb_status batch_launch_persistent(psb_batch *b, cudaStream_t s, int64_t *launches) {
   PSB_CHECK(batch_reset_counters(b, s));
-  for (int gi = 0; gi < 2; gi++) {
+  const bool both = b->grp[0].total_items && b->grp[1].total_items;
+  if (both) {
+    PSB_CHECK(batch_side_stream(b));
+    PSB_TRY(cudaEventRecord(b->fork, s));
+    PSB_TRY(cudaStreamWaitEvent(b->side, b->fork, 0));
+  }
+  const int first = b->grp[1].work > b->grp[0].work ? 1 : 0;
+  for (int k = 0; k < 2; k++) {
+    const int gi = k == 0 ? first : 1 - first;
     const BatchGroup &G = b->grp[gi];
     if (!G.total_items) continue;
+    cudaStream_t ss = both && k == 1 ? b->side : s;
     const int blocks = (int)std::min<int64_t>(G.blocks_persistent, G.total_items);
     if (gi == 0)
-      k_batch<0><<<blocks, kBThreads, batch_smem(0), s>>>(batch_dev(b, 0), -1);
+      k_batch<0><<<blocks, kBThreads, batch_smem(0), ss>>>(batch_dev(b, 0), -1);
     else
-      k_batch<1><<<blocks, kBThreads, batch_smem(1), s>>>(batch_dev(b, 1), -1);
+      k_batch<1><<<blocks, kBThreads, batch_smem(1), ss>>>(batch_dev(b, 1), -1);
     (*launches)++;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_status(e, "k_batch");
+  }
+  if (both) {
+    PSB_TRY(cudaEventRecord(b->join, b->side));
+    PSB_TRY(cudaStreamWaitEvent(s, b->join, 0));
   }
   return PSB_OK;
 }
@@ -805,11 +835,7 @@ psb_status batch_launch_persistent(psb_batch *b, cudaStream_t s, int64_t *launch
 // forked and joined inside one CUDA graph, recorded once and replayed.
 psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches) {
   if (!b->graph) {
-    if (!b->side) {
-      PSB_TRY(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
-      PSB_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
-      PSB_TRY(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming));
-    }
+    PSB_CHECK(batch_side_stream(b));
     cudaGraph_t g;
     PSB_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     psb_status st = batch_reset_counters(b, s);

@@ -10,11 +10,14 @@
 //                 slot is free); their grids come from a stream-ordered pool,
 //                 are filled on the device (copy-in or seeded generation) and
 //                 stay resident until the request finishes;
-//   rounds     -- every admitted request advances in one launch of the
+//   rounds     -- admitted requests advance together in one launch of the
 //                 persistent batched kernel (one work list over all of them,
-//                 each at its own step count); a round is R steps per request
-//                 with R chosen so a round is a few milliseconds of work;
-//                 requests admitted while a round runs join the next one;
+//                 each at its own step count); a round takes the requests
+//                 with the least remaining work until they fill the GPU at
+//                 every step (so small solves finish first rather than all
+//                 together), and runs R steps of each, R chosen so a round is
+//                 some 20 ms of work; requests admitted while a round runs
+//                 join the next one;
 //   retirement -- a request that converged (the kernel stops it at the check
 //                 step, so no work is spent past it), ran max_steps or was
 //                 cancelled leaves the list; its result is copied to the
@@ -56,6 +59,7 @@ struct SReq {
   double residual = -1.0;
   std::atomic<bool> cancel{false};
   bool complete = false;
+  int skipped = 0;  // consecutive rounds this admitted request was left out of
   BatchMemberHost h;
   double res[4] = {0, 0, 0, 0};
   cudaEvent_t copied = nullptr;
@@ -65,6 +69,13 @@ struct SReq {
 // fewest steps a round gives each request.
 constexpr double kRoundWork = 1.6e10;
 constexpr int kRoundMinSteps = 4;
+// A round advances the admitted requests with the least remaining work
+// (shortest remaining work first, so small solves finish early instead of
+// all finishing together) until their points per step reach kRoundPoints,
+// enough tiles to keep every SM busy at every step; a request left out of
+// kMaxSkipRounds rounds in a row is always taken.
+constexpr int64_t kRoundPoints = 96ll << 20;
+constexpr int kMaxSkipRounds = 8;
 
 // Residual terms of two grids (FIFO mode): per-CTA FP64 partials of
 // sum (a - b)^2 and sum a^2, combined on the host in CTA order.
@@ -270,16 +281,37 @@ static double residual_of(const double *r4) {
 // One round of the persistent batched kernel over every active request.
 static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
   Runtime &r = rt();
-  const int n = (int)S->active.size();
+  // This round's requests: cancelled ones (to retire them), those waiting
+  // too long, then the least remaining work first up to kRoundPoints.
+  std::vector<SReq *> order(S->active);
+  auto remaining = [](const SReq *q) {
+    return (double)q->h.points * (q->q.max_steps - q->steps_done);
+  };
+  std::stable_sort(order.begin(), order.end(), [&](const SReq *x, const SReq *y) {
+    const int px = x->cancel ? 0 : x->skipped >= kMaxSkipRounds ? 1 : 2;
+    const int py = y->cancel ? 0 : y->skipped >= kMaxSkipRounds ? 1 : 2;
+    if (px != py) return px < py;
+    return remaining(x) < remaining(y);
+  });
+  std::vector<SReq *> round_reqs;
+  int64_t points = 0;
+  for (SReq *q : order) {
+    if (q->cancel || q->skipped >= kMaxSkipRounds || points < kRoundPoints) {
+      round_reqs.push_back(q);
+      points += q->cancel ? 0 : q->h.points;
+      q->skipped = 0;
+    } else {
+      q->skipped++;
+    }
+  }
+  const int n = (int)round_reqs.size();
   std::vector<BatchMemberHost> hm(n);
   std::vector<int> steps(n), step0(n);
   std::vector<double> res_init(4 * n);
-  int64_t points = 0;
-  for (int i = 0; i < n; i++) points += S->active[i]->h.points;
   const int R = (int)std::max<double>(
       kRoundMinSteps, std::min<double>(1000.0, kRoundWork / std::max<int64_t>(1, points)));
   for (int i = 0; i < n; i++) {
-    SReq *q = S->active[i];
+    SReq *q = round_reqs[i];
     hm[i] = q->h;
     step0[i] = q->steps_done;
     steps[i] = q->cancel ? 0 : std::min(q->q.max_steps - q->steps_done, R);
@@ -308,7 +340,7 @@ static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
   PSB_CHECK(batch_read_state(S->batch, stop, res));
   // Periodic writers keep the halo of their outputs current.
   for (int i = 0; i < n; i++) {
-    SReq *q = S->active[i];
+    SReq *q = round_reqs[i];
     q->steps_done += stop[i] >= 0 ? stop[i] : steps[i];
     for (int k = 0; k < 4; k++) q->res[k] = res[4 * i + k];
     q->residual = residual_of(q->res);
@@ -322,17 +354,21 @@ static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
     S->device_ms += ms;
   }
   std::vector<SReq *> keep;
+  std::vector<char> ran(S->active.size(), 0);
   for (int i = 0; i < n; i++) {
-    SReq *q = S->active[i];
+    SReq *q = round_reqs[i];
     if (q->cancel) {
       q->status = PSB_ERR_CANCELLED;
       finished.push_back(q);
     } else if (stop[i] >= 0 || q->steps_done >= q->q.max_steps) {
       finished.push_back(q);
     } else {
-      keep.push_back(q);
+      continue;
     }
+    ran[std::find(S->active.begin(), S->active.end(), q) - S->active.begin()] = 1;
   }
+  for (size_t i = 0; i < S->active.size(); i++)
+    if (!ran[i]) keep.push_back(S->active[i]);
   S->active.swap(keep);
   return PSB_OK;
 }
