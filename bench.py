@@ -463,6 +463,52 @@ def c4_batch(ps, members, grids):
     return b
 
 
+def c4_e2e(ps, members, grids, b, lups, dist, reps=2):
+    """The batch through the public API with host buffers: every member's
+    input grids (7-point: the field; Himeno: both p grids and the twelve
+    coefficient fields) copied in from pinned host memory, the batch run,
+    every result grid copied back, all inside the timed region."""
+    import ctypes
+    ins, outs = [], []
+    for (kind, dims, steps), g in zip(members, grids):
+        ins += [g[0]] if kind == "diffp" else list(g)
+        outs.append(g[steps & 1])
+    n_in = sum(int(np.prod(g.dims)) for g in ins)
+    n_out = sum(int(np.prod(g.dims)) for g in outs)
+    hp = ctypes.c_void_p()
+    ps.check(ps.lib.psb_host_alloc((n_in + n_out) * 4, ctypes.byref(hp)), "psb_host_alloc")
+    host = np.ctypeslib.as_array((ctypes.c_float * (n_in + n_out)).from_address(hp.value))
+    off, ptr_in, ptr_out = 0, [], []
+    for g in ins:
+        ptr_in.append(hp.value + off * 4)
+        off += int(np.prod(g.dims))
+    for g in outs:
+        ptr_out.append(hp.value + off * 4)
+        off += int(np.prod(g.dims))
+    for g, p in zip(ins, ptr_in):  # the inputs as they are now, as host data
+        ps.check(ps.lib.psb_grid_copyout_async(g.ptr, ctypes.c_void_p(p)), "copyout")
+    ps.sync()
+
+    def one():
+        for g, p in zip(ins, ptr_in):
+            ps.check(ps.lib.psb_grid_copyin_async(g.ptr, ctypes.c_void_p(p)), "copyin")
+        b.run(0)
+        for g, p in zip(outs, ptr_out):
+            ps.check(ps.lib.psb_grid_copyout_async(g.ptr, ctypes.c_void_p(p)), "copyout")
+        ps.sync()
+
+    one()
+    dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        one()
+    secs = dist.max(time.perf_counter() - t0)
+    ps.check(ps.lib.psb_host_free(hp), "psb_host_free")
+    del host
+    return {"value": dist.sum(lups * reps) / secs / 1e9, "unit": "GLUPS",
+            "h2d_bytes_per_step": n_in * 4, "d2h_bytes_per_step": n_out * 4}
+
+
 def run_c4(args, dist):
     os.environ["PHYSIS_B200_DEVICE"] = str(dist.local)
     import physis_b200 as ps
@@ -486,7 +532,7 @@ def run_c4(args, dist):
             ms.append(b.stats()["device_ms"])
         return ms
 
-    res = {1: timed(1, 2, 1)}   # per-step graph mode
+    res = {1: timed(1, 2, 1) if not args.skip_graph else [float("nan")]}  # per-step graph mode
     timed(0, 0, args.warmup)    # warm up the persistent mode (the headline)
     sampler = ClockSampler(dist.local)
     dist.barrier()
@@ -495,9 +541,19 @@ def run_c4(args, dist):
     clocks = sampler.stop()
     dev_s = dist.max(sum(ms_p) / 1e3)
     value = dist.sum(lups * args.steps) / dev_s / 1e9
+    launches = b.stats()["launches"] * args.steps
     loop_plain = timed(2, 1, 0)[0] if not args.skip_loops else float("nan")
     loop_tuned = timed(3, 1, 0)[0] if not args.skip_loops else float("nan")
     per_run_s = dev_s / args.steps
+    e2e = None if args.no_e2e else c4_e2e(ps, members, grids, b, lups, dist)
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        rate_d, rate_h, kind, sample = cpu_rates(periodic=True)
+        lu_d = sum(d[0] * d[1] * d[2] * st for k, d, st in members if k == "diffp")
+        lu_h = lups - lu_d
+        cpu = {"value": lups / (lu_d / rate_d + lu_h / rate_h) / 1e9, "unit": "GLUPS",
+               "cores": 1, "kind": kind,
+               "sample": sample + "; GLUPS = the batch's updates / sum of updates / rate per kind"}
     line = {
         "metric": "lattice_updates_per_s_c4", "value": value, "unit": "GLUPS",
         "n_gpus": dist.world, "steps": args.steps, "warmup": args.warmup,
@@ -521,10 +577,10 @@ def run_c4(args, dist):
                      "unit": "GB/s", "frac": alg_bytes / per_run_s / 1e9 / peaks()[0],
                      "traffic": None, "algorithmic_bytes_per_launch": alg_bytes,
                      "avg_launch_us": per_run_s * 1e6},
-        "e2e": None,
-        "gpu_launches": args.steps,
+        "e2e": e2e,
+        "gpu_launches": launches,
         "clocks": clocks,
-        "cpu_baseline": None,
+        "cpu_baseline": cpu,
     }
     b.free()
     for g in grids:
@@ -707,37 +763,45 @@ def run_c5(args, dist):
         print(json.dumps(line), flush=True)
 
 
-def c5_cpu_baseline(trace, steps_done):
-    """Reference CPU target (1 thread) rates on a bounded sample, applied to the
-    trace's lattice updates (the served steps of every request)."""
+def cpu_rates(periodic=False):
+    """Rates (updates/s) of the reference CPU target, 1 thread, on bounded
+    samples: 7-point diffusion 128^3 x 40 steps and Himeno 129^3 x 16 sweeps
+    (about a second each), run loop only."""
     from oracle import oracle
     use_ref = oracle.ref_available()
     f = np.random.default_rng(3).random((128, 128, 128), dtype=np.float32)
     t0 = time.perf_counter()
     if use_ref:
-        _, secs_d = oracle.ref_diffusion7(f, 10, np.asarray(COEF, np.float32))
+        _, secs_d = oracle.ref_diffusion7(f, 40, np.asarray(COEF, np.float32), periodic=periodic)
     else:
-        oracle.diffusion7(f, 10, np.asarray(COEF, np.float32))
+        oracle.diffusion7(f, 40, np.asarray(COEF, np.float32), periodic=periodic)
         secs_d = time.perf_counter() - t0
-    rate_d = 128 ** 3 * 10 / secs_d
+    rate_d = 128 ** 3 * 40 / secs_d
     p, coef = himeno_fields((129, 129, 129))
     t0 = time.perf_counter()
     if use_ref:
-        _, secs_h = oracle.ref_himeno(p, coef, 0.8, 4)
+        _, secs_h = oracle.ref_himeno(p, coef, 0.8, 16)
     else:
-        oracle.himeno(p, coef, 0.8, 4)
+        oracle.himeno(p, coef, 0.8, 16)
         secs_h = time.perf_counter() - t0
-    rate_h = 127 ** 3 * 4 / secs_h
+    rate_h = 127 ** 3 * 16 / secs_h
+    sample = ("%s 128^3 %s diffusion x 40 steps (%.3f GLUPS) and 129^3 Himeno x 16 sweeps "
+              "(%.3f GLUPS), 1 thread, run loop only"
+              % ("reference CPU target" if use_ref else "oracle port",
+                 "periodic" if periodic else "clamped", rate_d / 1e9, rate_h / 1e9))
+    return rate_d, rate_h, "reference" if use_ref else "port", sample
+
+
+def c5_cpu_baseline(trace, steps_done):
+    """Reference CPU target rates applied to the trace's lattice updates (the
+    served steps of every request)."""
+    rate_d, rate_h, kind, sample = cpu_rates(periodic=False)
     total = 0.0
-    for i, (t, kind, side, seed) in enumerate(trace):
-        pts = c5_points(kind, side) * steps_done[i]
-        total += pts / (rate_h if kind == "him" else rate_d)
-    return {"value": len(trace) / total, "unit": "solves/s", "cores": 1,
-            "kind": "reference" if use_ref else "port",
-            "sample": "128^3 diffusion x 10 steps (%.3f GLUPS) and 129^3 Himeno x 4 sweeps "
-                      "(%.3f GLUPS) timed, run loop only; solves/s = requests / sum over the "
-                      "trace of served steps x points / rate (residual checks not counted)"
-                      % (rate_d / 1e9, rate_h / 1e9)}
+    for i, (t, k, side, seed) in enumerate(trace):
+        total += c5_points(k, side) * steps_done[i] / (rate_h if k == "him" else rate_d)
+    return {"value": len(trace) / total, "unit": "solves/s", "cores": 1, "kind": kind,
+            "sample": sample + "; solves/s = requests / sum over the trace of served steps x "
+                               "points / rate (residual checks not counted)"}
 
 
 def _ref_rate(pool, procs, kind, dims, dt, count, reps, warm):
@@ -852,6 +916,7 @@ def main():
     ap.add_argument("--no-residual", action="store_true", help="c3: skip the fused residual")
     ap.add_argument("--members", type=int, default=256, help="c4: batch members (profiling)")
     ap.add_argument("--skip-loops", action="store_true", help="c4: skip the per-grid loops")
+    ap.add_argument("--skip-graph", action="store_true", help="c4: skip the per-step graph mode")
     ap.add_argument("--c4-kind", default=None, choices=["diffp", "him"],
                     help="c4: keep only one kind of member (profiling)")
     ap.add_argument("--c5-requests", type=int, default=128, help="c5: requests in the trace")

@@ -170,6 +170,12 @@ psb_status grid_alloc_pool(int type, const int *dims, cudaMemPool_t pool, cudaSt
                            GridImpl **out);
 void grid_free_pool(GridImpl *g, cudaStream_t s);
 psb_status grid_copy_in_on(GridImpl *g, const void *src, cudaStream_t s);
+// Host <-> pitched grid through a dense staging buffer and a pack kernel.
+psb_status pitched_transfer(GridImpl *g, void *host, bool h2d, cudaStream_t s);
+// First half of a copy-out: allocate a dense staging buffer and pack the
+// grid into it on s (the caller copies it out and frees it with
+// cudaFreeAsync, ordered after s).
+psb_status pitched_stage_out(GridImpl *g, void **stage, cudaStream_t s);
 psb_status grid_copy_out_on(GridImpl *g, void *dst, cudaStream_t s);
 
 // Kernel launchers implemented in the .cu files.

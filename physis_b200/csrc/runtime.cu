@@ -277,32 +277,13 @@ void grid_free_pool(GridImpl *g, cudaStream_t s) {
 }
 
 psb_status grid_copy_in_on(GridImpl *g, const void *src, cudaStream_t s) {
-  const int E = g->pub.elm_size;
-  cudaMemcpy3DParms p;
-  memset(&p, 0, sizeof(p));
-  const int nx = g->pub.dim[0], ny = g->pub.dim[1], nz = g->pub.dim[2];
-  p.srcPtr = make_cudaPitchedPtr((void *)src, (size_t)nx * E, nx, ny);
-  p.dstPtr = make_cudaPitchedPtr(g->alloc, (size_t)g->pitch * E, g->pitch, g->rows);
-  p.dstPos = make_cudaPos((size_t)g->pad_left * E, g->halo, g->halo);
-  p.extent = make_cudaExtent((size_t)nx * E, ny, nz);
-  p.kind = cudaMemcpyHostToDevice;
-  PSB_TRY(cudaMemcpy3DAsync(&p, s));
+  PSB_CHECK(pitched_transfer(g, (void *)src, true, s));
   g->ghost_valid = PSB_BOUNDARY_NONE;
   return PSB_OK;
 }
 
 psb_status grid_copy_out_on(GridImpl *g, void *dst, cudaStream_t s) {
-  const int E = g->pub.elm_size;
-  cudaMemcpy3DParms p;
-  memset(&p, 0, sizeof(p));
-  const int nx = g->pub.dim[0], ny = g->pub.dim[1], nz = g->pub.dim[2];
-  p.srcPtr = make_cudaPitchedPtr(g->alloc, (size_t)g->pitch * E, g->pitch, g->rows);
-  p.srcPos = make_cudaPos((size_t)g->pad_left * E, g->halo, g->halo);
-  p.dstPtr = make_cudaPitchedPtr(dst, (size_t)nx * E, nx, ny);
-  p.extent = make_cudaExtent((size_t)nx * E, ny, nz);
-  p.kind = cudaMemcpyDeviceToHost;
-  PSB_TRY(cudaMemcpy3DAsync(&p, s));
-  return PSB_OK;
+  return pitched_transfer(g, dst, false, s);
 }
 
 static void grid_free(GridImpl *g) {
@@ -327,16 +308,7 @@ static psb_status copy_in(GridImpl *g, const void *src, bool sync) {
     PSB_TRY(cudaMemcpyAsync(g->alloc, src, (size_t)g->pub.num_elms * E, cudaMemcpyHostToDevice,
                             r.stream));
   } else {
-    int nd = g->pub.num_dims;
-    cudaMemcpy3DParms p;
-    memset(&p, 0, sizeof(p));
-    int nx = g->pub.dim[0], ny = nd > 1 ? g->pub.dim[1] : 1, nz = nd > 2 ? g->pub.dim[2] : 1;
-    p.srcPtr = make_cudaPitchedPtr((void *)src, (size_t)nx * E, nx, ny);
-    p.dstPtr = make_cudaPitchedPtr(g->alloc, (size_t)g->pitch * E, g->pitch, g->rows);
-    p.dstPos = make_cudaPos((size_t)g->pad_left * E, nd > 1 ? g->halo : 0, nd > 2 ? g->halo : 0);
-    p.extent = make_cudaExtent((size_t)nx * E, ny, nz);
-    p.kind = cudaMemcpyHostToDevice;
-    PSB_TRY(cudaMemcpy3DAsync(&p, r.stream));
+    PSB_CHECK(pitched_transfer(g, (void *)src, true, r.stream));
     g->ghost_valid = PSB_BOUNDARY_NONE;
   }
   if (sync) PSB_TRY(cudaStreamSynchronize(r.stream));
@@ -351,16 +323,7 @@ static psb_status copy_out(GridImpl *g, void *dst, bool sync) {
     PSB_TRY(cudaMemcpyAsync(dst, g->alloc, (size_t)g->pub.num_elms * E, cudaMemcpyDeviceToHost,
                             r.stream));
   } else {
-    int nd = g->pub.num_dims;
-    cudaMemcpy3DParms p;
-    memset(&p, 0, sizeof(p));
-    int nx = g->pub.dim[0], ny = nd > 1 ? g->pub.dim[1] : 1, nz = nd > 2 ? g->pub.dim[2] : 1;
-    p.srcPtr = make_cudaPitchedPtr(g->alloc, (size_t)g->pitch * E, g->pitch, g->rows);
-    p.srcPos = make_cudaPos((size_t)g->pad_left * E, nd > 1 ? g->halo : 0, nd > 2 ? g->halo : 0);
-    p.dstPtr = make_cudaPitchedPtr(dst, (size_t)nx * E, nx, ny);
-    p.extent = make_cudaExtent((size_t)nx * E, ny, nz);
-    p.kind = cudaMemcpyDeviceToHost;
-    PSB_TRY(cudaMemcpy3DAsync(&p, r.stream));
+    PSB_CHECK(pitched_transfer(g, dst, false, r.stream));
   }
   if (sync) PSB_TRY(cudaStreamSynchronize(r.stream));
   return PSB_OK;

@@ -63,6 +63,7 @@ struct SReq {
   BatchMemberHost h;
   double res[4] = {0, 0, 0, 0};
   cudaEvent_t copied = nullptr;
+  void *stage = nullptr;  // packed result on its way to the host
 };
 
 // Lattice updates a round aims at (some 20 ms of device time), and the
@@ -243,18 +244,40 @@ static psb_status admit_request(psb_server *S, SReq *q) {
   return PSB_OK;
 }
 
-// Queue the copy of a finished request's result and the release of its
-// grids on the copy stream. The request's last round has completed (the
-// worker synchronises every round), so the copy may overlap the next one.
-static psb_status retire_request(psb_server *S, SReq *q) {
+// Retiring a finished request takes two steps. First, on the runtime stream
+// before the next round is launched, its result grid is packed into a dense
+// staging buffer (a short HBM pass; once the round's persistent kernel holds
+// every SM nothing else would run). Then the copy stream, ordered after the
+// pack, moves the dense block to the caller's buffer and releases the
+// staging buffer and the grids, while the round runs.
+static psb_status retire_pack(psb_server *S, SReq *q) {
+  Runtime &r = rt();
+  q->stage = nullptr;
   if (q->status == PSB_OK && q->q.out && q->h.ngrids)
-    PSB_CHECK(grid_copy_out_on(q->h.grids[q->steps_done & 1], q->q.out, S->copy));
-  free_grids(S, q, S->copy);
+    PSB_CHECK(pitched_stage_out(q->h.grids[q->steps_done & 1], &q->stage, r.stream));
   if (!q->copied) PSB_TRY(cudaEventCreateWithFlags(&q->copied, cudaEventDisableTiming));
+  PSB_TRY(cudaEventRecord(q->copied, r.stream));
+  return PSB_OK;
+}
+
+static psb_status retire_copy(psb_server *S, SReq *q) {
+  PSB_TRY(cudaStreamWaitEvent(S->copy, q->copied, 0));
+  if (q->stage) {
+    const size_t bytes = (size_t)q->q.dims[0] * q->q.dims[1] * q->q.dims[2] * sizeof(float);
+    PSB_TRY(cudaMemcpyAsync(q->q.out, q->stage, bytes, cudaMemcpyDeviceToHost, S->copy));
+    PSB_TRY(cudaFreeAsync(q->stage, S->copy));
+    q->stage = nullptr;
+  }
+  free_grids(S, q, S->copy);
   PSB_TRY(cudaEventRecord(q->copied, S->copy));
   std::lock_guard<std::mutex> lk(S->mu);
   S->retiring.push_back(q);
   return PSB_OK;
+}
+
+static psb_status retire_request(psb_server *S, SReq *q) {
+  PSB_CHECK(retire_pack(S, q));
+  return retire_copy(S, q);
 }
 
 // Complete the retiring requests whose copies are done (server lock held).
@@ -317,18 +340,30 @@ static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
     steps[i] = q->cancel ? 0 : std::min(q->q.max_steps - q->steps_done, R);
     for (int k = 0; k < 4; k++) res_init[4 * i + k] = q->res[k];
   }
+  const double t0 = now_s();
   batch_set_members(S->batch, hm, res_init);
   PSB_CHECK(batch_prepare(S->batch, steps, step0));
+  const double t1 = now_s();
+  // Results of the previous round: packed now, copied out while this round runs.
+  const int nretire = (int)finished.size();
+  for (SReq *q : finished) PSB_CHECK(retire_pack(S, q));
   PSB_TRY(cudaEventRecord(S->ev0, r.stream));
   int64_t launches = 0;
   PSB_CHECK(batch_launch_persistent(S->batch, r.stream, &launches));
   PSB_TRY(cudaEventRecord(S->ev1, r.stream));
-  // Results of the previous round go out while this one runs.
-  for (SReq *q : finished) PSB_CHECK(retire_request(S, q));
+  for (SReq *q : finished) PSB_CHECK(retire_copy(S, q));
   finished.clear();
+  const double t2 = now_s();
   PSB_TRY(cudaEventSynchronize(S->ev1));
+  const double t3 = now_s();
   float ms = 0;
   cudaEventElapsedTime(&ms, S->ev0, S->ev1);
+  if (__ps_trace)
+    fprintf(__ps_trace,
+            "physis_b200 serve: round of %d requests (%lld points/step, %d steps), %d retired; "
+            "host prepare %.3f ms, launch+retire %.3f ms, wait %.3f ms; device %.3f ms\n",
+            n, (long long)points, R, nretire, (t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3,
+            ms);
   int err = 0;
   PSB_TRY(cudaMemcpy(&err, r.d_error, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) {
@@ -380,6 +415,8 @@ static void fail_active(psb_server *S, std::vector<SReq *> &finished, psb_status
   S->active.clear();
   for (SReq *q : finished) {
     if (q->status == PSB_OK) q->status = st;
+    if (q->stage) cudaFreeAsync(q->stage, r.stream);
+    q->stage = nullptr;
     free_grids(S, q, r.stream);
     std::lock_guard<std::mutex> lk(S->mu);
     S->used -= q->bytes;
@@ -426,6 +463,7 @@ static void worker_batched(psb_server *S) {
       }
     }
     std::lock_guard<std::recursive_mutex> g(r.mu);
+    const double ta = now_s();
     for (SReq *q : admit) {
       psb_status st = admit_request(S, q);
       if (st != PSB_OK) {
@@ -437,6 +475,9 @@ static void worker_batched(psb_server *S) {
       }
       S->active.push_back(q);
     }
+    if (__ps_trace && !admit.empty())
+      fprintf(__ps_trace, "physis_b200 serve: admitted %d requests in %.3f ms\n",
+              (int)admit.size(), (now_s() - ta) * 1e3);
     if (S->active.empty()) continue;
     psb_status st = run_round(S, finished);
     if (st != PSB_OK) fail_active(S, finished, st);

@@ -8,6 +8,9 @@
 //   kind 2: 1 inside, 0 on the faces                   (Himeno bnd)
 //   kind 3: (z / (nz - 1))^2                           (Himeno initial p)
 // computed in double and rounded to the grid's type once.
+#include <cstring>
+#include <mutex>
+
 #include "device.cuh"
 
 namespace psb {
@@ -48,6 +51,121 @@ __global__ void k_fill(GridView g, int kind, uint64_t seed, double lo, double hi
     }
     ((T *)g.origin)[(int64_t)x + (int64_t)y * g.sy + (int64_t)z * g.sz] = (T)v;
   }
+}
+
+// Rows of a pitched grid <-> a dense x-fastest array in device memory: one
+// warp per row, lanes along x (coalesced on both sides).
+template <typename W>
+__global__ void __launch_bounds__(256) k_pack(GridView g, W *dense, int unpack) {
+  const int nx = g.n[0], ny = g.n[1];
+  const int64_t rows = (int64_t)ny * g.n[2];
+  const int lane = threadIdx.x & 31;
+  for (int64_t r = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5); r < rows;
+       r += (int64_t)gridDim.x * 8) {
+    const int64_t y = r % ny, z = r / ny;
+    W *row = (W *)g.origin + y * g.sy + z * g.sz;
+    W *d = dense + r * nx;
+    if (unpack)
+      for (int x = lane; x < nx; x += 32) row[x] = d[x];
+    else
+      for (int x = lane; x < nx; x += 32) d[x] = row[x];
+  }
+}
+
+static std::mutex g_stage_mu;
+static cudaMemPool_t g_stage_pool = nullptr;
+
+static cudaMemPool_t staging_pool() {
+  std::lock_guard<std::mutex> lk(g_stage_mu);
+  if (!g_stage_pool) {
+    cudaMemPoolProps props;
+    memset(&props, 0, sizeof(props));
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = rt().device;
+    if (cudaMemPoolCreate(&g_stage_pool, &props) != cudaSuccess) {
+      cudaGetLastError();
+      g_stage_pool = nullptr;
+      return nullptr;
+    }
+    // Keep up to 1 GB of staging memory between copies.
+    uint64_t keep = 1ull << 30;
+    cudaMemPoolSetAttribute(g_stage_pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  }
+  return g_stage_pool;
+}
+
+// Host <-> pitched grid on stream s. The copy engines move a strided 3-D copy
+// row by row, which is slow for the short rows of narrow grids; instead the
+// dense host array crosses the link as one contiguous block into a staging
+// buffer (stream-ordered pool, no device-wide synchronisation) and k_pack
+// moves it into (or out of) the rows at HBM speed. If no staging memory can
+// be had, the strided copy is used.
+psb_status pitched_transfer(GridImpl *g, void *host, bool h2d, cudaStream_t s) {
+  const int E = g->pub.elm_size;
+  const size_t bytes = (size_t)g->pub.num_elms * E;
+  const GridView v = g->view();
+  void *stage = nullptr;
+  cudaMemPool_t pool = staging_pool();
+  if (pool && cudaMallocFromPoolAsync(&stage, bytes, pool, s) == cudaSuccess) {
+    const int64_t rows = (int64_t)v.n[1] * v.n[2];
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 7) / 8,
+                                                                    (int64_t)rt().sm_count * 16));
+    if (h2d) PSB_TRY(cudaMemcpyAsync(stage, host, bytes, cudaMemcpyHostToDevice, s));
+    if (E == 4)
+      k_pack<uint32_t><<<blocks, 256, 0, s>>>(v, (uint32_t *)stage, h2d ? 1 : 0);
+    else
+      k_pack<uint64_t><<<blocks, 256, 0, s>>>(v, (uint64_t *)stage, h2d ? 1 : 0);
+    PSB_TRY(cudaGetLastError());
+    if (!h2d) PSB_TRY(cudaMemcpyAsync(host, stage, bytes, cudaMemcpyDeviceToHost, s));
+    PSB_TRY(cudaFreeAsync(stage, s));
+    return PSB_OK;
+  }
+  cudaGetLastError();
+  const int nx = v.n[0], ny = v.n[1], nz = v.n[2];
+  const int nd = g->pub.num_dims;
+  cudaMemcpy3DParms p;
+  memset(&p, 0, sizeof(p));
+  cudaPitchedPtr dense = make_cudaPitchedPtr(host, (size_t)nx * E, nx, ny);
+  cudaPitchedPtr dev = make_cudaPitchedPtr(g->alloc, (size_t)g->pitch * E, g->pitch, g->rows);
+  cudaPos pos = make_cudaPos((size_t)g->pad_left * E, nd > 1 ? g->halo : 0, nd > 2 ? g->halo : 0);
+  if (h2d) {
+    p.srcPtr = dense;
+    p.dstPtr = dev;
+    p.dstPos = pos;
+    p.kind = cudaMemcpyHostToDevice;
+  } else {
+    p.srcPtr = dev;
+    p.srcPos = pos;
+    p.dstPtr = dense;
+    p.kind = cudaMemcpyDeviceToHost;
+  }
+  p.extent = make_cudaExtent((size_t)nx * E, ny, nz);
+  PSB_TRY(cudaMemcpy3DAsync(&p, s));
+  return PSB_OK;
+}
+
+// Two-phase copy-out for callers that overlap the transfer with kernels
+// occupying every SM: pack into a staging buffer on stream s (a short HBM
+// pass), then move the dense block to the host on another stream after an
+// event (copy engines only) and release the buffer there.
+psb_status pitched_stage_out(GridImpl *g, void **stage, cudaStream_t s) {
+  const int E = g->pub.elm_size;
+  const size_t bytes = (size_t)g->pub.num_elms * E;
+  const GridView v = g->view();
+  *stage = nullptr;
+  cudaMemPool_t pool = staging_pool();
+  if (!pool) return set_status(PSB_ERR_NOMEM);
+  PSB_TRY(cudaMallocFromPoolAsync(stage, bytes, pool, s));
+  const int64_t rows = (int64_t)v.n[1] * v.n[2];
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 7) / 8,
+                                                                  (int64_t)rt().sm_count * 16));
+  if (E == 4)
+    k_pack<uint32_t><<<blocks, 256, 0, s>>>(v, (uint32_t *)*stage, 0);
+  else
+    k_pack<uint64_t><<<blocks, 256, 0, s>>>(v, (uint64_t *)*stage, 0);
+  PSB_TRY(cudaGetLastError());
+  return PSB_OK;
 }
 
 }  // namespace psb
