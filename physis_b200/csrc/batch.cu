@@ -79,6 +79,13 @@ __host__ __device__ constexpr int kind_stage_bytes(int group) {
 // 512 (qfull) and 544 (qempty), item descriptors (kQ x 112 bytes) at 576,
 // stages from 1024.
 constexpr int kQ = 4;  // item descriptors in flight between producer and consumers
+#ifndef PSB_COEF_LEAD
+#define PSB_COEF_LEAD 0
+#endif
+// Himeno coefficient planes are brought into L2 this many planes ahead of
+// the p plane being issued (which itself runs up to kBStages planes ahead
+// of the consumers).
+constexpr int kCoefLead = PSB_COEF_LEAD;
 constexpr int kSmemRing = 1024;
 
 struct BMember {
@@ -264,13 +271,16 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, uint64
       // the same z into L2. The consumers load them one plane at a time
       // (registers hold one plane's coefficients); coming from L2 instead of
       // DRAM their latency no longer limits the sweep.
+      auto prefetch = [&](int z) {
+        if (z >= g.zb && z < g.zb + g.nzl)
+          for (int f = 0; f < 12; f++)
+            tma_prefetch_l2_3d(M->tcoef + f, g.x0 + ax0, g.y0 + ay0, z + az0);
+      };
+      for (int z = g.zb; z < g.zb - 1 + kCoefLead; z++) prefetch(z);
       for (int j = 0; j < g.nzl + 2 && ok; j++) {
         ok = ring_produce(R, pos, M->tmap[par], (uint32_t)(bx * by * 4), g.x0 - 4 + ax0,
                           g.y0 - 1 + ay0, g.zb - 1 + j + az0, 1);
-        const int z = g.zb - 1 + j;
-        if (ok && z >= g.zb && z < g.zb + g.nzl)
-          for (int f = 0; f < 12; f++)
-            tma_prefetch_l2_3d(M->tcoef + f, g.x0 + ax0, g.y0 + ay0, z + az0);
+        if (ok) prefetch(g.zb - 1 + j + kCoefLead);
       }
       if (!ok) break;
     }
@@ -564,7 +574,21 @@ static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int
   }
 }
 
-static TmaGeom batch_dgeom(const GridImpl *g) {
+// Planes per item. 64 when the kind's members together give enough items
+// per step for several waves of CTAs (long items, few halo planes);
+// otherwise each member takes the longest z chunk (32 or 16) that cuts one
+// of its steps into that many items, so a few large members are not
+// quantised into a fraction of a wave at every step.
+static int64_t items_target() { return (int64_t)rt().sm_count * 6; }
+
+static int pick_zchunk(int64_t tiles_xy, int nz, bool short_chunks) {
+  if (!short_chunks) return 64;
+  for (int zc = 64; zc > 16; zc >>= 1)
+    if (tiles_xy * ((nz + zc - 1) / zc) >= items_target()) return zc;
+  return 16;
+}
+
+static TmaGeom batch_dgeom(const GridImpl *g, bool short_chunks) {
   TmaGeom geo;
   pick_shape(g->pub.dim[0], g->pub.dim[1], kVY, &geo.tx_threads, &geo.ty_threads);
   const int TX = geo.tx_threads * 4, TY = geo.ty_threads * kVY;
@@ -576,13 +600,13 @@ static TmaGeom batch_dgeom(const GridImpl *g) {
   geo.x_base = 0;
   geo.tiles_x = (g->pub.dim[0] + TX - 1) / TX;
   geo.tiles_y = (g->pub.dim[1] + TY - 1) / TY;
-  geo.zchunk = 64;
+  geo.zchunk = pick_zchunk((int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2], short_chunks);
   geo.stages = kBStages;
   geo.stage_bytes = kind_stage_bytes(0);
   return geo;
 }
 
-static HimenoGeom batch_hgeom(const GridImpl *g) {
+static HimenoGeom batch_hgeom(const GridImpl *g, bool short_chunks) {
   HimenoGeom geo;
   // interior domain [1, n-1): tiles start at x = 0 (x_base), y = 1.
   pick_shape(g->pub.dim[0] - 1, g->pub.dim[1] - 2, 1, &geo.tx_threads, &geo.ty_threads);
@@ -595,7 +619,7 @@ static HimenoGeom batch_hgeom(const GridImpl *g) {
   geo.x_base = 0;
   geo.tiles_x = (g->pub.dim[0] - 1 + TX - 1) / TX;
   geo.tiles_y = (g->pub.dim[1] - 2 + TY - 1) / TY;
-  geo.zchunk = 64;
+  geo.zchunk = pick_zchunk((int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2] - 2, short_chunks);
   geo.stages = kBStages;
   geo.stage_bytes = kind_stage_bytes(1);
   geo.nx = g->pub.dim[0];
@@ -615,6 +639,23 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
   b->members.assign(n, BMember());
   std::vector<CUtensorMap> tmaps(2 * std::max(1, n));
   std::vector<int> coef_map(n, -1);  // index of a Himeno member's 12 coefficient maps
+  // Items per step of each kind with 64-plane chunks.
+  bool short_chunks[2];
+  {
+    int64_t items[2] = {0, 0};
+    for (int i = 0; i < n; i++) {
+      if (steps[i] <= 0) continue;
+      const GridImpl *g0 = b->hm[i].grids[0];
+      if (b->hm[i].kind == BK_HIMENO) {
+        const HimenoGeom hg = batch_hgeom(g0, false);
+        items[1] += (int64_t)hg.tiles_x * hg.tiles_y * ((g0->pub.dim[2] - 2 + 63) / 64);
+      } else {
+        const TmaGeom dg = batch_dgeom(g0, false);
+        items[0] += (int64_t)dg.tiles_x * dg.tiles_y * ((g0->pub.dim[2] + 63) / 64);
+      }
+    }
+    for (int k = 0; k < 2; k++) short_chunks[k] = items[k] < items_target();
+  }
   int64_t partial_slots = 0;
   for (int i = 0; i < n; i++) {
     const BatchMemberHost &h = b->hm[i];
@@ -633,7 +674,7 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     M.sz = g0->sz;
     const CUtensorMap *a = nullptr, *c = nullptr;
     if (h.kind == BK_HIMENO) {
-      M.hg = batch_hgeom(g0);
+      M.hg = batch_hgeom(g0, short_chunks[1]);
       for (int k = 0; k < 3; k++) {
         M.dom.lo[k] = 1;
         M.dom.hi[k] = g0->pub.dim[k] - 1;
@@ -652,7 +693,7 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
         tmaps.push_back(*cm);
       }
     } else {
-      M.dg = batch_dgeom(g0);
+      M.dg = batch_dgeom(g0, short_chunks[0]);
       for (int k = 0; k < 3; k++) {
         M.dom.lo[k] = 0;
         M.dom.hi[k] = g0->pub.dim[k];
