@@ -74,19 +74,20 @@ __host__ __device__ constexpr int kind_stage_bytes(int group) {
               stage_bytes_of(8, 16, group == 0 ? kVY : 1));
 }
 
+// Himeno items also stream their twelve coefficient tiles by TMA: a second
+// ring, one stage per output plane holding field i at i * kCoefTileBytes
+// (every tile shape covers 512 points).
+constexpr int kCoefTileBytes = 512 * 4;
+constexpr int kCoefStageBytes = 12 * kCoefTileBytes;
+constexpr int kCStages = 3;
+
 // Shared memory of the batched kernel (bytes from the 128-aligned base):
-// ring barriers full[32] at 0 and empty[32] at 256, item queue barriers at
-// 512 (qfull) and 544 (qempty), item descriptors (kQ x 112 bytes) at 576,
-// stages from 1024.
+// plane ring barriers full[32] at 0 and empty[32] at 256, item queue
+// barriers at 512 (qfull) and 544 (qempty), coefficient ring barriers at 576
+// (full) and 640 (empty), item descriptors (kQ x 16 bytes) at 704, plane
+// stages from 1280, then (Himeno) the coefficient stages.
 constexpr int kQ = 4;  // item descriptors in flight between producer and consumers
-#ifndef PSB_COEF_LEAD
-#define PSB_COEF_LEAD 0
-#endif
-// Himeno coefficient planes are brought into L2 this many planes ahead of
-// the p plane being issued (which itself runs up to kBStages planes ahead
-// of the consumers).
-constexpr int kCoefLead = PSB_COEF_LEAD;
-constexpr int kSmemRing = 1024;
+constexpr int kSmemRing = 1280;
 
 struct BMember {
   int kind;
@@ -124,16 +125,12 @@ struct BatchDev {
   int *err;
 };
 
-// An item handed from the producer thread to the consumer warps. Himeno
-// items carry their member's coefficient field origins, which the consumers
-// read from shared memory on every plane instead of holding 12 pointers in
-// registers.
+// An item handed from the producer thread to the consumer warps.
 struct ItemDesc {
   int m, s, t, flags;
-  const float *cf[12];
 };
 enum { kItemEnd = 1, kItemSkip = 2 };
-static_assert(576 + kQ * sizeof(ItemDesc) <= kSmemRing, "item descriptors overlap the ring");
+static_assert(704 + kQ * sizeof(ItemDesc) <= kSmemRing, "item descriptors overlap the ring");
 
 __device__ __forceinline__ int upper_index(const int64_t *a, int n, int64_t v) {
   // largest i in [0, n) with a[i] <= v (a non-decreasing, a[0] = 0)
@@ -188,15 +185,120 @@ __device__ __forceinline__ ItemGeom item_geom(const BMember &M, int t) {
   return g;
 }
 
+// Coefficient tiles of output plane z (tensor coordinates) into the next
+// stage of ring RC: twelve TMA loads completing on one barrier.
+__device__ __forceinline__ bool coef_produce(const Ring &RC, RingPos &p, const CUtensorMap *tcoef,
+                                             int cx, int cy, int cz) {
+  if (p.round > 0 && !mbar_wait_bounded(&RC.empty[p.slot], (p.round - 1) & 1)) return false;
+  mbar_arrive_expect_tx(&RC.full[p.slot], (uint32_t)kCoefStageBytes);
+  unsigned char *dst = RC.base + p.slot * RC.stage_bytes;
+  for (int f = 0; f < 12; f++)
+    tma_load_3d(dst + f * kCoefTileBytes, tcoef + f, &RC.full[p.slot], cx, cy, cz);
+  ring_next(p, RC.S);
+  return true;
+}
+
+// Consumer warps, one Himeno tile with staged coefficients: planes zb-1 ..
+// zb+nzl of p through ring R (as himeno_consume), and for each output plane
+// one stage of ring RC holding its twelve coefficient tiles (rows of TX
+// floats). Both rings are advanced past the tile, every stage released.
+__device__ __forceinline__ bool himeno_consume_staged(const Ring &R, RingPos &p, const Ring &RC,
+                                                      RingPos &pcoef, float *pout, int64_t sy,
+                                                      int64_t sz, const Dom3 d, float omega,
+                                                      const HimenoGeom geo, int x0, int y0,
+                                                      int zb, int nzl, double *acc_out) {
+  constexpr int V = 4;
+  const int S = R.S;
+  const int tid = threadIdx.x;
+  const int tx = tid % geo.tx_threads, ty = tid / geo.tx_threads;
+  const int lane = tid & 31;
+  const int BX = geo.bx;
+  const int rc = (ty + 1) * BX + V + tx * V;
+  const int co_off = (ty * geo.tx_threads * V + tx * V) * 4;  // bytes into a coefficient tile
+  const int xg0 = x0 + tx * V;
+  const int yg = y0 + ty;
+  const bool row_in = yg >= d.lo[1] && yg < d.hi[1];
+  const bool xvec = xg0 >= d.lo[0] && xg0 + V <= d.hi[0];
+  auto wait_stage = [&](const Ring &Q, const RingPos &q) -> bool {
+    bool ok = mbar_wait_bounded(&Q.full[q.slot], q.round & 1);
+    return __all_sync(0xffffffffu, ok);
+  };
+  auto release = [&](const Ring &Q, int slot) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&Q.empty[slot]);
+  };
+  auto plane_ptr = [&](int slot) -> const float * {
+    return reinterpret_cast<const float *>(R.base + slot * R.stage_bytes);
+  };
+  double acc = 0.0;
+  RingPos pm = p;  // plane z-1
+  RingPos pc = p;  // plane z
+  ring_next(pc, S);
+  RingPos pp = pc;  // plane z+1 (advanced before use)
+  bool bad = !wait_stage(R, pm);
+  bad = bad || !wait_stage(R, pc);
+  int64_t off = (int64_t)xg0 + (int64_t)yg * sy + (int64_t)zb * sz;
+  for (int jj = 0; jj < nzl && !bad; jj++) {
+    ring_next(pp, S);
+    if (!wait_stage(R, pp) || !wait_stage(RC, pcoef)) {
+      bad = true;
+      break;
+    }
+    const float *qm = plane_ptr(pm.slot), *qc = plane_ptr(pc.slot), *qp = plane_ptr(pp.slot);
+    if (row_in) {
+      const unsigned char *cs = RC.base + pcoef.slot * RC.stage_bytes + co_off;
+      Vec16<float> co[12];
+#pragma unroll
+      for (int i = 0; i < 12; i++)
+        co[i] = lds16(reinterpret_cast<const float *>(cs + i * kCoefTileBytes));
+      float outv[V];
+#pragma unroll
+      for (int v = 0; v < V; v++) {
+        const int o = rc + v;
+        float c[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) c[i] = co[i].v[v];
+        float ss;
+        outv[v] = himeno_point(c, qc[o], qc[o + 1], qc[o - 1], qc[o + BX], qc[o - BX], qp[o],
+                               qm[o], qp[o + BX], qp[o - BX], qm[o + BX], qm[o - BX],
+                               qc[o + 1 + BX], qc[o + 1 - BX], qc[o - 1 + BX], qc[o - 1 - BX],
+                               qp[o + 1], qm[o + 1], qp[o - 1], qm[o - 1], omega, &ss);
+        if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) acc += (double)ss * (double)ss;
+      }
+      float *dst = pout + off;
+      if (xvec) {
+        *reinterpret_cast<float4 *>(dst) = make_float4(outv[0], outv[1], outv[2], outv[3]);
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; v++)
+          if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) dst[v] = outv[v];
+      }
+    }
+    release(RC, pcoef.slot);
+    ring_next(pcoef, RC.S);
+    release(R, pm.slot);  // plane z-1 is done for this warp
+    pm = pc;
+    pc = pp;
+    off += sz;
+  }
+  *acc_out += acc;
+  if (bad) return false;
+  release(R, pm.slot);
+  release(R, pc.slot);
+  p = pc;
+  ring_next(p, S);
+  return true;
+}
+
 // Producer thread: takes items (from the shared cursor, or item `blockIdx.x`
 // of `step` when step >= 0), waits until the item's member has completed
 // its previous step, hands the item to the consumers through the descriptor
 // queue and streams its input planes into the ring. It runs ahead of the
 // consumers by up to the ring's depth, across item boundaries.
 template <int GROUP>
-__device__ void batch_produce(const BatchDev &B, int step, const Ring &R, uint64_t *qfull,
-                              uint64_t *qempty, ItemDesc *desc) {
-  RingPos pos{0, 0};
+__device__ void batch_produce(const BatchDev &B, int step, const Ring &R, const Ring &RC,
+                              uint64_t *qfull, uint64_t *qempty, ItemDesc *desc) {
+  RingPos pos{0, 0}, cpos{0, 0};
   bool ok = true;
   for (uint32_t nq = 0;; nq++) {
     long long item;
@@ -245,8 +347,6 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, uint64
     desc[q].s = s;
     desc[q].t = t;
     desc[q].flags = flags;
-    if (GROUP == 1 && !(flags & (kItemEnd | kItemSkip)))
-      for (int i = 0; i < 12; i++) desc[q].cf[i] = M->cf.f[i];
     mbar_arrive(&qfull[q]);  // release: the descriptor is visible to the consumers
     if (flags & kItemEnd) break;
     if (flags & kItemSkip) continue;
@@ -267,20 +367,16 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, uint64
         break;
       }
     } else {
-      // Himeno: with each plane of p, bring the twelve coefficient planes of
-      // the same z into L2. The consumers load them one plane at a time
-      // (registers hold one plane's coefficients); coming from L2 instead of
-      // DRAM their latency no longer limits the sweep.
-      auto prefetch = [&](int z) {
-        if (z >= g.zb && z < g.zb + g.nzl)
-          for (int f = 0; f < 12; f++)
-            tma_prefetch_l2_3d(M->tcoef + f, g.x0 + ax0, g.y0 + ay0, z + az0);
-      };
-      for (int z = g.zb; z < g.zb - 1 + kCoefLead; z++) prefetch(z);
+      // Himeno: after each plane of p that is also an output plane, the
+      // twelve coefficient tiles of that plane into the coefficient ring
+      // (the order the consumers need them in, so neither ring can wait on
+      // a stage of the other that is not yet issued).
       for (int j = 0; j < g.nzl + 2 && ok; j++) {
+        const int z = g.zb - 1 + j;
         ok = ring_produce(R, pos, M->tmap[par], (uint32_t)(bx * by * 4), g.x0 - 4 + ax0,
-                          g.y0 - 1 + ay0, g.zb - 1 + j + az0, 1);
-        if (ok) prefetch(g.zb - 1 + j + kCoefLead);
+                          g.y0 - 1 + ay0, z + az0, 1);
+        if (ok && z >= g.zb && z < g.zb + g.nzl)
+          ok = coef_produce(RC, cpos, M->tcoef, g.x0 + ax0, g.y0 + ay0, z + az0);
       }
       if (!ok) break;
     }
@@ -288,6 +384,7 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, uint64
   if (!ok) {
     atomicExch(B.err, 1);
     ring_drain(R, pos);
+    if (GROUP == 1) ring_drain(RC, cpos);
   }
 }
 
@@ -356,12 +453,11 @@ __device__ __forceinline__ void item_done(const BMember &M, int s, int t, int wa
 }
 
 // Consumer warps: take item after item from the descriptor queue and run
-// the tile's computation from the ring. A descriptor slot is released when
-// the item is done (Himeno items read their coefficient origins from it).
+// the tile's computation from the rings.
 template <int GROUP>
-__device__ void batch_consume(const BatchDev &B, const Ring &R, uint64_t *qfull, uint64_t *qempty,
-                              const ItemDesc *desc) {
-  RingPos pos{0, 0};
+__device__ void batch_consume(const BatchDev &B, const Ring &R, const Ring &RC, uint64_t *qfull,
+                              uint64_t *qempty, const ItemDesc *desc) {
+  RingPos pos{0, 0}, cpos{0, 0};
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (uint32_t nq = 0;; nq++) {
     const int q = nq % kQ;
@@ -379,6 +475,8 @@ __device__ void batch_consume(const BatchDev &B, const Ring &R, uint64_t *qfull,
     const BMember &M = B.members[dm];
     const bool skip = (dflags & kItemSkip) != 0;
     const int par = (M.step0 + ds) & 1;
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&qempty[q]);
     const int gstep = M.step0 + ds;
     const bool check = M.check_every > 0 &&
                        ((gstep + 1) % M.check_every == 0 || (GROUP == 1 && gstep == 0));
@@ -387,10 +485,8 @@ __device__ void batch_consume(const BatchDev &B, const Ring &R, uint64_t *qfull,
       const ItemGeom g = item_geom<GROUP>(M, dt);
       bool ok;
       if constexpr (GROUP == 1) {
-        const float *const *cf = desc[q].cf;
-        ok = himeno_consume(R, pos, (float *)M.buf[par ^ 1].origin,
-                            [&](int i) { return cf[i]; }, M.sy, M.sz, M.dom, M.omega, M.hg,
-                            g.x0, g.y0, g.zb, g.nzl, &a);
+        ok = himeno_consume_staged(R, pos, RC, cpos, (float *)M.buf[par ^ 1].origin, M.sy, M.sz,
+                                   M.dom, M.omega, M.hg, g.x0, g.y0, g.zb, g.nzl, &a);
       } else {
         TileAcc acc{0, 0};
         const GridView out = M.buf[par ^ 1];
@@ -417,8 +513,6 @@ __device__ void batch_consume(const BatchDev &B, const Ring &R, uint64_t *qfull,
         return;
       }
     }
-    __syncwarp();
-    if (lane == 0) mbar_arrive(&qempty[q]);
     item_done<GROUP>(M, ds, dt, warp, lane, check, check && !skip, a, b);
   }
 }
@@ -430,22 +524,21 @@ __device__ __forceinline__ unsigned char *aligned_smem(unsigned char *raw) {
 // The batched kernel of one stencil kind. step < 0: persistent -- each CTA
 // takes items from the kind's work list until it is exhausted (mode 0).
 // step >= 0: one item per CTA, item blockIdx.x of that step (mode 1, one
-// launch per step). Both kinds fit the register budget of 3 CTAs per SM
-// without spills.
-#ifndef PSB_BATCH_HIMENO_CTAS
-#define PSB_BATCH_HIMENO_CTAS 3
-#endif
+// launch per step). Diffusion items run 3 CTAs per SM; Himeno items, whose
+// CTAs also hold three stages of coefficient tiles (72 KB), run 2.
 template <int GROUP>
-__global__ void __launch_bounds__(kBThreads, GROUP == 0 ? 3 : PSB_BATCH_HIMENO_CTAS)
-    k_batch(BatchDev B, int step) {
+__global__ void __launch_bounds__(kBThreads, GROUP == 0 ? 3 : 2) k_batch(BatchDev B, int step) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   unsigned char *smem = aligned_smem(smem_raw);
   uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
   uint64_t *qfull = bars + 64, *qempty = bars + 68;
-  ItemDesc *desc = reinterpret_cast<ItemDesc *>(smem + 576);
+  ItemDesc *desc = reinterpret_cast<ItemDesc *>(smem + 704);
   const Ring R{bars, bars + 32, smem + kSmemRing, kBStages, kind_stage_bytes(GROUP)};
+  const Ring RC{bars + 72, bars + 80, smem + kSmemRing + kBStages * kind_stage_bytes(GROUP),
+                kCStages, kCoefStageBytes};
   if (threadIdx.x == 0) {
     ring_init(R, kBWarps);
+    if (GROUP == 1) ring_init(RC, kBWarps);
     for (int q = 0; q < kQ; q++) {
       mbar_init(&qfull[q], 1);
       mbar_init(&qempty[q], kBWarps);
@@ -454,10 +547,10 @@ __global__ void __launch_bounds__(kBThreads, GROUP == 0 ? 3 : PSB_BATCH_HIMENO_C
   }
   __syncthreads();
   if (threadIdx.x >= kBConsumers) {
-    if (threadIdx.x == kBConsumers) batch_produce<GROUP>(B, step, R, qfull, qempty, desc);
+    if (threadIdx.x == kBConsumers) batch_produce<GROUP>(B, step, R, RC, qfull, qempty, desc);
     return;
   }
-  batch_consume<GROUP>(B, R, qfull, qempty, desc);
+  batch_consume<GROUP>(B, R, RC, qfull, qempty, desc);
 }
 
 }  // namespace psb
@@ -627,7 +720,8 @@ static HimenoGeom batch_hgeom(const GridImpl *g, bool short_chunks) {
 }
 
 static size_t batch_smem(int group) {
-  return 128 + kSmemRing + (size_t)kBStages * kind_stage_bytes(group);
+  return 128 + kSmemRing + (size_t)kBStages * kind_stage_bytes(group) +
+         (group == 1 ? (size_t)kCStages * kCoefStageBytes : 0);
 }
 
 // Build the device work lists and member descriptors for one launch in which
@@ -785,6 +879,8 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     } else {
       PSB_TRY(cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
+      PSB_TRY(cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)batch_smem(1)));
       PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<1>, kBThreads,
                                                             batch_smem(1)));
     }
