@@ -159,6 +159,113 @@ __device__ __forceinline__ bool himeno_consume(const Ring &R, RingPos &p, float 
   return true;
 }
 
+// Coefficient tiles of output plane z (tensor coordinates) into the next
+// stage of ring RC: twelve TMA loads (maps tcoef[f * stride], boxes of
+// tile_bytes) completing on one barrier, field f at f * tile_bytes.
+__device__ __forceinline__ bool coef_produce(const Ring &RC, RingPos &p, const CUtensorMap *tcoef,
+                                             int stride, int tile_bytes, int cx, int cy, int cz) {
+  if (p.round > 0 && !mbar_wait_bounded(&RC.empty[p.slot], (p.round - 1) & 1)) return false;
+  mbar_arrive_expect_tx(&RC.full[p.slot], (uint32_t)(12 * tile_bytes));
+  unsigned char *dst = RC.base + p.slot * RC.stage_bytes;
+  for (int f = 0; f < 12; f++)
+    tma_load_3d(dst + f * tile_bytes, tcoef + f * stride, &RC.full[p.slot], cx, cy, cz);
+  ring_next(p, RC.S);
+  return true;
+}
+
+// Consumer warps, one Himeno tile with staged coefficients: planes zb-1 ..
+// zb+nzl of p through ring R (as himeno_consume), and for each output plane
+// one stage of ring RC holding its twelve coefficient tiles (rows of TX
+// floats). Both rings are advanced past the tile, every stage released.
+__device__ __forceinline__ bool himeno_consume_staged(const Ring &R, RingPos &p, const Ring &RC,
+                                                      RingPos &pcoef, int tile_bytes, float *pout,
+                                                      int64_t sy,
+                                                      int64_t sz, const Dom3 d, float omega,
+                                                      const HimenoGeom geo, int x0, int y0,
+                                                      int zb, int nzl, double *acc_out) {
+  constexpr int V = 4;
+  const int S = R.S;
+  const int tid = threadIdx.x;
+  const int tx = tid % geo.tx_threads, ty = tid / geo.tx_threads;
+  const int lane = tid & 31;
+  const int BX = geo.bx;
+  const int rc = (ty + 1) * BX + V + tx * V;
+  const int co_off = (ty * geo.tx_threads * V + tx * V) * 4;  // bytes into a coefficient tile
+  const int xg0 = x0 + tx * V;
+  const int yg = y0 + ty;
+  const bool row_in = yg >= d.lo[1] && yg < d.hi[1];
+  const bool xvec = xg0 >= d.lo[0] && xg0 + V <= d.hi[0];
+  auto wait_stage = [&](const Ring &Q, const RingPos &q) -> bool {
+    bool ok = mbar_wait_bounded(&Q.full[q.slot], q.round & 1);
+    return __all_sync(0xffffffffu, ok);
+  };
+  auto release = [&](const Ring &Q, int slot) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&Q.empty[slot]);
+  };
+  auto plane_ptr = [&](int slot) -> const float * {
+    return reinterpret_cast<const float *>(R.base + slot * R.stage_bytes);
+  };
+  double acc = 0.0;
+  RingPos pm = p;  // plane z-1
+  RingPos pc = p;  // plane z
+  ring_next(pc, S);
+  RingPos pp = pc;  // plane z+1 (advanced before use)
+  bool bad = !wait_stage(R, pm);
+  bad = bad || !wait_stage(R, pc);
+  int64_t off = (int64_t)xg0 + (int64_t)yg * sy + (int64_t)zb * sz;
+  for (int jj = 0; jj < nzl && !bad; jj++) {
+    ring_next(pp, S);
+    if (!wait_stage(R, pp) || !wait_stage(RC, pcoef)) {
+      bad = true;
+      break;
+    }
+    const float *qm = plane_ptr(pm.slot), *qc = plane_ptr(pc.slot), *qp = plane_ptr(pp.slot);
+    if (row_in) {
+      const unsigned char *cs = RC.base + pcoef.slot * RC.stage_bytes + co_off;
+      Vec16<float> co[12];
+#pragma unroll
+      for (int i = 0; i < 12; i++)
+        co[i] = lds16(reinterpret_cast<const float *>(cs + i * tile_bytes));
+      float outv[V];
+#pragma unroll
+      for (int v = 0; v < V; v++) {
+        const int o = rc + v;
+        float c[12];
+#pragma unroll
+        for (int i = 0; i < 12; i++) c[i] = co[i].v[v];
+        float ss;
+        outv[v] = himeno_point(c, qc[o], qc[o + 1], qc[o - 1], qc[o + BX], qc[o - BX], qp[o],
+                               qm[o], qp[o + BX], qp[o - BX], qm[o + BX], qm[o - BX],
+                               qc[o + 1 + BX], qc[o + 1 - BX], qc[o - 1 + BX], qc[o - 1 - BX],
+                               qp[o + 1], qm[o + 1], qp[o - 1], qm[o - 1], omega, &ss);
+        if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) acc += (double)ss * (double)ss;
+      }
+      float *dst = pout + off;
+      if (xvec) {
+        *reinterpret_cast<float4 *>(dst) = make_float4(outv[0], outv[1], outv[2], outv[3]);
+      } else {
+#pragma unroll
+        for (int v = 0; v < V; v++)
+          if (xg0 + v >= d.lo[0] && xg0 + v < d.hi[0]) dst[v] = outv[v];
+      }
+    }
+    release(RC, pcoef.slot);
+    ring_next(pcoef, RC.S);
+    release(R, pm.slot);  // plane z-1 is done for this warp
+    pm = pc;
+    pc = pp;
+    off += sz;
+  }
+  *acc_out += acc;
+  if (bad) return false;
+  release(R, pm.slot);
+  release(R, pc.slot);
+  p = pc;
+  ring_next(p, S);
+  return true;
+}
+
 // One tile of a Himeno sweep as a whole CTA (single-grid kernels): the
 // (TX x TY) column at (tile_x, tile_y) over z chunk zc. `smem` is the CTA's
 // 128-byte aligned dynamic shared memory. Consumer threads add sum(ss*ss) of
