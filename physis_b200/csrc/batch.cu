@@ -52,31 +52,32 @@ constexpr int kBWarps = kBConsumers / 32;
 constexpr int kBThreads = kBConsumers + 32;
 constexpr int kBStages = 6;
 
-// Tile shapes of batched items: 128 consumer threads as 16 x 8, 32 x 4 or
-// 8 x 16 (x threads of 4 floats each x rows); kind_stage_bytes lists them
-// too. Ties go to the earlier shape.
-constexpr int kBShapes[3][2] = {{16, 8}, {32, 4}, {8, 16}};
+// Tile shapes of batched items: t consumer threads along x (4 floats each,
+// t = kMinTx .. kMaxTx) by floor(128 / t) thread rows; threads past
+// t * floor(128 / t) idle. Each member takes the t that covers its x-y
+// extent with the fewest tiles, so narrow grids waste few threads on
+// partial tiles (a 50-wide grid uses t = 13, 52 points).
+constexpr int kMinTx = 8, kMaxTx = 32;
 
 __host__ __device__ constexpr int stage_bytes_of(int tx_threads, int ty_threads,
                                                  int rows_per_thread) {
   return ((tx_threads * 4 + 8) * (ty_threads * rows_per_thread + 2) * 4 + 127) / 128 * 128;
 }
 
-__host__ __device__ constexpr int max3(int a, int b, int c) {
-  return a > b ? (a > c ? a : c) : (b > c ? b : c);
-}
-
 // One ring stride per kernel kind (the largest stage of its shapes): the
 // planes of differently shaped tiles follow each other through one ring.
 __host__ __device__ constexpr int kind_stage_bytes(int group) {
-  return max3(stage_bytes_of(16, 8, group == 0 ? kVY : 1),
-              stage_bytes_of(32, 4, group == 0 ? kVY : 1),
-              stage_bytes_of(8, 16, group == 0 ? kVY : 1));
+  int m = 0;
+  for (int t = kMinTx; t <= kMaxTx; t++) {
+    const int b = stage_bytes_of(t, kBConsumers / t, group == 0 ? kVY : 1);
+    m = b > m ? b : m;
+  }
+  return m;
 }
 
 // Himeno items also stream their twelve coefficient tiles by TMA: a second
 // ring, one stage per output plane holding field i at i * kCoefTileBytes
-// (every tile shape covers 512 points).
+// (no tile shape covers more than 512 points).
 constexpr int kCoefTileBytes = 512 * 4;
 constexpr int kCoefStageBytes = 12 * kCoefTileBytes;
 constexpr int kCStages = 3;
@@ -271,7 +272,8 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, const 
         ok = ring_produce(R, pos, M->tmap[par], (uint32_t)(bx * by * 4), g.x0 - 4 + ax0,
                           g.y0 - 1 + ay0, z + az0, 1);
         if (ok && z >= g.zb && z < g.zb + g.nzl)
-          ok = coef_produce(RC, cpos, M->tcoef, 1, kCoefTileBytes, g.x0 + ax0, g.y0 + ay0,
+          ok = coef_produce(RC, cpos, M->tcoef, 1, kCoefTileBytes,
+                            M->hg.tx_threads * 4 * M->hg.ty_threads * 4, g.x0 + ax0, g.y0 + ay0,
                             z + az0);
       }
       if (!ok) break;
@@ -548,17 +550,32 @@ static psb_status dev_reserve(T **p, size_t *cap, size_t bytes) {
 // Each member takes the tile shape with the fewest tiles over its x-y
 // extent (then the fewest box elements), so small and narrow members waste
 // few threads on partial tiles.
+#ifndef PSB_PROMO_P
+#define PSB_PROMO_P CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+#endif
+#ifndef PSB_PROMO_C
+#define PSB_PROMO_C CU_TENSOR_MAP_L2_PROMOTION_L2_128B
+#endif
+#ifndef PSB_PROMO_D
+#define PSB_PROMO_D CU_TENSOR_MAP_L2_PROMOTION_L2_256B
+#endif
+// L2 promotion of the batched kernels' tensor maps. Coefficient tiles start
+// 128 bytes into a 256-byte line, so promoting their rows to 256 bytes
+// fetches lines that small members never use (measured: 128-byte
+// promotion is up to 14% faster on small Himeno members).
+static const int kPromoP = PSB_PROMO_P, kPromoC = PSB_PROMO_C, kPromoD = PSB_PROMO_D;
+
 static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int *ty_threads) {
   int64_t best_tiles = -1, best_box = 0;
-  for (const auto &sh : kBShapes) {
-    const int TX = sh[0] * 4, TY = sh[1] * rows_per_thread;
+  for (int t = kMinTx; t <= kMaxTx; t++) {
+    const int TX = t * 4, TY = (kBConsumers / t) * rows_per_thread;
     const int64_t tiles = (int64_t)((nx + TX - 1) / TX) * ((ny + TY - 1) / TY);
     const int64_t box = tiles * (TX + 8) * (TY + 2);
     if (best_tiles < 0 || tiles < best_tiles || (tiles == best_tiles && box < best_box)) {
       best_tiles = tiles;
       best_box = box;
-      *tx_threads = sh[0];
-      *ty_threads = sh[1];
+      *tx_threads = t;
+      *ty_threads = kBConsumers / t;
     }
   }
 }
@@ -674,12 +691,12 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
       M.nzc = (g0->pub.dim[2] - 2 + M.hg.zchunk - 1) / M.hg.zchunk;
       M.omega = (float)h.params[0];
       for (int k = 0; k < 12; k++) M.cf.f[k] = (const float *)h.grids[2 + k]->view().origin;
-      PSB_CHECK(get_tmap(g0, M.hg.bx, M.hg.by, &a));
-      PSB_CHECK(get_tmap(g1, M.hg.bx, M.hg.by, &c));
+      PSB_CHECK(get_tmap(g0, M.hg.bx, M.hg.by, &a, kPromoP));
+      PSB_CHECK(get_tmap(g1, M.hg.bx, M.hg.by, &c, kPromoP));
       coef_map[i] = (int)tmaps.size();
       for (int k = 0; k < 12; k++) {
         const CUtensorMap *cm = nullptr;
-        PSB_CHECK(get_tmap(h.grids[2 + k], M.hg.tx_threads * 4, M.hg.ty_threads, &cm));
+        PSB_CHECK(get_tmap(h.grids[2 + k], M.hg.tx_threads * 4, M.hg.ty_threads, &cm, kPromoC));
         tmaps.push_back(*cm);
       }
     } else {
@@ -698,8 +715,8 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
       M.k7.ct = (float)h.params[4];
       M.k7.cb = (float)h.params[5];
       M.k7.cc = (float)h.params[6];
-      PSB_CHECK(get_tmap(g0, M.dg.bx, M.dg.by, &a));
-      PSB_CHECK(get_tmap(g1, M.dg.bx, M.dg.by, &c));
+      PSB_CHECK(get_tmap(g0, M.dg.bx, M.dg.by, &a, kPromoD));
+      PSB_CHECK(get_tmap(g1, M.dg.bx, M.dg.by, &c, kPromoD));
     }
     tmaps[2 * i] = *a;
     tmaps[2 * i + 1] = *c;

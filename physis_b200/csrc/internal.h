@@ -155,7 +155,10 @@ int type_from_size(int elm_size);  // float for 4, double for 8
 // TMA descriptor of a 3-D (or lower) grid, box (bx, by, 1). Coordinates used
 // by kernels are relative to the allocation for pitched grids (origin at
 // (pad_left, halo, halo)) and to the logical origin for dense grids.
-psb_status get_tmap(GridImpl *g, int bx, int by, const CUtensorMap **out);
+// l2_promotion: a CUtensorMapL2promotion (how much L2 fetches around each
+// box row); boxes whose rows are not 256-byte aligned may want less.
+psb_status get_tmap(GridImpl *g, int bx, int by, const CUtensorMap **out,
+                    int l2_promotion = CU_TENSOR_MAP_L2_PROMOTION_L2_256B);
 bool tma_eligible(const GridImpl *g);
 
 // Stencil launches (one application of map m on the runtime stream).

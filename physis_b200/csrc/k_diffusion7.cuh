@@ -172,7 +172,11 @@ __device__ __forceinline__ bool diff7_consume(const Ring &R, RingPos &p, const G
   constexpr int VY = kVY;
   const int S = R.S;
   const int tid = threadIdx.x;
-  const int tx = tid % geo.tx_threads, ty = tid / geo.tx_threads;
+  // Threads past tx_threads * ty_threads (shapes that do not divide the
+  // consumer count) take part in every wait and release but own no points.
+  const int tx = tid % geo.tx_threads;
+  const bool active = tid / geo.tx_threads < geo.ty_threads;
+  const int ty = active ? tid / geo.tx_threads : geo.ty_threads - 1;
   const int lane = tid & 31;
   const int BX = geo.bx;
   const int xg0 = x0 + tx * V;
@@ -192,7 +196,7 @@ __device__ __forceinline__ bool diff7_consume(const Ring &R, RingPos &p, const G
   yedge = !PERIODIC && yedge;
   bool row_in[VY];
 #pragma unroll
-  for (int r = 0; r < VY; r++) row_in[r] = yg0 + r >= d.lo[1] && yg0 + r < d.hi[1];
+  for (int r = 0; r < VY; r++) row_in[r] = active && yg0 + r >= d.lo[1] && yg0 + r < d.hi[1];
   const bool xvec = xg0 >= d.lo[0] && xg0 + V <= d.hi[0];
   // Periodic x-face images of this thread's vector: x = 0 goes to x = nx,
   // x = nx-1 to x = -1.

@@ -161,14 +161,15 @@ __device__ __forceinline__ bool himeno_consume(const Ring &R, RingPos &p, float 
 
 // Coefficient tiles of output plane z (tensor coordinates) into the next
 // stage of ring RC: twelve TMA loads (maps tcoef[f * stride], boxes of
-// tile_bytes) completing on one barrier, field f at f * tile_bytes.
+// box_bytes) completing on one barrier, field f at f * field_bytes.
 __device__ __forceinline__ bool coef_produce(const Ring &RC, RingPos &p, const CUtensorMap *tcoef,
-                                             int stride, int tile_bytes, int cx, int cy, int cz) {
+                                             int stride, int field_bytes, int box_bytes, int cx,
+                                             int cy, int cz) {
   if (p.round > 0 && !mbar_wait_bounded(&RC.empty[p.slot], (p.round - 1) & 1)) return false;
-  mbar_arrive_expect_tx(&RC.full[p.slot], (uint32_t)(12 * tile_bytes));
+  mbar_arrive_expect_tx(&RC.full[p.slot], (uint32_t)(12 * box_bytes));
   unsigned char *dst = RC.base + p.slot * RC.stage_bytes;
   for (int f = 0; f < 12; f++)
-    tma_load_3d(dst + f * tile_bytes, tcoef + f * stride, &RC.full[p.slot], cx, cy, cz);
+    tma_load_3d(dst + f * field_bytes, tcoef + f * stride, &RC.full[p.slot], cx, cy, cz);
   ring_next(p, RC.S);
   return true;
 }
@@ -186,14 +187,18 @@ __device__ __forceinline__ bool himeno_consume_staged(const Ring &R, RingPos &p,
   constexpr int V = 4;
   const int S = R.S;
   const int tid = threadIdx.x;
-  const int tx = tid % geo.tx_threads, ty = tid / geo.tx_threads;
+  // Threads past tx_threads * ty_threads (shapes that do not divide the
+  // consumer count) take part in every wait and release but own no points.
+  const int tx = tid % geo.tx_threads;
+  const bool active = tid / geo.tx_threads < geo.ty_threads;
+  const int ty = active ? tid / geo.tx_threads : geo.ty_threads - 1;
   const int lane = tid & 31;
   const int BX = geo.bx;
   const int rc = (ty + 1) * BX + V + tx * V;
   const int co_off = (ty * geo.tx_threads * V + tx * V) * 4;  // bytes into a coefficient tile
   const int xg0 = x0 + tx * V;
   const int yg = y0 + ty;
-  const bool row_in = yg >= d.lo[1] && yg < d.hi[1];
+  const bool row_in = active && yg >= d.lo[1] && yg < d.hi[1];
   const bool xvec = xg0 >= d.lo[0] && xg0 + V <= d.hi[0];
   auto wait_stage = [&](const Ring &Q, const RingPos &q) -> bool {
     bool ok = mbar_wait_bounded(&Q.full[q.slot], q.round & 1);

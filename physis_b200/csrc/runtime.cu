@@ -376,8 +376,8 @@ bool tma_eligible(const GridImpl *g) {
   return true;
 }
 
-psb_status get_tmap(GridImpl *g, int bx, int by, const CUtensorMap **out) {
-  uint64_t key = ((uint64_t)bx << 32) | (uint32_t)by;
+psb_status get_tmap(GridImpl *g, int bx, int by, const CUtensorMap **out, int l2_promotion) {
+  uint64_t key = ((uint64_t)l2_promotion << 48) | ((uint64_t)bx << 24) | (uint32_t)by;
   auto it = g->tmaps.find(key);
   if (it != g->tmaps.end()) {
     *out = &it->second;
@@ -401,7 +401,7 @@ psb_status get_tmap(GridImpl *g, int bx, int by, const CUtensorMap **out) {
   // The whole allocation is described; kernels address it in allocation
   // coordinates (logical + (pad_left, halo, halo)).
   CUresult res = fn(&m, dt, 3, g->alloc, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_SWIZZLE_NONE, (CUtensorMapL2promotion)l2_promotion,
                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (res != CUDA_SUCCESS) return set_status(PSB_ERR_UNSUPPORTED);
   auto ins = g->tmaps.emplace(key, m);
