@@ -463,6 +463,14 @@ def c4_batch(ps, members, grids):
     return b
 
 
+def c4_traffic(alg_bytes):
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return alg_bytes * float(json.load(f)["k_batch_c4_traffic_per_algorithmic_byte"])
+    except Exception:
+        return None
+
+
 def c4_e2e(ps, members, grids, b, lups, dist, reps=2):
     """The batch through the public API with host buffers: every member's
     input grids (7-point: the field; Himeno: both p grids and the twelve
@@ -575,8 +583,11 @@ def run_c4(args, dist):
         },
         "roofline": {"bound": "hbm", "achieved": alg_bytes / per_run_s / 1e9, "peak": peaks()[0],
                      "unit": "GB/s", "frac": alg_bytes / per_run_s / 1e9 / peaks()[0],
-                     "traffic": None, "algorithmic_bytes_per_launch": alg_bytes,
-                     "avg_launch_us": per_run_s * 1e6},
+                     "traffic": c4_traffic(alg_bytes), "algorithmic_bytes_per_launch": alg_bytes,
+                     "avg_launch_us": per_run_s * 1e6,
+                     "launch": "one run of the batch: the two kinds' persistent k_batch launches",
+                     "traffic_note": "scaled from an ncu capture of the first 32 members "
+                                     "(DRAM bytes per algorithmic byte)"},
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clocks,
