@@ -182,6 +182,125 @@ static psb_status launch_tma(MapImpl &m, const psb_tune_config &cfg, cudaStream_
   return PSB_OK;
 }
 
+// --------------------------------------------------------------------------
+// Temporal blocking (two steps per launch), persistent: one CTA per SM
+// walks the (tile, z chunk) items blockIdx.x, blockIdx.x + gridDim.x, ...;
+// its three rings carry on from item to item.
+// --------------------------------------------------------------------------
+constexpr int kTbS1 = 6, kTbS2 = 4;  // stages of the input and intermediate rings
+constexpr int kTbStage1 = (kTbBX1 * kTbBY1 * 4 + 127) / 128 * 128;
+constexpr int kTbStage2 = (kTbBX2 * kTbBY2 * 4 + 127) / 128 * 128;
+constexpr int kTbSmem = 128 + 512 + kTbS1 * kTbStage1 + kTbS2 * kTbStage2;
+
+struct TbGeom {
+  int ax0, ay0, az0;
+  int tiles_x, tiles_y, nzc, zchunk;
+  int64_t items;
+};
+
+__global__ void __launch_bounds__(kTbThreads, 1) k_diff7_tb2(const __grid_constant__ CUtensorMap tin,
+                                                             GridView out, int nx, int ny, int nz,
+                                                             C7<float> k, TbGeom tg, int *err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char *smem = smem_raw + ((128 - (smem_u32(smem_raw) & 127)) & 127);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  const Ring R1{bars, bars + 16, smem + 512, kTbS1, kTbStage1};
+  const Ring R2{bars + 32, bars + 48, smem + 512 + kTbS1 * kTbStage1, kTbS2, kTbStage2};
+  if (threadIdx.x == 0) {
+    ring_init(R1, kTbS1Warps);
+    for (int i = 0; i < kTbS2; i++) {
+      mbar_init(&R2.full[i], kTbS1Warps);
+      mbar_init(&R2.empty[i], kTbS2Warps);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5;
+  RingPos p1{0, 0}, p2{0, 0};
+  Dom3 d;
+  d.lo[0] = d.lo[1] = d.lo[2] = 0;
+  d.hi[0] = nx;
+  d.hi[1] = ny;
+  d.hi[2] = nz;
+  TmaGeom g2;  // the intermediate ring, as the ordinary consumer sees it
+  g2.tx_threads = 32;
+  g2.ty_threads = kTbS2Warps;
+  g2.bx = kTbBX2;
+  g2.by = kTbBY2;
+  g2.stage_bytes = kTbStage2;
+  g2.stages = kTbS2;
+  g2.ax0 = g2.ay0 = g2.az0 = 0;
+  g2.tiles_x = tg.tiles_x;
+  g2.tiles_y = tg.tiles_y;
+  g2.zchunk = tg.zchunk;
+  g2.x_base = 0;
+  for (int64_t item = blockIdx.x; item < tg.items; item += gridDim.x) {
+    int64_t t = item;
+    const int tile_x = (int)(t % tg.tiles_x);
+    t /= tg.tiles_x;
+    const int tile_y = (int)(t % tg.tiles_y);
+    const int zc = (int)(t / tg.tiles_y);
+    const int x0 = tile_x * kTbTX, y0 = tile_y * kTbTY, zb = zc * tg.zchunk;
+    const int nzl = min(zb + tg.zchunk, nz) - zb;
+    bool ok;
+    if (warp == 0) {
+      if (threadIdx.x != 0) return;
+      ok = ring_produce(R1, p1, &tin, (uint32_t)(kTbBX1 * kTbBY1 * 4), x0 - 8 + tg.ax0,
+                        y0 - 2 + tg.ay0, zb - 2 + tg.az0, nzl + 4);
+      if (!ok) {
+        atomicExch(err, 1);
+        ring_drain(R1, p1);
+        return;
+      }
+    } else if (warp <= kTbS1Warps) {
+      ok = diff7_tb_stage1(R1, p1, R2, p2, threadIdx.x - 32, nx, ny, nz, k, x0, y0, zb, nzl);
+      if (!ok) {
+        if ((threadIdx.x & 31) == 0) atomicExch(err, 1);
+        return;
+      }
+    } else {
+      ok = diff7_consume<float, false, false>(R2, p2, out, nx, ny, nz, d, k, g2, x0, y0, zb, nzl,
+                                              0, nullptr, threadIdx.x - 32 - 32 * kTbS1Warps);
+      if (!ok) {
+        if ((threadIdx.x & 31) == 0) atomicExch(err, 1);
+        return;
+      }
+    }
+  }
+}
+
+// Two steps of the clamped float 7-point map m over the whole grid: reads
+// in, writes out (the intermediate step exists only in shared memory).
+psb_status diffusion7_tb2_launch(MapImpl &m, GridImpl *in, GridImpl *out, int zchunk,
+                                 cudaStream_t s, int64_t *launches) {
+  const CUtensorMap *map = nullptr;
+  PSB_CHECK(get_tmap(in, kTbBX1, kTbBY1, &map));
+  static bool configured = false;
+  if (!configured) {
+    PSB_TRY(cudaFuncSetAttribute(k_diff7_tb2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 kTbSmem));
+    configured = true;
+  }
+  TbGeom tg;
+  tg.ax0 = in->pad_left;
+  tg.ay0 = in->halo;
+  tg.az0 = in->halo;
+  tg.tiles_x = (in->pub.dim[0] + kTbTX - 1) / kTbTX;
+  tg.tiles_y = (in->pub.dim[1] + kTbTY - 1) / kTbTY;
+  tg.zchunk = std::max(4, zchunk);
+  tg.nzc = (in->pub.dim[2] + tg.zchunk - 1) / tg.zchunk;
+  tg.items = (int64_t)tg.tiles_x * tg.tiles_y * tg.nzc;
+  C7<float> k{(float)m.params[0], (float)m.params[1], (float)m.params[2], (float)m.params[3],
+              (float)m.params[4], (float)m.params[5], (float)m.params[6]};
+  const int blocks = (int)std::min<int64_t>(rt().sm_count, tg.items);
+  k_diff7_tb2<<<blocks, kTbThreads, kTbSmem, s>>>(*map, out->view(), in->pub.dim[0],
+                                                  in->pub.dim[1], in->pub.dim[2], k, tg,
+                                                  rt().d_error);
+  (*launches)++;
+  PSB_TRY(cudaGetLastError());
+  return PSB_OK;
+}
+
 psb_status diffusion7_launch(MapImpl &m, const psb_tune_config &cfg, cudaStream_t s,
                              int64_t *launches) {
   GridImpl *gi = m.grids[0], *go = m.grids[1];

@@ -167,11 +167,14 @@ template <typename T, bool PERIODIC, bool ACC>
 __device__ __forceinline__ bool diff7_consume(const Ring &R, RingPos &p, const GridView out,
                                               int nx, int ny, int nz, const Dom3 d,
                                               const C7<T> k, const TmaGeom geo, int x0, int y0,
-                                              int zb, int nzl, int images, TileAcc *acc) {
+                                              int zb, int nzl, int images, TileAcc *acc,
+                                              int tid = -1) {
   constexpr int V = 16 / sizeof(T);
   constexpr int VY = kVY;
   const int S = R.S;
-  const int tid = threadIdx.x;
+  // tid: this thread's index among the consumer threads (whole warps; the
+  // threads of the CTA by default).
+  if (tid < 0) tid = threadIdx.x;
   // Threads past tx_threads * ty_threads (shapes that do not divide the
   // consumer count) take part in every wait and release but own no points.
   const int tx = tid % geo.tx_threads;
@@ -351,6 +354,207 @@ __device__ __forceinline__ bool diff7_consume(const Ring &R, RingPos &p, const G
   release(pt.slot);
   p = pt;
   ring_next(p, S);
+  return true;
+}
+
+// --------------------------------------------------------------------------
+// Temporal blocking, depth 2 (float, clamped faces)
+//
+// One pass advances two time steps. Per CTA: a producer thread streams input
+// planes (box 144 x 20: the 128 x 16 output tile with a 2-cell halo, x
+// rounded out to 16 bytes) into ring R1; the "stage-1" warps compute the
+// intermediate step over the tile plus a 1-cell halo (130 x 18 points, each
+// row as 32 vectors plus two edge scalars) into ring R2, whose stages have
+// exactly the layout of a 136 x 18 input box of the output tile (18 / VY1
+// stage-1 warps, VY1 rows each); eight
+// "stage-2" warps run the ordinary consumer (diff7_consume) on R2. Every
+// point of both steps is computed with the single-step arithmetic and face
+// rules, so results are bit-identical to two separate steps; intermediate
+// values outside the grid are never read (clamped faces select the point
+// itself instead).
+// --------------------------------------------------------------------------
+constexpr int kTbTX = 128, kTbTY = 16;
+constexpr int kTbBX1 = kTbTX + 16, kTbBY1 = kTbTY + 4;   // input box
+constexpr int kTbBX2 = kTbTX + 8, kTbBY2 = kTbTY + 2;    // intermediate plane
+#ifndef PSB_TB_VY1
+#define PSB_TB_VY1 2
+#endif
+constexpr int kTbVY1 = PSB_TB_VY1;                 // intermediate rows per stage-1 thread
+constexpr int kTbS1Warps = kTbBY2 / kTbVY1, kTbS2Warps = 8;
+constexpr int kTbThreads = 32 + 32 * kTbS1Warps + 32 * kTbS2Warps;
+
+// Stage 1: intermediate planes zb-1 .. zb+nzl of the tile at (x0, y0) from
+// input planes zb-2 .. zb+nzl+1 (ring R1, all released), written to ring R2
+// (this group fills its stages; the stage-2 warps release them). t1 is the
+// thread's index in the stage-1 group.
+__device__ __forceinline__ bool diff7_tb_stage1(const Ring &R1, RingPos &p1, const Ring &R2,
+                                                RingPos &p2, int t1, int nx, int ny, int nz,
+                                                const C7<float> k, int x0, int y0, int zb,
+                                                int nzl) {
+  constexpr int V = 4, VY = kTbVY1;
+  constexpr int BX = kTbBX1;
+  const int lane = t1 & 31;
+  const int tx = t1 & 31, ty = t1 >> 5;  // 32 vector columns x groups of VY rows
+  const int xg0 = x0 + tx * V;
+  const int ri0 = ty * VY;                // first intermediate row (y = y0 - 1 + ri)
+  const int yg0 = y0 - 1 + ri0;
+  const int rc0 = (ri0 + 1) * BX + 8 + tx * V;  // input-box offset of (xg0, row ri0)
+  const int wc0 = ri0 * kTbBX2 + 4 + tx * V;     // R2 offset of the same point
+  // Edge scalars: columns x0-1 and x0+128 of the 18 intermediate rows, one per
+  // fifth thread so that every warp takes a few.
+  const bool edge = (t1 % 5) == 0 && t1 / 5 < 2 * kTbBY2;
+  const int ecol = edge ? (t1 / 5) / kTbBY2 : 0;   // 0: x0 - 1, 1: x0 + 128
+  const int erow = edge ? (t1 / 5) % kTbBY2 : 0;
+  const int ex = ecol ? x0 + kTbTX : x0 - 1;
+  const int ey = y0 - 1 + erow;
+  const int erc = (erow + 1) * BX + (ecol ? 8 + kTbTX : 7);
+  const int ewc = erow * kTbBX2 + (ecol ? 4 + kTbTX : 3);
+
+  unsigned xfix = 0;
+  if (xg0 == 0) xfix |= 16u;
+#pragma unroll
+  for (int v = 0; v < V; v++)
+    if (xg0 + v == nx - 1) xfix |= 1u << v;
+  bool yedge = false;
+#pragma unroll
+  for (int r = 0; r < VY; r++) yedge = yedge || yg0 + r == 0 || yg0 + r == ny - 1;
+  const K7<float> kk = make_k7(k);
+
+  auto wait_full = [&](const Ring &R, const RingPos &q) -> bool {
+    bool ok = mbar_wait_bounded(&R.full[q.slot], q.round & 1);
+    return __all_sync(0xffffffffu, ok);
+  };
+  auto release = [&](int slot) {
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&R1.empty[slot]);
+  };
+  auto plane = [&](int slot) -> const float * {
+    return reinterpret_cast<const float *>(R1.base + slot * R1.stage_bytes);
+  };
+
+  RingPos pz = p1;
+  ring_next(pz, R1.S);
+  RingPos pt = pz;
+  int z = zb - 1;  // intermediate plane of the current step
+  float eb = 0.f, ec = 0.f;
+
+  auto step = [&](Vec16<float>(&vb)[VY], Vec16<float>(&vc)[VY], Vec16<float>(&vt)[VY]) -> bool {
+    ring_next(pt, R1.S);
+    if (!wait_full(R1, pt)) return false;
+    const float *pzp = plane(pz.slot);
+    const float *ptp = plane(pt.slot);
+#pragma unroll
+    for (int r = 0; r < VY; r++) vt[r] = lds16(ptp + rc0 + r * BX);
+    const Vec16<float> vn = lds16(pzp + rc0 - BX);
+    const Vec16<float> vs = lds16(pzp + rc0 + VY * BX);
+    float wl[VY], er[VY];
+#pragma unroll
+    for (int r = 0; r < VY; r++) {
+      wl[r] = pzp[rc0 + r * BX - 1];
+      er[r] = pzp[rc0 + r * BX + V];
+    }
+    float en = 0.f, es = 0.f, ew = 0.f, ee = 0.f, et = 0.f;
+    if (edge) {
+      et = ptp[erc];
+      en = pzp[erc - BX];
+      es = pzp[erc + BX];
+      ew = pzp[erc - 1];
+      ee = pzp[erc + 1];
+    }
+    release(pz.slot);
+    const bool zedge = z == 0 || z == nz - 1;
+    Vec16<float> res[VY];
+    if (!(yedge || zedge)) {
+#pragma unroll
+      for (int r = 0; r < VY; r++)
+        res[r] = diff7_row(kk, vc[r], wl[r], er[r], r == 0 ? vn : vc[r - 1],
+                           r == VY - 1 ? vs : vc[r + 1], vb[r], vt[r], xfix);
+    } else {
+#pragma unroll
+      for (int r = 0; r < VY; r++) {
+        const Vec16<float> &nv = r == 0 ? vn : vc[r - 1];
+        const Vec16<float> &sv = r == VY - 1 ? vs : vc[r + 1];
+        const int y = yg0 + r;
+#pragma unroll
+        for (int v = 0; v < V; v++) {
+          const int x = xg0 + v;
+          float c = vc[r].v[v];
+          float w = v == 0 ? wl[r] : vc[r].v[v - 1];
+          float e = v == V - 1 ? er[r] : vc[r].v[v + 1];
+          float n = nv.v[v], s = sv.v[v], bb = vb[r].v[v], t = vt[r].v[v];
+          if (x == 0) w = c;
+          if (x == nx - 1) e = c;
+          if (y == 0) n = c;
+          if (y == ny - 1) s = c;
+          if (z == 0) bb = c;
+          if (z == nz - 1) t = c;
+          res[r].v[v] = diff7_point(k, c, w, e, n, s, bb, t);
+        }
+      }
+    }
+    float eres = 0.f;
+    if (edge) {
+      float w = ew, e = ee, n = en, s = es, bb = eb, t = et;
+      if (ex == 0) w = ec;
+      if (ex == nx - 1) e = ec;
+      if (ey == 0) n = ec;
+      if (ey == ny - 1) s = ec;
+      if (z == 0) bb = ec;
+      if (z == nz - 1) t = ec;
+      eres = diff7_point(k, ec, w, e, n, s, bb, t);
+      eb = ec;
+      ec = et;
+    }
+    // The intermediate plane into the next stage of R2.
+    if (p2.round > 0 && !__all_sync(0xffffffffu, mbar_wait_bounded(&R2.empty[p2.slot],
+                                                                   (p2.round - 1) & 1)))
+      return false;
+    float *dst = reinterpret_cast<float *>(R2.base + p2.slot * R2.stage_bytes);
+#pragma unroll
+    for (int r = 0; r < VY; r++)
+      *reinterpret_cast<float4 *>(dst + wc0 + r * kTbBX2) =
+          make_float4(res[r].v[0], res[r].v[1], res[r].v[2], res[r].v[3]);
+    if (edge) dst[ewc] = eres;
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&R2.full[p2.slot]);
+    ring_next(p2, R2.S);
+    pz = pt;
+    z++;
+    return true;
+  };
+
+  const int nsteps = nzl + 2;
+  Vec16<float> A[VY], B[VY], C[VY];
+  bool bad = !wait_full(R1, p1);
+  bad = bad || !wait_full(R1, pz);
+  if (!bad) {
+    const float *q0 = plane(p1.slot), *q1 = plane(pz.slot);
+#pragma unroll
+    for (int r = 0; r < VY; r++) {
+      A[r] = lds16(q0 + rc0 + r * BX);
+      B[r] = lds16(q1 + rc0 + r * BX);
+    }
+    if (edge) {
+      eb = q0[erc];
+      ec = q1[erc];
+    }
+    release(p1.slot);
+    int jj = 0;
+    for (; jj + 3 <= nsteps; jj += 3) {
+      if (!step(A, B, C) || !step(B, C, A) || !step(C, A, B)) {
+        bad = true;
+        break;
+      }
+    }
+    if (!bad && jj < nsteps) {
+      bad = !step(A, B, C);
+      if (!bad && jj + 1 < nsteps) bad = !step(B, C, A);
+    }
+  }
+  if (bad) return false;
+  release(pt.slot);
+  p1 = pt;
+  ring_next(p1, R1.S);
   return true;
 }
 

@@ -215,6 +215,47 @@ void maps_forget_grid(const GridImpl *g) {
   }
 }
 
+// The pattern temporal blocking applies to: PSStencilRun(m1, m2, iter) with
+// m1: A -> B and m2: B -> A the same clamped float 7-point map over the
+// whole of two pitched grids.
+static bool tb2_pair(MapImpl **ms, int n) {
+  if (n != 2) return false;
+  const MapImpl &a = *ms[0], &b = *ms[1];
+  if (a.kernel_id != PSB_KERNEL_DIFFUSION7 || b.kernel_id != PSB_KERNEL_DIFFUSION7) return false;
+  if (a.color != -1 || b.color != -1 || a.nparams != 7 || b.nparams != 7) return false;
+  for (int i = 0; i < 7; i++)
+    if (a.params[i] != b.params[i]) return false;
+  GridImpl *A = a.grids[0], *B = a.grids[1];
+  if (b.grids[0] != B || b.grids[1] != A || A == B) return false;
+  for (GridImpl *g : {A, B}) {
+    if (g->layout != PSB_LAYOUT_PITCHED || g->type != PS_FLOAT || g->pub.num_dims != 3 ||
+        !tma_eligible(g))
+      return false;
+    for (int i = 0; i < 3; i++)
+      if (g->pub.dim[i] != A->pub.dim[i]) return false;
+  }
+  for (const MapImpl *m : {&a, &b})
+    for (int i = 0; i < 3; i++)
+      if (m->dom.local_min[i] != 0 || m->dom.local_max[i] != A->pub.dim[i]) return false;
+  return true;
+}
+
+// iter pairs as F two-step launches (F the largest even number below iter)
+// alternating A -> B and B -> A, then the remaining one or two pairs
+// unfused: both grids end exactly as after the unfused run (A the last
+// step, B the one before it).
+static psb_status run_tb2(MapImpl **ms, int iter, int zchunk, int64_t *launches) {
+  Runtime &r = rt();
+  GridImpl *A = ms[0]->grids[0], *B = ms[0]->grids[1];
+  const int F = (iter - 1) & ~1;
+  for (int f = 0; f < F; f++)
+    PSB_CHECK(diffusion7_tb2_launch(*ms[0], f & 1 ? B : A, f & 1 ? A : B, zchunk, r.stream,
+                                    launches));
+  A->ghost_valid = B->ghost_valid = PSB_BOUNDARY_NONE;
+  for (int it = F; it < iter; it++) PSB_CHECK(launch_iteration(ms, 2, launches));
+  return PSB_OK;
+}
+
 static psb_status run_maps(MapImpl **ms, int n, int iter) {
   Runtime &r = rt();
   if (iter <= 0) return PSB_OK;
@@ -223,6 +264,19 @@ static psb_status run_maps(MapImpl **ms, int n, int iter) {
   int64_t launches = 0;
   legacy_join_in();
   PSB_TRY(cudaEventRecord(r.ev_start, r.stream));
+  if (r.impl != PSB_IMPL_PLAIN && r.impl != PSB_IMPL_GENERIC && tb2_pair(ms, n)) {
+    psb_tune_config cfg;
+    const int *dims = ms[0]->grids[0]->pub.dim;
+    tune_lookup(PSB_KERNEL_DIFFUSION7, PS_FLOAT, dims, &cfg);
+    if (cfg.t_depth == 2) {
+      PSB_CHECK(run_tb2(ms, iter, cfg.z_chunk, &launches));
+      PSB_TRY(cudaEventRecord(r.ev_stop, r.stream));
+      legacy_join_out();
+      r.last_launches = launches;
+      r.last_timed = true;
+      return PSB_OK;
+    }
+  }
   // The first iteration always runs eagerly: it performs every lazy set-up
   // (TMA descriptors, residual buffers, kernel attributes) outside stream
   // capture. The remaining iterations replay a CUDA graph of `unroll`

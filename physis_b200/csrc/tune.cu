@@ -168,8 +168,12 @@ static double time_config(MapImpl &m, const psb_tune_config &cfg, int reps) {
   for (int round = 0; round < 4; round++) {
     cudaEventRecord(a, r.stream);
     for (int i = 0; i < reps; i++) {
-      psb_status st = m.kernel_id == PSB_KERNEL_HIMENO19 ? himeno_launch(m, cfg, r.stream, &launches)
-                                                         : diffusion7_launch(m, cfg, r.stream, &launches);
+      // Two-step (temporally blocked) candidates advance two steps per launch.
+      psb_status st =
+          m.kernel_id == PSB_KERNEL_HIMENO19 ? himeno_launch(m, cfg, r.stream, &launches)
+          : cfg.t_depth == 2 ? diffusion7_tb2_launch(m, m.grids[0], m.grids[1], cfg.z_chunk,
+                                                     r.stream, &launches)
+                             : diffusion7_launch(m, cfg, r.stream, &launches);
       if (st != PSB_OK) {
         cudaEventDestroy(a);
         cudaEventDestroy(b);
@@ -184,6 +188,7 @@ static double time_config(MapImpl &m, const psb_tune_config &cfg, int reps) {
     }
     float ms = 0;
     cudaEventElapsedTime(&ms, a, b);
+    ms /= cfg.t_depth == 2 ? 2 : 1;  // per step
     if (round > 0 && (best < 0 || ms / reps < best)) best = ms / reps;  // round 0 warms up
   }
   cudaEventDestroy(a);
@@ -291,13 +296,28 @@ psb_status psb_autotune(int kernel_id, int type, const PSIndex *dims, int force,
           c.t_depth = 1;
           cands.push_back(c);
         }
+  // Temporal blocking (two steps per launch; clamped float 7-point only).
+  // Its tile fields are a valid single-step configuration too, for maps run
+  // alone.
+  if (kernel_id == PSB_KERNEL_DIFFUSION7 && type == PS_FLOAT)
+    for (int zc : {32, 64, 128}) {
+      if (zc > dims[2] * 2) continue;
+      psb_tune_config c;
+      c.impl = PSB_IMPL_TMA;
+      c.tile_x = 128;
+      c.tile_y = 8;
+      c.z_chunk = zc;
+      c.stages = 6;
+      c.t_depth = 2;
+      cands.push_back(c);
+    }
   double best_ms = -1;
   psb_tune_config best = default_config(kernel_id, type, (const int *)dims);
   for (auto &c : cands) {
     double ms = time_config(m, c, reps);
     if (__ps_trace)
-      fprintf(__ps_trace, "physis_b200: tune impl=%d tile=%dx%d zc=%d st=%d: %.4f ms\n", c.impl,
-              c.tile_x, c.tile_y, c.z_chunk, c.stages, ms);
+      fprintf(__ps_trace, "physis_b200: tune impl=%d tile=%dx%d zc=%d st=%d t=%d: %.4f ms\n",
+              c.impl, c.tile_x, c.tile_y, c.z_chunk, c.stages, c.t_depth, ms);
     if (ms > 0 && (best_ms < 0 || ms < best_ms)) {
       best_ms = ms;
       best = c;

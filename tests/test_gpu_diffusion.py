@@ -103,3 +103,47 @@ def test_periodic_conserves_total():
     f = np.random.default_rng(8).random((128, 96, 160)).astype(np.float64)
     out = U.diffusion_gpu(f, 10, COEF, periodic=True, impl=ps.IMPL_TMA)
     assert abs(out.sum() - f.sum()) <= 1e-12 * f.size
+
+
+def _tb_run(field, pairs, zchunk):
+    """PSStencilRun(m(g1->g2), m(g2->g1), pairs) with two-step temporal
+    blocking selected for this grid size; returns (g1, g2)."""
+    nz, ny, nx = field.shape
+    dims = (nx, ny, nz)
+    old = ps.tune_get(ps.DIFFUSION7, ps.PS_FLOAT, dims)
+    ps.tune_set(ps.DIFFUSION7, ps.PS_FLOAT, dims, impl=ps.IMPL_TMA, tile_x=128, tile_y=8,
+                z_chunk=zchunk, stages=6, t_depth=2)
+    g1 = ps.grid_new(ps.PS_FLOAT, dims)
+    g2 = ps.grid_new(ps.PS_FLOAT, dims)
+    try:
+        ps.PSGridCopyin(g1, field)
+        d = ps.PSDomain3DNew(0, nx, 0, ny, 0, nz)
+        m1 = ps.PSStencilMap(ps.DIFFUSION7, d, g1, g2, *COEF)
+        m2 = ps.PSStencilMap(ps.DIFFUSION7, d, g2, g1, *COEF)
+        ps.PSStencilRun(m1, m2, pairs)
+        return ps.PSGridCopyout(g1), ps.PSGridCopyout(g2), ps.last_run_stats()[1]
+    finally:
+        ps.PSGridFree(g1)
+        ps.PSGridFree(g2)
+        ps.tune_set(ps.DIFFUSION7, ps.PS_FLOAT, dims, **old)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,pairs,zchunk", [
+    ((8, 16, 128), 3, 8),        # one tile exactly
+    ((37, 50, 130), 5, 16),      # ragged tiles in x and y
+    ((40, 64, 256), 4, 12),      # several tiles, partial z chunk
+    ((9, 33, 200), 1, 4),        # one pair only: no two-step launch
+    ((70, 20, 300), 6, 32),
+])
+def test_temporal_blocking_bit_exact(shape, pairs, zchunk):
+    """Two steps per launch give the same bits as single steps, in both grids
+    (g1 after 2*pairs steps, g2 after 2*pairs - 1)."""
+    f = np.random.default_rng(sum(shape)).random(shape, dtype=np.float32)
+    got1, got2, launches = _tb_run(f, pairs, zchunk)
+    want2 = oracle.diffusion7(f, 2 * pairs - 1, COEF)
+    want1 = oracle.diffusion7(want2, 1, COEF)
+    assert U.bits_equal(got1, want1)
+    assert U.bits_equal(got2, want2)
+    fused = (pairs - 1) & ~1
+    assert launches == fused + 2 * (pairs - fused)
