@@ -283,6 +283,14 @@ PSStencil __PSStencilMapRed(void *kernel, ...);
 PSStencil __PSStencilMapBlack(void *kernel, ...);
 void __PSStencilRunN(int nargs, ...);
 void PSReduce(void *v, ...);
+/* PSReduce(&v, op, kernel, dom, grids...): the kernel-function form of
+ * docs/programming.md:298-320 (not implemented by the reference,
+ * translator/reference_translator.cc:1357-1360). kernel is a registered
+ * generic stencil; the value it would emit at each point of dom (in the
+ * emitted grid's element type, which v also has) is reduced by op, and
+ * nothing is stored. The PSReduce macro below dispatches both forms on the
+ * argument count. */
+void __PSReduceN(int nargs, void *v, ...);
 
 #define PSB__NARGS_(_1,_2,_3,_4,_5,_6,_7,_8,_9,_10,_11,_12,_13,_14,_15,_16,N,...) N
 #define PSB__NARGS(...) PSB__NARGS_(__VA_ARGS__,16,15,14,13,12,11,10,9,8,7,6,5,4,3,2,1)
@@ -291,6 +299,7 @@ void PSReduce(void *v, ...);
 #define PSStencilMapRed(k, ...) __PSStencilMapRed((void *)(intptr_t)(k), __VA_ARGS__)
 #define PSStencilMapBlack(k, ...) __PSStencilMapBlack((void *)(intptr_t)(k), __VA_ARGS__)
 #define PSStencilRun(...) __PSStencilRunN(PSB__NARGS(__VA_ARGS__), __VA_ARGS__)
+#define PSReduce(...) __PSReduceN(PSB__NARGS(__VA_ARGS__), __VA_ARGS__)
 
 /* ------------------------------------------------------------------------ */
 /* Group 2b: native status-returning API                                    */
@@ -451,6 +460,13 @@ psb_status psb_himeno_residual_history(PSStencil map, double *out, int n);
 
 /* Reduction of a domain of a grid, FP64 result for every element type. */
 psb_status psb_reduce(__PSGrid *g, int op, const __PSDomain *dom, double *result);
+/* Kernel-function reduction (the PSReduce kernel form, status-returning):
+ * reduce over dom the values generic stencil kernel_id would emit with the
+ * given grids (FP64 accumulation, SUM compensated, deterministic). Built-in
+ * kernels: PSB_ERR_UNSUPPORTED. */
+psb_status psb_reduce_map(int kernel_id, const __PSDomain *dom, __PSGrid *const *grids,
+                          int ngrids, const double *params, int nparams, int op,
+                          double *result);
 
 /* Allocation-free reduction (no counterpart in the reference). For callers
  * that cannot call cudaMalloc -- a host framework that owns all device memory

@@ -170,6 +170,9 @@ def _load():
         "psb_himeno_residual": (S, [ctypes.c_int, ctypes.POINTER(ctypes.c_double)]),
         "psb_himeno_residual_history": (S, [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int]),
         "psb_reduce": (S, [G, ctypes.c_int, ctypes.POINTER(PSDomain), ctypes.POINTER(ctypes.c_double)]),
+        "psb_reduce_map": (S, [ctypes.c_int, ctypes.POINTER(PSDomain), ctypes.POINTER(G), ctypes.c_int,
+                               ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.c_int,
+                               ctypes.POINTER(ctypes.c_double)]),
         "psb_last_run_stats": (S, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int64)]),
         "psb_autotune": (S, [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.c_int,
                              ctypes.POINTER(TuneConfig)]),
@@ -450,6 +453,17 @@ def PSReduce(op, g, dom=None):
             lib.__PSReduceGridDouble(ctypes.byref(v), op, g.ptr)
         return v.value
     return reduce64(op, g, dom)
+
+
+def PSReduceMap(op, kernel, dom, *grids):
+    """Kernel-function reduction (the PSReduce(&v, op, kernel, dom, ...) form):
+    reduce over dom the values the generic stencil `kernel` would emit with
+    these grids, without storing them. Returns the FP64 result."""
+    gp = (ctypes.c_void_p * len(grids))(*[g.ptr.value for g in grids])
+    r = ctypes.c_double()
+    check(lib.psb_reduce_map(int(kernel), ctypes.byref(dom), gp, len(grids), None, 0, op,
+                             ctypes.byref(r)), "psb_reduce_map")
+    return r.value
 
 
 def reduce64(op, g, dom=None):

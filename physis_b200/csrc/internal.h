@@ -194,6 +194,9 @@ psb_status generic_launch(MapImpl &m, const GenericDesc &d, int color, cudaStrea
                           int64_t *launches);
 psb_status reduce_view(const GridView &v, int type, int op, const Dom3 &dom, double *result,
                        cudaStream_t s);
+// Reduce the values generic stencil gd would emit over m's domain (no store).
+psb_status generic_reduce(MapImpl &m, const GenericDesc &gd, int op, double *result,
+                          cudaStream_t s);
 
 // Drop cached CUDA graphs (they bake grid pointers and tile shapes).
 void drop_all_graphs();

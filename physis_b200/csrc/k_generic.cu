@@ -14,71 +14,12 @@
 // k_halo_fill rewrites the resident halo of a pitched grid so that ghost
 // cell q holds the periodic image of the interior (used once, before the
 // first periodic TMA read of a grid whose halo is stale).
-#include "device.cuh"
+#include <algorithm>
+
+#include "k_generic.cuh"
+#include "reduce.cuh"
 
 namespace psb {
-
-struct GenFactor {
-  int grid;
-  int off[3];
-  int boundary;
-  double c;
-};
-
-struct GenTable {
-  int nterms;
-  int has_post;
-  GenFactor post;
-  GenFactor a[PSB_MAX_TERMS];
-  GenFactor b[PSB_MAX_TERMS];
-};
-
-struct GenGrids {
-  GridView g[PSB_MAX_GRIDS];
-  int axes[PSB_MAX_GRIDS][3];
-  int nd[PSB_MAX_GRIDS];
-  int out;
-};
-
-__device__ __forceinline__ int64_t gen_offset(const GridView &g, const int *axes, int nd,
-                                              const GenFactor &f, const int *p) {
-  int64_t off = 0;
-  for (int k = 0; k < nd; k++) {
-    const int ax = axes[k];
-    const int n = g.n[k];
-    int i = p[ax] + f.off[ax];
-    if (f.boundary == PSB_BOUNDARY_PERIODIC) {
-      i = (i + n) % n;
-    } else if (f.boundary == PSB_BOUNDARY_CLAMP) {
-      i = i < 0 ? 0 : (i > n - 1 ? n - 1 : i);
-    }
-    off += (int64_t)i * (k == 0 ? 1 : (k == 1 ? g.sy : g.sz));
-  }
-  return off;
-}
-
-template <typename A>
-__device__ __forceinline__ A gen_factor(const GenGrids &G, const GenFactor &f, const int *p) {
-  if (f.grid < 0) return (A)f.c;
-  const GridView &g = G.g[f.grid];
-  const int64_t o = gen_offset(g, G.axes[f.grid], G.nd[f.grid], f, p);
-  switch (g.type) {
-    case PS_FLOAT: return (A)((const float *)g.origin)[o];
-    case PS_DOUBLE: return (A)((const double *)g.origin)[o];
-    case PS_INT: return (A)((const int32_t *)g.origin)[o];
-    default: return (A)((const int64_t *)g.origin)[o];
-  }
-}
-
-template <typename A>
-__device__ __forceinline__ void gen_store(const GridView &g, int64_t o, A v) {
-  switch (g.type) {
-    case PS_FLOAT: ((float *)g.origin)[o] = (float)v; break;
-    case PS_DOUBLE: ((double *)g.origin)[o] = (double)v; break;
-    case PS_INT: ((int32_t *)g.origin)[o] = (int32_t)v; break;
-    default: ((int64_t *)g.origin)[o] = (int64_t)v; break;
-  }
-}
 
 template <typename A>
 __global__ void __launch_bounds__(256) k_generic(const GenTable *__restrict__ tab, GenGrids G,
@@ -171,6 +112,123 @@ psb_status generic_launch(MapImpl &m, const GenericDesc &gd, int color, cudaStre
     default: k_generic<int64_t><<<grid, block, 0, s>>>(tab, G, d, color); break;
   }
   (*launches)++;
+  return PSB_OK;
+}
+
+// --------------------------------------------------------------------------
+// Kernel-function reduction: the value a generic stencil would emit at each
+// point of the domain (evaluated exactly as k_generic does, converted to the
+// emitted grid's element type) is reduced instead of stored -- the
+// PSReduce(&v, op, kernel, dom, ...) form of the reference's documentation
+// (docs/programming.md:298-320; the reference leaves it unimplemented,
+// translator/reference_translator.cc:1357-1360). One pass, no temporary
+// grid: each warp walks x rows of the domain, values accumulate in FP64
+// (SUM compensated), CTAs combine in index order through the same scratch
+// as the grid reduction.
+// --------------------------------------------------------------------------
+__device__ __forceinline__ double as_emitted(int type, double v) {
+  switch (type) {
+    case PS_FLOAT: return (double)(float)v;
+    case PS_INT: return (double)(int32_t)v;
+    case PS_LONG: return (double)(int64_t)v;
+    default: return v;
+  }
+}
+
+template <typename A>
+__global__ void __launch_bounds__(256) k_generic_reduce(const GenTable *__restrict__ tab,
+                                                        GenGrids G, Dom3 d, int op,
+                                                        ReduceScratch sc) {
+  __shared__ GenTable t;
+  __shared__ RAcc scratch[32];
+  __shared__ int is_last;
+  {
+    const int words = sizeof(GenTable) / 4;
+    const uint32_t *src = reinterpret_cast<const uint32_t *>(tab);
+    uint32_t *dst = reinterpret_cast<uint32_t *>(&t);
+    for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+  }
+  __syncthreads();
+  const int out_type = G.g[G.out].type;
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  const int rx = d.hi[0] - d.lo[0], ry = d.hi[1] - d.lo[1];
+  const int64_t rows = (int64_t)ry * (d.hi[2] - d.lo[2]);
+  RAcc a = racc_init(op);
+  for (int64_t r = warp; r < rows; r += nwarps) {
+    int p[3];
+    p[1] = d.lo[1] + (int)(r % ry);
+    p[2] = d.lo[2] + (int)(r / ry);
+    for (int x = lane; x < rx; x += 32) {
+      p[0] = d.lo[0] + x;
+      A acc = 0;
+      for (int i = 0; i < t.nterms; i++) {
+        A v = xmul(gen_factor<A>(G, t.a[i], p), gen_factor<A>(G, t.b[i], p));
+        acc = i ? xadd(acc, v) : v;
+      }
+      if (t.has_post) acc = xmul(acc, gen_factor<A>(G, t.post, p));
+      racc_add(op, a, as_emitted(out_type, (double)acc));
+    }
+  }
+  RAcc b = racc_block(op, a, scratch);
+  if (threadIdx.x == 0) {
+    sc.partials[blockIdx.x] = b;
+    __threadfence();
+    const unsigned tk = atomicAdd(sc.ticket, 1u);
+    is_last = (tk == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  RAcc acc = racc_init(op);
+  for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) {
+    RAcc q;
+    q.s = __ldcg(&sc.partials[i].s);
+    q.c = __ldcg(&sc.partials[i].c);
+    acc = racc_merge(op, acc, q);
+  }
+  RAcc tot = racc_block(op, acc, scratch);
+  if (threadIdx.x == 0) {
+    *sc.result = op == PS_SUM ? tot.s + tot.c : tot.s;
+    *sc.ticket = 0;
+  }
+}
+
+psb_status generic_reduce(MapImpl &m, const GenericDesc &gd, int op, double *result,
+                          cudaStream_t s) {
+  const psb_generic_stencil &desc = gd.host;
+  GenGrids G;
+  for (int i = 0; i < desc.ngrids; i++) {
+    G.g[i] = m.grids[i]->view();
+    G.g[i].type = desc.grid_type[i];
+    G.nd[i] = 0;
+    for (int k = 0; k < 3; k++) {
+      G.axes[i][k] = desc.grid_axes[i][k];
+      if (desc.grid_axes[i][k] >= 0) G.nd[i] = k + 1;
+    }
+  }
+  G.out = desc.out_grid;
+  Dom3 d;
+  for (int i = 0; i < 3; i++) {
+    d.lo[i] = i < desc.ndims ? m.dom.local_min[i] : 0;
+    d.hi[i] = i < desc.ndims ? m.dom.local_max[i] : 1;
+  }
+  const int64_t rows = (int64_t)(d.hi[1] - d.lo[1]) * (d.hi[2] - d.lo[2]);
+  if (rows <= 0 || d.hi[0] <= d.lo[0]) return set_status(PSB_ERR_INVALID);
+  ReduceScratch sc;
+  PSB_CHECK(reduce_scratch(&sc));
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((rows + 7) / 8, kReduceMaxBlocks));
+  const GenTable *tab = (const GenTable *)gd.dev;
+  switch (desc.accum_type) {
+    case PS_FLOAT: k_generic_reduce<float><<<blocks, 256, 0, s>>>(tab, G, d, op, sc); break;
+    case PS_DOUBLE: k_generic_reduce<double><<<blocks, 256, 0, s>>>(tab, G, d, op, sc); break;
+    case PS_INT: k_generic_reduce<int32_t><<<blocks, 256, 0, s>>>(tab, G, d, op, sc); break;
+    default: k_generic_reduce<int64_t><<<blocks, 256, 0, s>>>(tab, G, d, op, sc); break;
+  }
+  PSB_TRY(cudaGetLastError());
+  PSB_TRY(cudaMemcpyAsync(result, sc.result, sizeof(double), cudaMemcpyDeviceToHost, s));
+  PSB_TRY(cudaStreamSynchronize(s));
   return PSB_OK;
 }
 

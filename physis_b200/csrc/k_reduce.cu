@@ -18,87 +18,9 @@
 #include <cstdio>
 #include <mutex>
 
-#include "device.cuh"
+#include "reduce.cuh"
 
 namespace psb {
-
-struct RAcc {
-  double s;  // value (sum, product, max or min)
-  double c;  // compensation (SUM only)
-};
-
-__device__ __forceinline__ RAcc racc_init(int op) {
-  RAcc a;
-  a.c = 0.0;
-  switch (op) {
-    case PS_MAX: a.s = -DBL_MAX; break;
-    case PS_MIN: a.s = DBL_MAX; break;
-    case PS_SUM: a.s = 0.0; break;
-    default: a.s = 1.0; break;
-  }
-  return a;
-}
-
-// Neumaier step: add x to (s, c).
-__device__ __forceinline__ void neumaier(RAcc &a, double x) {
-  double t = a.s + x;
-  if (fabs(a.s) >= fabs(x)) a.c += (a.s - t) + x;
-  else a.c += (x - t) + a.s;
-  a.s = t;
-}
-
-__device__ __forceinline__ RAcc racc_merge(int op, RAcc a, RAcc b) {
-  switch (op) {
-    case PS_MAX: a.s = a.s > b.s ? a.s : b.s; return a;
-    case PS_MIN: a.s = a.s < b.s ? a.s : b.s; return a;
-    case PS_SUM: {
-      RAcc r = a;
-      neumaier(r, b.s);
-      r.c += b.c;
-      return r;
-    }
-    default: a.s = a.s * b.s; return a;
-  }
-}
-
-__device__ __forceinline__ void racc_add(int op, RAcc &a, double x) {
-  switch (op) {
-    case PS_MAX: a.s = a.s > x ? a.s : x; break;
-    case PS_MIN: a.s = a.s < x ? a.s : x; break;
-    case PS_SUM: neumaier(a, x); break;
-    default: a.s = a.s * x; break;
-  }
-}
-
-__device__ RAcc racc_block(int op, RAcc v, RAcc *scratch) {
-  for (int o = 16; o > 0; o >>= 1) {
-    RAcc u;
-    u.s = __shfl_down_sync(0xffffffffu, v.s, o);
-    u.c = __shfl_down_sync(0xffffffffu, v.c, o);
-    v = racc_merge(op, v, u);
-  }
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  __syncthreads();
-  if (lane == 0) scratch[warp] = v;
-  __syncthreads();
-  RAcc r = racc_init(op);
-  if (warp == 0) {
-    if (lane < nw) r = scratch[lane];
-    for (int o = 16; o > 0; o >>= 1) {
-      RAcc u;
-      u.s = __shfl_down_sync(0xffffffffu, r.s, o);
-      u.c = __shfl_down_sync(0xffffffffu, r.c, o);
-      r = racc_merge(op, r, u);
-    }
-  }
-  return r;
-}
-
-struct ReduceScratch {
-  RAcc *partials;
-  unsigned *ticket;
-  double *result;
-};
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_reduce(GridView g, Dom3 d, int op, ReduceScratch sc) {
@@ -141,20 +63,25 @@ __global__ void __launch_bounds__(256) k_reduce(GridView g, Dom3 d, int op, Redu
   }
 }
 
-static const int kReduceMaxBlocks = 1184;  // 148 SMs x 8
+// (kReduceMaxBlocks, the partials' capacity, is in reduce.cuh.)
 
-psb_status reduce_view(const GridView &v, int type, int op, const Dom3 &dom, double *result,
-                       cudaStream_t s) {
+psb_status reduce_scratch(ReduceScratch *sc) {
   static void *scratch = nullptr;
   if (!scratch) {
     size_t bytes = sizeof(RAcc) * kReduceMaxBlocks + 256;
     PSB_TRY(cudaMalloc(&scratch, bytes));
     PSB_TRY(cudaMemset(scratch, 0, bytes));
   }
+  sc->partials = (RAcc *)scratch;
+  sc->ticket = (unsigned *)((char *)scratch + sizeof(RAcc) * kReduceMaxBlocks);
+  sc->result = (double *)((char *)scratch + sizeof(RAcc) * kReduceMaxBlocks + 128);
+  return PSB_OK;
+}
+
+psb_status reduce_view(const GridView &v, int type, int op, const Dom3 &dom, double *result,
+                       cudaStream_t s) {
   ReduceScratch sc;
-  sc.partials = (RAcc *)scratch;
-  sc.ticket = (unsigned *)((char *)scratch + sizeof(RAcc) * kReduceMaxBlocks);
-  sc.result = (double *)((char *)scratch + sizeof(RAcc) * kReduceMaxBlocks + 128);
+  PSB_CHECK(reduce_scratch(&sc));
   int64_t rows = (int64_t)(dom.hi[1] - dom.lo[1]) * (dom.hi[2] - dom.lo[2]);
   if (rows <= 0 || dom.hi[0] <= dom.lo[0]) return set_status(PSB_ERR_INVALID);
   int blocks = (int)std::min<int64_t>((rows + 7) / 8, kReduceMaxBlocks);

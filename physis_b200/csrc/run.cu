@@ -38,7 +38,9 @@ static const GenericDesc *generic_of(int kernel_id) {
 }
 
 // Expected grid count / types of a kernel.
-static psb_status check_map(const MapImpl &m) {
+// writes: false for a kernel-function reduction (nothing is stored, so an
+// emitted grid that is also read at offsets is fine).
+static psb_status check_map(const MapImpl &m, bool writes = true) {
   switch (m.kernel_id) {
     case PSB_KERNEL_DIFFUSION7:
     case PSB_KERNEL_DIFFUSION7_PERIODIC: {
@@ -109,7 +111,7 @@ static psb_status check_map(const MapImpl &m) {
       // A grid that is both read at an offset and written, without
       // red-black ordering, would race; the reference's ref target gives it
       // Gauss-Seidel meaning, which a parallel sweep cannot reproduce.
-      if (m.color < 0) {
+      if (writes && m.color < 0) {
         const GridImpl *out = m.grids[d.out_grid];
         for (int t = 0; t < d.nterms; t++) {
           const psb_factor *fs[2] = {&d.terms[t].a, &d.terms[t].b};
@@ -678,7 +680,7 @@ void __PSReduceGridDouble(void *buf, enum PSReduceOp op, __PSGrid *g) {
   reduce_abi<double>(buf, op, g, PS_DOUBLE);
 }
 
-void PSReduce(void *v, ...) {
+void(PSReduce)(void *v, ...) {
   // PSReduce(&v, op, grid): the grid form of physis_user.h:114. The result
   // type follows the grid's element type.
   va_list vl;
@@ -696,6 +698,75 @@ void PSReduce(void *v, ...) {
     case PS_INT: reduce_abi<int32_t>(v, (PSReduceOp)op, p, PS_INT); break;
     case PS_LONG: reduce_abi<int64_t>(v, (PSReduceOp)op, p, PS_LONG); break;
     default: reduce_abi<float>(v, (PSReduceOp)op, p, PS_FLOAT); break;
+  }
+}
+
+psb_status psb_reduce_map(int kernel_id, const __PSDomain *dom, __PSGrid *const *grids,
+                          int ngrids, const double *params, int nparams, int op,
+                          double *result) {
+  PSB_CHECK(ensure_init());
+  if (!dom || !grids || !result || op < PS_MAX || op > PS_PROD || ngrids < 1 ||
+      ngrids > PSB_MAX_GRIDS || nparams < 0 || nparams > PSB_MAX_PARAMS)
+    return set_status(PSB_ERR_INVALID);
+  const GenericDesc *gd = generic_of(kernel_id);
+  if (!gd) return set_status(kernel_id < PSB_KERNEL_FIRST_GENERIC ? PSB_ERR_UNSUPPORTED
+                                                                  : PSB_ERR_INVALID);
+  MapImpl m;
+  m.kernel_id = kernel_id;
+  m.dom = *dom;
+  m.ngrids = ngrids;
+  for (int i = 0; i < ngrids; i++) {
+    m.grids[i] = as_impl(grids[i]);
+    if (!m.grids[i] || m.grids[i]->user_type) return set_status(PSB_ERR_INVALID);
+  }
+  m.nparams = nparams;
+  for (int i = 0; i < nparams; i++) m.params[i] = params[i];
+  PSB_CHECK(check_map(m, false));
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
+  legacy_join_in();
+  PSB_CHECK(generic_reduce(m, *gd, op, result, r.stream));
+  legacy_join_out();
+  return PSB_OK;
+}
+
+// PSReduce(&v, op, grid) or PSReduce(&v, op, kernel, dom, grids...): the
+// macro passes the argument count. The kernel form reduces the values the
+// stencil would emit; v has the emitted grid's element type.
+void __PSReduceN(int nargs, void *v, ...) {
+  va_list vl;
+  va_start(vl, v);
+  const int op = va_arg(vl, int);
+  if (nargs == 3) {
+    __PSGrid *g = va_arg(vl, __PSGrid *);
+    va_end(vl);
+    (PSReduce)(v, op, g);
+    return;
+  }
+  const int kid = (int)(intptr_t)va_arg(vl, void *);
+  int np = 0;
+  const int ng = kernel_ngrids(kid, &np);
+  if (ng < 0) {
+    va_end(vl);
+    fprintf(stderr, "physis_b200: PSReduce: unknown kernel %d\n", kid);
+    exit(EXIT_FAILURE);
+  }
+  __PSDomain dom = va_arg(vl, __PSDomain);
+  __PSGrid *grids[PSB_MAX_GRIDS];
+  for (int i = 0; i < ng; i++) grids[i] = va_arg(vl, __PSGrid *);
+  va_end(vl);
+  double r = 0;
+  psb_status s = psb_reduce_map(kid, &dom, grids, ng, nullptr, 0, op, &r);
+  if (s != PSB_OK) {
+    fprintf(stderr, "physis_b200: PSReduce failed: %s\n", psb_status_string(s));
+    exit(EXIT_FAILURE);
+  }
+  const GenericDesc *gd = generic_of(kid);
+  switch (gd->host.grid_type[gd->host.out_grid]) {
+    case PS_DOUBLE: *(double *)v = r; break;
+    case PS_INT: *(int32_t *)v = (int32_t)r; break;
+    case PS_LONG: *(int64_t *)v = (int64_t)r; break;
+    default: *(float *)v = (float)r; break;
   }
 }
 
