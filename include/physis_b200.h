@@ -398,6 +398,31 @@ const char *psb_status_string(psb_status s);
 
 /* Grid creation with an explicit layout and element type (PSPrimitiveType).
  * dims has num_dims entries. */
+/* Grids of user-defined point types (the reference's DeclareGrid3D(Name,
+ * struct T) with struct members, physis_user.h:52-75, tests
+ * test_user-defined-type-*.c; its CUDA target keeps them as SoA device
+ * arrays, translator/cuda_runtime_builder.cc:319-1100). A type is a list of
+ * fields, each `count` scalars of one primitive type at `offset` bytes into
+ * a record of record_bytes. On the device every scalar component (field f,
+ * element k) is its own pitched grid; copy-in/copy-out of the user-type
+ * grid (PSGridCopyin/Copyout, psb_grid_copyin/copyout_async) convert between
+ * the host array of records and the components on the device. Stencils bind
+ * components (psb_grid_component) like ordinary grids. */
+#define PSB_MAX_FIELDS 16
+#define PSB_MAX_COMPONENTS 64
+typedef struct {
+  int nfields;
+  size_t record_bytes;
+  int field_type[PSB_MAX_FIELDS];     /* PS_FLOAT / PS_DOUBLE / PS_INT / PS_LONG */
+  int field_count[PSB_MAX_FIELDS];    /* scalars in the field (array members) */
+  size_t field_offset[PSB_MAX_FIELDS];
+} psb_user_type;
+psb_status psb_grid_new_user(int num_dims, const PSIndex *dims, const psb_user_type *type,
+                             __PSGrid **out);
+/* Component k of field f of a user-type grid: a grid handle sharing the
+ * component's storage (valid until the user-type grid is freed; do not
+ * free it). */
+psb_status psb_grid_component(__PSGrid *g, int field, int index, __PSGrid **out);
 psb_status psb_grid_new(int type, int num_dims, const PSIndex *dims, int layout,
                         __PSGrid **out);
 /* Strides in elements between y rows and z planes, the layout and the

@@ -99,6 +99,18 @@ class TuneConfig(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+PSB_MAX_FIELDS = 16
+PS_USER = 4
+
+
+class UserType(ctypes.Structure):
+    """psb_user_type."""
+    _fields_ = [("nfields", ctypes.c_int), ("record_bytes", ctypes.c_size_t),
+                ("field_type", ctypes.c_int * PSB_MAX_FIELDS),
+                ("field_count", ctypes.c_int * PSB_MAX_FIELDS),
+                ("field_offset", ctypes.c_size_t * PSB_MAX_FIELDS)]
+
+
 class Request(ctypes.Structure):
     """psb_request."""
     _fields_ = [("kernel_id", ctypes.c_int), ("dims", ctypes.c_int32 * 3),
@@ -150,6 +162,9 @@ def _load():
         "psb_grid_layout": (S, [G, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int64)]),
         "psb_grid_copyin_async": (S, [G, ctypes.c_void_p]),
+        "psb_grid_new_user": (S, [ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(UserType),
+                                  ctypes.POINTER(G)]),
+        "psb_grid_component": (S, [G, ctypes.c_int, ctypes.c_int, ctypes.POINTER(G)]),
         "psb_grid_copyout_async": (S, [G, ctypes.c_void_p]),
         "psb_sync": (S, []),
         "psb_host_alloc": (S, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
@@ -269,6 +284,53 @@ def grid_new(type_, dims, layout=LAYOUT_PITCHED):
     p = ctypes.c_void_p()
     check(lib.psb_grid_new(type_, len(dims), d, layout, ctypes.byref(p)), "psb_grid_new")
     return Grid(p.value, type_, dims)
+
+
+def grid_new_user(dims, fields, record_bytes):
+    """Grid of a user-defined point type. fields: list of (type, count,
+    byte offset) in record order; record_bytes: the record size (e.g. a
+    numpy structured dtype's itemsize)."""
+    ut = UserType()
+    ut.nfields = len(fields)
+    ut.record_bytes = int(record_bytes)
+    for i, (t, n, off) in enumerate(fields):
+        ut.field_type[i] = t
+        ut.field_count[i] = n
+        ut.field_offset[i] = off
+    d = (ctypes.c_int32 * 3)(*(list(dims) + [0] * (3 - len(dims))))
+    p = ctypes.c_void_p()
+    check(lib.psb_grid_new_user(len(dims), d, ctypes.byref(ut), ctypes.byref(p)), "psb_grid_new_user")
+    g = Grid(p.value, PS_USER, dims)
+    g.fields = list(fields)
+    g.record_bytes = int(record_bytes)
+    return g
+
+
+def component(g, field, index=0):
+    """Component `index` of field `field` of a user-type grid, as a grid that
+    stencils can bind (owned by g: do not free it)."""
+    p = ctypes.c_void_p()
+    check(lib.psb_grid_component(g.ptr, field, index, ctypes.byref(p)), "psb_grid_component")
+    return Grid(p.value, g.fields[field][0], g.dims)
+
+
+def user_copyin(g, records):
+    """Copy a host array of records (numpy, itemsize = record_bytes) into a
+    user-type grid."""
+    a = np.ascontiguousarray(records)
+    if a.itemsize * a.size != g.record_bytes * int(np.prod(g.dims)):
+        raise ValueError("record array does not match the grid")
+    check(lib.psb_grid_copyin_async(g.ptr, a.ctypes.data), "psb_grid_copyin_async")
+    sync()
+
+
+def user_copyout(g, records):
+    """Copy a user-type grid into a host array of records (in place)."""
+    if not records.flags.c_contiguous or records.itemsize * records.size != \
+            g.record_bytes * int(np.prod(g.dims)):
+        raise ValueError("record array does not match the grid")
+    check(lib.psb_grid_copyout_async(g.ptr, records.ctypes.data), "psb_grid_copyout_async")
+    sync()
 
 
 def _mk(type_, nd):

@@ -61,6 +61,12 @@ struct GridImpl {
   uint32_t magic = 0x50534232u;
   // TMA descriptors built on demand, keyed by box shape.
   std::map<uint64_t, CUtensorMap> tmaps;
+  // User-defined point type kept as SoA components (one pitched grid per
+  // scalar component, in field order); empty for ordinary grids.
+  std::vector<GridImpl *> comps;
+  std::vector<int> comp_field_first;  // index of field f's first component
+  psb_user_type utype{};
+  bool component = false;  // a component of a user-type grid (not freed alone)
 
   int64_t nelems() const { return pub.num_elms; }
   GridView view() const;
@@ -173,6 +179,8 @@ psb_status grid_alloc_pool(int type, const int *dims, cudaMemPool_t pool, cudaSt
                            GridImpl **out);
 void grid_free_pool(GridImpl *g, cudaStream_t s);
 psb_status grid_copy_in_on(GridImpl *g, const void *src, cudaStream_t s);
+// Host array of records <-> the SoA components of a user-type grid.
+psb_status user_transfer(GridImpl *g, void *host, bool h2d, cudaStream_t s);
 // Host <-> pitched grid through a dense staging buffer and a pack kernel.
 psb_status pitched_transfer(GridImpl *g, void *host, bool h2d, cudaStream_t s);
 // First half of a copy-out: allocate a dense staging buffer and pack the

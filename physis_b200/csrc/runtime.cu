@@ -288,6 +288,12 @@ psb_status grid_copy_out_on(GridImpl *g, void *dst, cudaStream_t s) {
 
 static void grid_free(GridImpl *g) {
   if (!g) return;
+  if (g->component) return;  // freed with its user-type grid
+  for (GridImpl *c : g->comps) {
+    c->component = false;
+    grid_free(c);
+  }
+  g->comps.clear();
   drop_all_graphs();
   maps_forget_grid(g);
   if (g->user_type) {
@@ -304,7 +310,9 @@ static psb_status copy_in(GridImpl *g, const void *src, bool sync) {
   Runtime &r = rt();
   legacy_join_in();
   int E = g->pub.elm_size;
-  if (g->layout == PSB_LAYOUT_DENSE) {
+  if (!g->comps.empty()) {
+    PSB_CHECK(user_transfer(g, (void *)src, true, r.stream));
+  } else if (g->layout == PSB_LAYOUT_DENSE) {
     PSB_TRY(cudaMemcpyAsync(g->alloc, src, (size_t)g->pub.num_elms * E, cudaMemcpyHostToDevice,
                             r.stream));
   } else {
@@ -319,7 +327,9 @@ static psb_status copy_out(GridImpl *g, void *dst, bool sync) {
   Runtime &r = rt();
   legacy_join_in();
   int E = g->pub.elm_size;
-  if (g->layout == PSB_LAYOUT_DENSE) {
+  if (!g->comps.empty()) {
+    PSB_CHECK(user_transfer(g, dst, false, r.stream));
+  } else if (g->layout == PSB_LAYOUT_DENSE) {
     PSB_TRY(cudaMemcpyAsync(dst, g->alloc, (size_t)g->pub.num_elms * E, cudaMemcpyDeviceToHost,
                             r.stream));
   } else {
@@ -697,6 +707,63 @@ const char *psb_status_string(psb_status s) {
     case PSB_ERR_BUSY: return "busy";
   }
   return "unknown";
+}
+
+psb_status psb_grid_new_user(int num_dims, const PSIndex *dims, const psb_user_type *ut,
+                             __PSGrid **out) {
+  if (!out || !dims || !ut || num_dims < 1 || num_dims > 3) return set_status(PSB_ERR_INVALID);
+  *out = nullptr;
+  if (ut->nfields < 1 || ut->nfields > PSB_MAX_FIELDS || ut->record_bytes == 0)
+    return set_status(PSB_ERR_INVALID);
+  int ncomp = 0;
+  for (int f = 0; f < ut->nfields; f++) {
+    const int es = type_size(ut->field_type[f]);
+    if (es == 0 || ut->field_count[f] < 1 || ut->field_offset[f] % es != 0 ||
+        ut->field_offset[f] + (size_t)es * ut->field_count[f] > ut->record_bytes)
+      return set_status(PSB_ERR_INVALID);
+    ncomp += ut->field_count[f];
+  }
+  if (ncomp > PSB_MAX_COMPONENTS) return set_status(PSB_ERR_INVALID);
+  int d[3] = {1, 1, 1};
+  for (int i = 0; i < num_dims; i++) {
+    if (dims[i] <= 0) return set_status(PSB_ERR_INVALID);
+    d[i] = dims[i];
+  }
+  PSB_CHECK(ensure_init());
+  GridImpl *g = new GridImpl();
+  g->pub.elm_size = (int)ut->record_bytes;
+  g->pub.num_dims = num_dims;
+  g->pub.num_elms = 1;
+  for (int i = 0; i < PS_MAX_DIM; i++) g->pub.dim[i] = i < num_dims ? d[i] : 0;
+  for (int i = 0; i < num_dims; i++) g->pub.num_elms *= d[i];
+  g->type = PS_USER;
+  g->layout = PSB_LAYOUT_PITCHED;
+  g->utype = *ut;
+  for (int f = 0; f < ut->nfields; f++) {
+    g->comp_field_first.push_back((int)g->comps.size());
+    for (int k = 0; k < ut->field_count[f]; k++) {
+      GridImpl *c = nullptr;
+      psb_status s = grid_alloc(ut->field_type[f], type_size(ut->field_type[f]), num_dims, d,
+                                PSB_LAYOUT_PITCHED, &c);
+      if (s != PSB_OK) {
+        grid_free(g);
+        return set_status(s);
+      }
+      c->component = true;
+      g->comps.push_back(c);
+    }
+  }
+  *out = &g->pub;
+  return PSB_OK;
+}
+
+psb_status psb_grid_component(__PSGrid *p, int field, int index, __PSGrid **out) {
+  GridImpl *g = as_impl(p);
+  if (!g || !out || g->comps.empty() || field < 0 || field >= g->utype.nfields || index < 0 ||
+      index >= g->utype.field_count[field])
+    return set_status(PSB_ERR_INVALID);
+  *out = &g->comps[g->comp_field_first[field] + index]->pub;
+  return PSB_OK;
 }
 
 psb_status psb_grid_new(int type, int num_dims, const PSIndex *dims, int layout, __PSGrid **out) {

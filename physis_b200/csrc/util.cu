@@ -10,6 +10,7 @@
 // computed in double and rounded to the grid's type once.
 #include <cstring>
 #include <mutex>
+#include <vector>
 
 #include "device.cuh"
 
@@ -142,6 +143,75 @@ psb_status pitched_transfer(GridImpl *g, void *host, bool h2d, cudaStream_t s) {
   }
   p.extent = make_cudaExtent((size_t)nx * E, ny, nz);
   PSB_TRY(cudaMemcpy3DAsync(&p, s));
+  return PSB_OK;
+}
+
+// User-defined point types: a host array of records <-> one pitched grid per
+// scalar component. One thread per point walks the record's components, so
+// the record is read (or written) contiguously and every component grid is
+// written (or read) coalesced across the warp.
+struct AosComp {
+  GridView v;
+  int offset;  // bytes into the record
+  int esize;   // 4 or 8
+};
+
+__global__ void __launch_bounds__(256) k_aos(const AosComp *comps, int ncomp, int record,
+                                             unsigned char *stage, int64_t npts, int unpack) {
+  const GridView v0 = comps[0].v;
+  const int nx = v0.n[0], ny = v0.n[1];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npts;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int x = (int)(i % nx);
+    const int64_t r = i / nx;
+    const int64_t y = r % ny, z = r / ny;
+    unsigned char *rec = stage + i * record;
+    for (int c = 0; c < ncomp; c++) {
+      const AosComp &a = comps[c];
+      const int64_t o = x + y * a.v.sy + z * a.v.sz;
+      if (a.esize == 4) {
+        uint32_t *g = (uint32_t *)a.v.origin + o;
+        uint32_t *h = (uint32_t *)(rec + a.offset);
+        if (unpack) *g = *h; else *h = *g;
+      } else {
+        uint64_t *g = (uint64_t *)a.v.origin + o;
+        uint64_t *h = (uint64_t *)(rec + a.offset);
+        if (unpack) *g = *h; else *h = *g;
+      }
+    }
+  }
+}
+
+psb_status user_transfer(GridImpl *g, void *host, bool h2d, cudaStream_t s) {
+  const psb_user_type &ut = g->utype;
+  std::vector<AosComp> comps;
+  for (int f = 0; f < ut.nfields; f++)
+    for (int k = 0; k < ut.field_count[f]; k++) {
+      AosComp a;
+      GridImpl *c = g->comps[g->comp_field_first[f] + k];
+      a.v = c->view();
+      a.esize = c->pub.elm_size;
+      a.offset = (int)(ut.field_offset[f] + (size_t)k * a.esize);
+      comps.push_back(a);
+    }
+  const int64_t npts = g->pub.num_elms;
+  const size_t data = (size_t)npts * ut.record_bytes;
+  const size_t table = comps.size() * sizeof(AosComp);
+  const size_t data_off = (table + 255) / 256 * 256;
+  cudaMemPool_t pool = staging_pool();
+  if (!pool) return set_status(PSB_ERR_NOMEM);
+  void *stage = nullptr;
+  PSB_TRY(cudaMallocFromPoolAsync(&stage, data_off + data, pool, s));
+  unsigned char *base = (unsigned char *)stage;
+  PSB_TRY(cudaMemcpyAsync(base, comps.data(), table, cudaMemcpyHostToDevice, s));
+  if (h2d) PSB_TRY(cudaMemcpyAsync(base + data_off, host, data, cudaMemcpyHostToDevice, s));
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((npts + 255) / 256,
+                                                                  (int64_t)rt().sm_count * 16));
+  k_aos<<<blocks, 256, 0, s>>>((const AosComp *)base, (int)comps.size(), (int)ut.record_bytes,
+                               base + data_off, npts, h2d ? 1 : 0);
+  PSB_TRY(cudaGetLastError());
+  if (!h2d) PSB_TRY(cudaMemcpyAsync(host, base + data_off, data, cudaMemcpyDeviceToHost, s));
+  PSB_TRY(cudaFreeAsync(stage, s));
   return PSB_OK;
 }
 

@@ -79,7 +79,8 @@ def test_ctypes_structs_match_header(tmp_path):
     """Sizes and field offsets of the ctypes mirrors equal the C header's."""
     import physis_b200 as ps
     structs = {"psb_request": ps.Request, "psb_result": ps.Result,
-               "psb_tune_config": ps.TuneConfig, "psb_generic_stencil": ps.GenericStencilStruct}
+               "psb_tune_config": ps.TuneConfig, "psb_generic_stencil": ps.GenericStencilStruct,
+               "psb_user_type": ps.UserType}
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "physis_b200.h"',
              'int main(void) {']
     for cname, cls in structs.items():
