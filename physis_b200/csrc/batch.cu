@@ -582,16 +582,17 @@ static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int
 
 // Planes per item. 64 when the kind's members together give enough items
 // per step for several waves of CTAs (long items, few halo planes);
-// otherwise each member takes the longest z chunk (32 or 16) that cuts one
-// of its steps into that many items, so a few large members are not
-// quantised into a fraction of a wave at every step.
+// otherwise each member takes the longest z chunk (32 down to 4) that cuts
+// one of its steps into that many items, so a few large members are not
+// quantised into a fraction of a wave at every step and a small member's
+// steps (a chain of dependent launches' worth of work) stay short.
 static int64_t items_target() { return (int64_t)rt().sm_count * 6; }
 
 static int pick_zchunk(int64_t tiles_xy, int nz, bool short_chunks) {
   if (!short_chunks) return 64;
-  for (int zc = 64; zc > 16; zc >>= 1)
+  for (int zc = 64; zc > 4; zc >>= 1)
     if (tiles_xy * ((nz + zc - 1) / zc) >= items_target()) return zc;
-  return 16;
+  return 4;
 }
 
 static TmaGeom batch_dgeom(const GridImpl *g, bool short_chunks) {
