@@ -301,6 +301,43 @@ static double residual_of(const double *r4) {
   return r4[1] > 0 ? sqrt(r4[0] / r4[1]) : 0.0;
 }
 
+// Take the queued requests that fit the budget and the slot limit, in
+// arrival order (server lock held), after those already in `admit`.
+static void take_admissible_locked(psb_server *S, std::vector<SReq *> &admit) {
+  while (!S->queue.empty()) {
+    SReq *q = S->queue.front();
+    const size_t slots = S->active.size() + admit.size();
+    if (S->max_slots > 0 && slots >= (size_t)S->max_slots) break;
+    if (S->used + q->bytes > S->budget) break;
+    S->queue.pop_front();
+    S->used += q->bytes;
+    S->peak = std::max(S->peak, S->used);
+    admit.push_back(q);
+  }
+}
+
+// Allocate and fill the taken requests (runtime lock held) and add them to
+// the active list; a request that cannot be set up completes with its error.
+static void admit_all(psb_server *S, std::vector<SReq *> &admit) {
+  Runtime &r = rt();
+  const double ta = now_s();
+  for (SReq *q : admit) {
+    psb_status st = admit_request(S, q);
+    if (st != PSB_OK) {
+      free_grids(S, q, r.stream);
+      std::lock_guard<std::mutex> lk(S->mu);
+      S->used -= q->bytes;
+      complete_locked(S, q, st);
+      continue;
+    }
+    S->active.push_back(q);
+  }
+  if (__ps_trace && !admit.empty())
+    fprintf(__ps_trace, "physis_b200 serve: admitted %d requests in %.3f ms\n",
+            (int)admit.size(), (now_s() - ta) * 1e3);
+  admit.clear();
+}
+
 // One round of the persistent batched kernel over every active request.
 static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
   Runtime &r = rt();
@@ -353,6 +390,16 @@ static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
   PSB_TRY(cudaEventRecord(S->ev1, r.stream));
   for (SReq *q : finished) PSB_CHECK(retire_copy(S, q));
   finished.clear();
+  // Requests that arrived meanwhile are set up while the round runs (their
+  // allocations and fills queue behind it) and join the next round.
+  {
+    std::vector<SReq *> admit;
+    {
+      std::lock_guard<std::mutex> lk(S->mu);
+      take_admissible_locked(S, admit);
+    }
+    admit_all(S, admit);
+  }
   const double t2 = now_s();
   PSB_TRY(cudaEventSynchronize(S->ev1));
   const double t3 = now_s();
@@ -434,16 +481,7 @@ static void worker_batched(psb_server *S) {
     {
       std::unique_lock<std::mutex> lk(S->mu);
       poll_retiring_locked(S, false);
-      while (!S->queue.empty()) {
-        SReq *q = S->queue.front();
-        const size_t slots = S->active.size() + admit.size();
-        if (S->max_slots > 0 && slots >= (size_t)S->max_slots) break;
-        if (S->used + q->bytes > S->budget) break;
-        S->queue.pop_front();
-        S->used += q->bytes;
-        S->peak = std::max(S->peak, S->used);
-        admit.push_back(q);
-      }
+      take_admissible_locked(S, admit);
       if (admit.empty() && S->active.empty()) {
         if (!finished.empty()) {
           // Nothing to overlap with: send the results now.
@@ -463,21 +501,7 @@ static void worker_batched(psb_server *S) {
       }
     }
     std::lock_guard<std::recursive_mutex> g(r.mu);
-    const double ta = now_s();
-    for (SReq *q : admit) {
-      psb_status st = admit_request(S, q);
-      if (st != PSB_OK) {
-        free_grids(S, q, r.stream);
-        std::lock_guard<std::mutex> lk(S->mu);
-        S->used -= q->bytes;
-        complete_locked(S, q, st);
-        continue;
-      }
-      S->active.push_back(q);
-    }
-    if (__ps_trace && !admit.empty())
-      fprintf(__ps_trace, "physis_b200 serve: admitted %d requests in %.3f ms\n",
-              (int)admit.size(), (now_s() - ta) * 1e3);
+    admit_all(S, admit);
     if (S->active.empty()) continue;
     psb_status st = run_round(S, finished);
     if (st != PSB_OK) fail_active(S, finished, st);
