@@ -142,6 +142,9 @@ struct psb_server {
   cudaMemPool_t pool = nullptr;
   cudaStream_t copy = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  cudaEvent_t ev_prev = nullptr;  // end of the previous batched round (trace only)
+  bool have_prev = false;
+  double create_s = 0;
   double *d_norm = nullptr;
   std::thread worker;
 };
@@ -301,40 +304,44 @@ static double residual_of(const double *r4) {
   return r4[1] > 0 ? sqrt(r4[0] / r4[1]) : 0.0;
 }
 
-// Take the queued requests that fit the budget and the slot limit, in
-// arrival order (server lock held), after those already in `admit`.
-static void take_admissible_locked(psb_server *S, std::vector<SReq *> &admit) {
-  while (!S->queue.empty()) {
-    SReq *q = S->queue.front();
-    const size_t slots = S->active.size() + admit.size();
-    if (S->max_slots > 0 && slots >= (size_t)S->max_slots) break;
-    if (S->used + q->bytes > S->budget) break;
-    S->queue.pop_front();
-    S->used += q->bytes;
-    S->peak = std::max(S->peak, S->used);
-    admit.push_back(q);
-  }
+// Take the oldest queued request if it fits the budget and the slot limit
+// (server lock held); nullptr if none does.
+static SReq *take_one_locked(psb_server *S, size_t pending) {
+  if (S->queue.empty()) return nullptr;
+  SReq *q = S->queue.front();
+  if (S->max_slots > 0 && S->active.size() + pending >= (size_t)S->max_slots) return nullptr;
+  if (S->used + q->bytes > S->budget) return nullptr;
+  S->queue.pop_front();
+  S->used += q->bytes;
+  S->peak = std::max(S->peak, S->used);
+  return q;
 }
 
-// Allocate and fill the taken requests (runtime lock held) and add them to
-// the active list; a request that cannot be set up completes with its error.
-static void admit_all(psb_server *S, std::vector<SReq *> &admit) {
-  Runtime &r = rt();
+// Allocate and fill one taken request (runtime lock held) and add it to the
+// active list; a request that cannot be set up completes with its error.
+static void admit_one(psb_server *S, SReq *q) {
   const double ta = now_s();
-  for (SReq *q : admit) {
-    psb_status st = admit_request(S, q);
-    if (st != PSB_OK) {
-      free_grids(S, q, r.stream);
-      std::lock_guard<std::mutex> lk(S->mu);
-      S->used -= q->bytes;
-      complete_locked(S, q, st);
-      continue;
-    }
-    S->active.push_back(q);
+  psb_status st = admit_request(S, q);
+  if (__ps_trace)
+    fprintf(__ps_trace, "physis_b200 serve: t=%.3f s set up request %lld (kind %d, %dx%dx%d, %.1f MB) "
+            "in %.3f ms\n", ta - S->create_s, (long long)q->id, q->kind, q->q.dims[0],
+            q->q.dims[1], q->q.dims[2], q->bytes / 1e6, (now_s() - ta) * 1e3);
+  if (st != PSB_OK) {
+    free_grids(S, q, rt().stream);
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->used -= q->bytes;
+    complete_locked(S, q, st);
+    return;
   }
+  S->active.push_back(q);
+}
+
+static void admit_all(psb_server *S, std::vector<SReq *> &admit) {
+  const double ta = now_s();
+  for (SReq *q : admit) admit_one(S, q);
   if (__ps_trace && !admit.empty())
-    fprintf(__ps_trace, "physis_b200 serve: admitted %d requests in %.3f ms\n",
-            (int)admit.size(), (now_s() - ta) * 1e3);
+    fprintf(__ps_trace, "physis_b200 serve: t=%.3f s admitted %d requests in %.3f ms\n",
+            ta - S->create_s, (int)admit.size(), (now_s() - ta) * 1e3);
   admit.clear();
 }
 
@@ -391,26 +398,47 @@ static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
   for (SReq *q : finished) PSB_CHECK(retire_copy(S, q));
   finished.clear();
   // Requests that arrived meanwhile are set up while the round runs (their
-  // allocations and fills queue behind it) and join the next round.
+  // allocations and fills queue behind it) and join the next round. Setting
+  // one up can take milliseconds of host time (a growing pool maps new
+  // memory), so after the first one the worker stops when the round ends
+  // and leaves the rest for the next round: the device never waits on a
+  // long admission.
   {
-    std::vector<SReq *> admit;
-    {
-      std::lock_guard<std::mutex> lk(S->mu);
-      take_admissible_locked(S, admit);
+    const double ta = now_s();
+    int admitted = 0;
+    for (;;) {
+      if (admitted && cudaEventQuery(S->ev1) != cudaErrorNotReady) break;
+      SReq *q;
+      {
+        std::lock_guard<std::mutex> lk(S->mu);
+        q = take_one_locked(S, 0);
+      }
+      if (!q) break;
+      admit_one(S, q);
+      admitted++;
     }
-    admit_all(S, admit);
+    if (__ps_trace && admitted)
+      fprintf(__ps_trace, "physis_b200 serve: t=%.3f s admitted %d requests in %.3f ms\n",
+              ta - S->create_s, admitted, (now_s() - ta) * 1e3);
   }
   const double t2 = now_s();
   PSB_TRY(cudaEventSynchronize(S->ev1));
   const double t3 = now_s();
   float ms = 0;
   cudaEventElapsedTime(&ms, S->ev0, S->ev1);
-  if (__ps_trace)
+  if (__ps_trace) {
+    // Device idle time between the previous round's end and this one's start.
+    float idle = -1;
+    if (S->have_prev) cudaEventElapsedTime(&idle, S->ev_prev, S->ev0);
     fprintf(__ps_trace,
-            "physis_b200 serve: round of %d requests (%lld points/step, %d steps), %d retired; "
-            "host prepare %.3f ms, launch+retire %.3f ms, wait %.3f ms; device %.3f ms\n",
-            n, (long long)points, R, nretire, (t1 - t0) * 1e3, (t2 - t1) * 1e3, (t3 - t2) * 1e3,
-            ms);
+            "physis_b200 serve: t=%.3f s round of %d requests (%lld points/step, %d steps), "
+            "%d retired; host prepare %.3f ms, launch+retire %.3f ms, wait %.3f ms; device %.3f "
+            "ms, idle before %.3f ms\n",
+            t0 - S->create_s, n, (long long)points, R, nretire, (t1 - t0) * 1e3,
+            (t2 - t1) * 1e3, (t3 - t2) * 1e3, ms, idle);
+    std::swap(S->ev1, S->ev_prev);
+    S->have_prev = true;
+  }
   int err = 0;
   PSB_TRY(cudaMemcpy(&err, r.d_error, sizeof(int), cudaMemcpyDeviceToHost));
   if (err) {
@@ -481,7 +509,10 @@ static void worker_batched(psb_server *S) {
     {
       std::unique_lock<std::mutex> lk(S->mu);
       poll_retiring_locked(S, false);
-      take_admissible_locked(S, admit);
+      // With requests active, new ones are set up while a round runs; with
+      // none, one is set up here to start the next round.
+      if (S->active.empty())
+        if (SReq *q = take_one_locked(S, 0)) admit.push_back(q);
       if (admit.empty() && S->active.empty()) {
         if (!finished.empty()) {
           // Nothing to overlap with: send the results now.
@@ -653,6 +684,7 @@ psb_status psb_server_create(size_t mem_budget_bytes, int max_slots, int mode, p
   S->max_slots = max_slots;
   S->mode = mode;
   S->device = r.device;
+  S->create_s = now_s();
   cudaMemPoolProps props;
   memset(&props, 0, sizeof(props));
   props.allocType = cudaMemAllocationTypePinned;
@@ -667,6 +699,7 @@ psb_status psb_server_create(size_t mem_budget_bytes, int max_slots, int mode, p
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&S->copy, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreate(&S->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&S->ev1);
+  if (e == cudaSuccess) e = cudaEventCreate(&S->ev_prev);
   if (e == cudaSuccess) e = cudaMalloc(&S->d_norm, sizeof(double) * 2 * kNormBlocks);
   if (e != cudaSuccess) {
     psb_status st = cuda_status(e, "psb_server_create");
@@ -674,6 +707,7 @@ psb_status psb_server_create(size_t mem_budget_bytes, int max_slots, int mode, p
     if (S->copy) cudaStreamDestroy(S->copy);
     if (S->ev0) cudaEventDestroy(S->ev0);
     if (S->ev1) cudaEventDestroy(S->ev1);
+    if (S->ev_prev) cudaEventDestroy(S->ev_prev);
     delete S;
     return st;
   }
@@ -798,6 +832,7 @@ psb_status psb_server_destroy(psb_server *S) {
   cudaFree(S->d_norm);
   cudaEventDestroy(S->ev0);
   cudaEventDestroy(S->ev1);
+  cudaEventDestroy(S->ev_prev);
   cudaStreamDestroy(S->copy);
   cudaMemPoolDestroy(S->pool);
   delete S;
