@@ -134,11 +134,12 @@ enum { kItemEnd = 1, kItemSkip = 2 };
 static_assert(704 + kQ * sizeof(ItemDesc) <= kSmemRing, "item descriptors overlap the ring");
 
 __device__ __forceinline__ int upper_index(const int64_t *a, int n, int64_t v) {
-  // largest i in [0, n) with a[i] <= v (a non-decreasing, a[0] = 0)
+  // largest i in [0, n) with a[i] <= v (a non-decreasing, a[0] = 0); the
+  // work-list tables are read-only during a launch (non-coherent loads)
   int lo = 0, hi = n - 1;
   while (lo < hi) {
     int mid = (lo + hi + 1) >> 1;
-    if (a[mid] <= v) lo = mid;
+    if (__ldg(a + mid) <= v) lo = mid;
     else hi = mid - 1;
   }
   return lo;
@@ -208,10 +209,10 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, const 
       flags = kItemEnd;
     } else {
       s = upper_index(B.step_offset, B.max_steps + 1, item);
-      const int64_t local = item - B.step_offset[s];
+      const int64_t local = item - __ldg(B.step_offset + s);
       const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
-      m = B.order[k];
-      t = (int)(local - B.tile_prefix[k]);
+      m = __ldg(B.order + k);
+      t = (int)(local - __ldg(B.tile_prefix + k));
       M = &B.members[m];
       // Every tile of step s-1 of this member, and its convergence decision.
       const unsigned need = (unsigned)s * step_unit(*M);
@@ -580,22 +581,24 @@ static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int
   }
 }
 
-// Planes per item. 64 when the kind's members together give enough items
-// per step for several waves of CTAs (long items, few halo planes);
-// otherwise each member takes the longest z chunk (32 down to 4) that cuts
-// one of its steps into that many items, so a few large members are not
-// quantised into a fraction of a wave at every step and a small member's
-// steps (a chain of dependent launches' worth of work) stay short.
+// Planes per item. The members of a kind together should give enough items
+// per step for several waves of CTAs (items_target()); each item's fixed
+// costs (a descriptor, a dependency check, two halo planes) favour long
+// chunks. So the kind takes the longest chunk `floor` (64 down to 4) at
+// which its members together reach the target, and a member whose own
+// steps reach it with a longer chunk takes that one: a few large members
+// are not quantised into a fraction of a wave at every step, many small
+// members are not cut finer than the batch needs, and a lone small
+// member's steps (a chain of dependent launches' worth of work) stay short.
 static int64_t items_target() { return (int64_t)rt().sm_count * 6; }
 
-static int pick_zchunk(int64_t tiles_xy, int nz, bool short_chunks) {
-  if (!short_chunks) return 64;
-  for (int zc = 64; zc > 4; zc >>= 1)
+static int pick_zchunk(int64_t tiles_xy, int nz, int floor) {
+  for (int zc = 64; zc > floor; zc >>= 1)
     if (tiles_xy * ((nz + zc - 1) / zc) >= items_target()) return zc;
-  return 4;
+  return floor;
 }
 
-static TmaGeom batch_dgeom(const GridImpl *g, bool short_chunks) {
+static TmaGeom batch_dgeom(const GridImpl *g, int zc_floor) {
   TmaGeom geo;
   pick_shape(g->pub.dim[0], g->pub.dim[1], kVY, &geo.tx_threads, &geo.ty_threads);
   const int TX = geo.tx_threads * 4, TY = geo.ty_threads * kVY;
@@ -607,13 +610,13 @@ static TmaGeom batch_dgeom(const GridImpl *g, bool short_chunks) {
   geo.x_base = 0;
   geo.tiles_x = (g->pub.dim[0] + TX - 1) / TX;
   geo.tiles_y = (g->pub.dim[1] + TY - 1) / TY;
-  geo.zchunk = pick_zchunk((int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2], short_chunks);
+  geo.zchunk = pick_zchunk((int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2], zc_floor);
   geo.stages = kBStages;
   geo.stage_bytes = kind_stage_bytes(0);
   return geo;
 }
 
-static HimenoGeom batch_hgeom(const GridImpl *g, bool short_chunks) {
+static HimenoGeom batch_hgeom(const GridImpl *g, int zc_floor) {
   HimenoGeom geo;
   // interior domain [1, n-1): tiles start at x = 0 (x_base), y = 1.
   pick_shape(g->pub.dim[0] - 1, g->pub.dim[1] - 2, 1, &geo.tx_threads, &geo.ty_threads);
@@ -626,7 +629,7 @@ static HimenoGeom batch_hgeom(const GridImpl *g, bool short_chunks) {
   geo.x_base = 0;
   geo.tiles_x = (g->pub.dim[0] - 1 + TX - 1) / TX;
   geo.tiles_y = (g->pub.dim[1] - 2 + TY - 1) / TY;
-  geo.zchunk = pick_zchunk((int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2] - 2, short_chunks);
+  geo.zchunk = pick_zchunk((int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2] - 2, zc_floor);
   geo.stages = kBStages;
   geo.stage_bytes = kind_stage_bytes(1);
   geo.nx = g->pub.dim[0];
@@ -647,22 +650,28 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
   b->members.assign(n, BMember());
   std::vector<CUtensorMap> tmaps(2 * std::max(1, n));
   std::vector<int> coef_map(n, -1);  // index of a Himeno member's 12 coefficient maps
-  // Items per step of each kind with 64-plane chunks.
-  bool short_chunks[2];
-  {
-    int64_t items[2] = {0, 0};
-    for (int i = 0; i < n; i++) {
-      if (steps[i] <= 0) continue;
-      const GridImpl *g0 = b->hm[i].grids[0];
-      if (b->hm[i].kind == BK_HIMENO) {
-        const HimenoGeom hg = batch_hgeom(g0, false);
-        items[1] += (int64_t)hg.tiles_x * hg.tiles_y * ((g0->pub.dim[2] - 2 + 63) / 64);
-      } else {
-        const TmaGeom dg = batch_dgeom(g0, false);
-        items[0] += (int64_t)dg.tiles_x * dg.tiles_y * ((g0->pub.dim[2] + 63) / 64);
+  // The longest z chunk at which each kind's members together give
+  // items_target() items per step (4 if none does).
+  int zc_floor[2] = {4, 4};
+  for (int k = 0; k < 2; k++) {
+    for (int zc = 64; zc > 4; zc >>= 1) {
+      int64_t items = 0;
+      for (int i = 0; i < n; i++) {
+        if (steps[i] <= 0 || (b->hm[i].kind == BK_HIMENO) != (k == 1)) continue;
+        const GridImpl *g0 = b->hm[i].grids[0];
+        if (k == 1) {
+          const HimenoGeom hg = batch_hgeom(g0, 64);
+          items += (int64_t)hg.tiles_x * hg.tiles_y * ((g0->pub.dim[2] - 2 + zc - 1) / zc);
+        } else {
+          const TmaGeom dg = batch_dgeom(g0, 64);
+          items += (int64_t)dg.tiles_x * dg.tiles_y * ((g0->pub.dim[2] + zc - 1) / zc);
+        }
+      }
+      if (items >= items_target()) {
+        zc_floor[k] = zc;
+        break;
       }
     }
-    for (int k = 0; k < 2; k++) short_chunks[k] = items[k] < items_target();
   }
   int64_t partial_slots = 0;
   for (int i = 0; i < n; i++) {
@@ -682,7 +691,7 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     M.sz = g0->sz;
     const CUtensorMap *a = nullptr, *c = nullptr;
     if (h.kind == BK_HIMENO) {
-      M.hg = batch_hgeom(g0, short_chunks[1]);
+      M.hg = batch_hgeom(g0, zc_floor[1]);
       for (int k = 0; k < 3; k++) {
         M.dom.lo[k] = 1;
         M.dom.hi[k] = g0->pub.dim[k] - 1;
@@ -701,7 +710,7 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
         tmaps.push_back(*cm);
       }
     } else {
-      M.dg = batch_dgeom(g0, short_chunks[0]);
+      M.dg = batch_dgeom(g0, zc_floor[0]);
       for (int k = 0; k < 3; k++) {
         M.dom.lo[k] = 0;
         M.dom.hi[k] = g0->pub.dim[k];
