@@ -314,7 +314,9 @@ typedef enum {
   PSB_ERR_TIMEOUT = 5,        /* a bounded device-side wait gave up */
   PSB_ERR_UNSUPPORTED = 6,    /* valid request this build does not run */
   PSB_ERR_CANCELLED = 7,      /* a serving request was cancelled */
-  PSB_ERR_BUSY = 8            /* queue full / resource in use */
+  PSB_ERR_BUSY = 8,           /* queue full / resource in use */
+  PSB_ERR_BOUNDS = 9          /* a compiled stencil read outside its grid
+                                 (the read returned 0, nothing was touched) */
 } psb_status;
 
 /* Halo (ghost) width of pitched grids, in cells, in y and z. In x the halo
@@ -344,7 +346,9 @@ typedef enum {
    * grids (p_in, p_out, a0, a1, a2, a3, b0, b1, b2, c0, c1, c2, bnd, wrk1);
    * scalar omega. float only. */
   PSB_KERNEL_HIMENO19 = 3,
-  PSB_KERNEL_FIRST_GENERIC = 64
+  PSB_KERNEL_FIRST_GENERIC = 64,
+  /* Ids of compiled stencils (psb_compiled_register) start here. */
+  PSB_KERNEL_FIRST_COMPILED = 1 << 16
 } psb_kernel;
 
 /* Per-access boundary handling of a generic term (reference forms:
@@ -448,6 +452,50 @@ psb_status psb_grid_copy(__PSGrid *dst, const __PSGrid *src);
 
 /* Register a generic stencil; *kernel_id is usable with PSStencilMap. */
 psb_status psb_generic_register(const psb_generic_stencil *desc, int *kernel_id);
+
+/* Compiled stencils: a DSL stencil function (docs/programming.md:117-190 of
+ * the reference: `const int` index parameters, grids, scalars;
+ * PSGridGet / PSGridGetPeriodic / PSGridEmit / PSGridDim) translated by the
+ * front end physis_b200/dsl.py into a CUDA kernel of its own shared library,
+ * in place of the reference's translator (translator/cuda_translator.cc,
+ * which needs ROSE). The library exports a launch function; registering it
+ * gives a kernel id usable with PSStencilMap / PSStencilRun like a built-in.
+ * At each application the runtime passes the domain, the bound grids' views
+ * and the map's scalars; the kernel runs on the given stream. */
+typedef struct {
+  void *origin;          /* element (0,0,0) */
+  int64_t sy, sz;        /* element strides of y and z */
+  int n[3];              /* extents (1 past the grid's dimensions) */
+  int type;              /* PSPrimitiveType */
+} psb_grid_view;
+
+typedef struct {
+  int lo[3], hi[3];      /* domain, half-open; unused dimensions [0, 1) */
+  int color;             /* -1 every point; 0 / 1 red / black points */
+  int ngrids, nparams;
+  psb_grid_view grids[PSB_MAX_GRIDS];
+  double params[PSB_MAX_PARAMS];
+  int *error;            /* device word; a read outside its grid sets it to
+                            PSB_ERR_BOUNDS (reported by psb_sync / copy-out) */
+  int device;            /* CUDA device of the grids and the stream */
+} psb_launch_args;
+
+typedef psb_status (*psb_compiled_launch)(const psb_launch_args *args, void *cuda_stream);
+
+typedef struct {
+  int ndims;                          /* index parameters of the function */
+  int ngrids;
+  int grid_type[PSB_MAX_GRIDS];       /* element type of each grid parameter */
+  int grid_ndims[PSB_MAX_GRIDS];
+  int emits[PSB_MAX_GRIDS];           /* 1 if the function emits into the grid */
+  int reads_offset[PSB_MAX_GRIDS];    /* 1 if it reads the grid off the point */
+  int nparams;                        /* scalar parameters after the grids */
+  int param_type[PSB_MAX_PARAMS];     /* PS_FLOAT / PS_DOUBLE / PS_INT / PS_LONG
+                                         (how PSStencilMap's varargs read them) */
+  psb_compiled_launch launch;
+} psb_compiled_stencil;
+
+psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_id);
 
 /* Non-varargs map and run. grids: ngrids grid pointers in the kernel's
  * order; params: nparams scalars (converted to the kernel's type). */

@@ -44,9 +44,10 @@ BOUNDARY_NONE, BOUNDARY_PERIODIC, BOUNDARY_CLAMP = 0, 1, 2
 IMPL_AUTO, IMPL_PLAIN, IMPL_TMA, IMPL_GENERIC = 0, 1, 2, 3
 STATUS = {0: "ok", 1: "invalid argument", 2: "out of device memory or budget", 3: "CUDA error",
           4: "runtime not initialised", 5: "device-side wait timed out", 6: "unsupported",
-          7: "cancelled", 8: "busy"}
+          7: "cancelled", 8: "busy", 9: "read outside the grid"}
 PSB_OK, PSB_ERR_INVALID, PSB_ERR_NOMEM, PSB_ERR_CUDA = 0, 1, 2, 3
 PSB_ERR_NOT_INIT, PSB_ERR_TIMEOUT, PSB_ERR_UNSUPPORTED, PSB_ERR_CANCELLED, PSB_ERR_BUSY = 4, 5, 6, 7, 8
+PSB_ERR_BOUNDS = 9
 
 NP_TYPE = {PS_FLOAT: np.float32, PS_DOUBLE: np.float64, PS_INT: np.int32, PS_LONG: np.int64}
 
@@ -89,6 +90,31 @@ class GenericStencilStruct(ctypes.Structure):
                 ("accum_type", ctypes.c_int), ("nterms", ctypes.c_int),
                 ("terms", Term * PSB_MAX_TERMS), ("has_post", ctypes.c_int), ("post", Factor),
                 ("redblack", ctypes.c_int)]
+
+
+class GridViewStruct(ctypes.Structure):
+    """psb_grid_view."""
+    _fields_ = [("origin", ctypes.c_void_p), ("sy", ctypes.c_int64), ("sz", ctypes.c_int64),
+                ("n", ctypes.c_int * 3), ("type", ctypes.c_int)]
+
+
+class LaunchArgs(ctypes.Structure):
+    """psb_launch_args."""
+    _fields_ = [("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3), ("color", ctypes.c_int),
+                ("ngrids", ctypes.c_int), ("nparams", ctypes.c_int),
+                ("grids", GridViewStruct * PSB_MAX_GRIDS),
+                ("params", ctypes.c_double * PSB_MAX_PARAMS), ("error", ctypes.c_void_p),
+                ("device", ctypes.c_int)]
+
+
+class CompiledStencilStruct(ctypes.Structure):
+    """psb_compiled_stencil."""
+    _fields_ = [("ndims", ctypes.c_int), ("ngrids", ctypes.c_int),
+                ("grid_type", ctypes.c_int * PSB_MAX_GRIDS),
+                ("grid_ndims", ctypes.c_int * PSB_MAX_GRIDS),
+                ("emits", ctypes.c_int * PSB_MAX_GRIDS),
+                ("reads_offset", ctypes.c_int * PSB_MAX_GRIDS), ("nparams", ctypes.c_int),
+                ("param_type", ctypes.c_int * PSB_MAX_PARAMS), ("launch", ctypes.c_void_p)]
 
 
 class TuneConfig(ctypes.Structure):
@@ -172,6 +198,8 @@ def _load():
         "psb_grid_copy": (S, [G, G]),
         "psb_grid_fill": (S, [G, ctypes.c_int, ctypes.c_uint64, ctypes.c_double, ctypes.c_double]),
         "psb_generic_register": (S, [ctypes.POINTER(GenericStencilStruct), ctypes.POINTER(ctypes.c_int)]),
+        "psb_compiled_register": (S, [ctypes.POINTER(CompiledStencilStruct),
+                                      ctypes.POINTER(ctypes.c_int)]),
         "psb_stencil_map": (S, [ctypes.c_int, ctypes.POINTER(PSDomain), ctypes.POINTER(G), ctypes.c_int,
                                 ctypes.POINTER(ctypes.c_double), ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
         "psb_stencil_map_rb": (S, [ctypes.c_int, ctypes.POINTER(PSDomain), ctypes.POINTER(G), ctypes.c_int,

@@ -121,6 +121,7 @@ struct Runtime {
   bool last_timed = false;
   std::vector<MapImpl> maps;
   std::vector<GenericDesc> generics;
+  std::vector<psb_compiled_stencil> compiled;
   std::map<TuneKey, psb_tune_config> tune;
   bool tune_loaded = false;
   std::string tune_path;

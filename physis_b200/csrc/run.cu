@@ -37,6 +37,38 @@ static const GenericDesc *generic_of(int kernel_id) {
   return &rt().generics[i];
 }
 
+static const psb_compiled_stencil *compiled_of(int kernel_id) {
+  int i = kernel_id - PSB_KERNEL_FIRST_COMPILED;
+  if (i < 0 || i >= (int)rt().compiled.size()) return nullptr;
+  return &rt().compiled[i];
+}
+
+// A map of a compiled stencil: grids of the declared types and ranks, a
+// domain inside every emitted grid (reads are bounds-checked in the kernel),
+// and no grid that is both emitted and read off the point unless red-black
+// ordering separates the two.
+static psb_status check_compiled_map(const MapImpl &m, const psb_compiled_stencil &d) {
+  if (m.ngrids != d.ngrids || m.nparams != d.nparams) return PSB_ERR_INVALID;
+  for (int i = 0; i < d.ngrids; i++) {
+    const GridImpl *g = m.grids[i];
+    if (type_size(d.grid_type[i]) != g->pub.elm_size || d.grid_ndims[i] != g->pub.num_dims)
+      return PSB_ERR_INVALID;
+    if (g->type >= 0 && g->type != d.grid_type[i]) return PSB_ERR_INVALID;
+  }
+  for (int k = 0; k < d.ndims; k++)
+    if (m.dom.local_min[k] < 0 || m.dom.local_max[k] < m.dom.local_min[k]) return PSB_ERR_INVALID;
+  for (int i = 0; i < d.ngrids; i++) {
+    if (!d.emits[i]) continue;
+    const GridImpl *g = m.grids[i];
+    for (int k = 0; k < d.ndims; k++)
+      if (m.dom.local_max[k] > g->pub.dim[k]) return PSB_ERR_INVALID;
+    if (m.color < 0)
+      for (int j = 0; j < d.ngrids; j++)
+        if (m.grids[j] == g && d.reads_offset[j]) return PSB_ERR_UNSUPPORTED;
+  }
+  return PSB_OK;
+}
+
 // Expected grid count / types of a kernel.
 // writes: false for a kernel-function reduction (nothing is stored, so an
 // emitted grid that is also read at offsets is fine).
@@ -72,6 +104,8 @@ static psb_status check_map(const MapImpl &m, bool writes = true) {
       return PSB_OK;
     }
     default: {
+      if (const psb_compiled_stencil *cd = compiled_of(m.kernel_id))
+        return check_compiled_map(m, *cd);
       const GenericDesc *gd = generic_of(m.kernel_id);
       if (!gd) return PSB_ERR_INVALID;
       const psb_generic_stencil &d = gd->host;
@@ -162,6 +196,32 @@ psb_status launch_map(MapImpl &m, int color, int64_t *launches) {
         if (m.dom.local_min[i] != 0 || m.dom.local_max[i] != o->pub.dim[i]) full = false;
       if (full) o->ghost_valid = PSB_BOUNDARY_PERIODIC;
     }
+  } else if (const psb_compiled_stencil *cd = compiled_of(m.kernel_id)) {
+    psb_launch_args a;
+    memset(&a, 0, sizeof(a));
+    for (int k = 0; k < 3; k++) {
+      a.lo[k] = k < cd->ndims ? m.dom.local_min[k] : 0;
+      a.hi[k] = k < cd->ndims ? m.dom.local_max[k] : 1;
+    }
+    a.color = color;
+    a.ngrids = m.ngrids;
+    a.nparams = m.nparams;
+    for (int i = 0; i < m.ngrids; i++) {
+      const GridView v = m.grids[i]->view();
+      a.grids[i].origin = v.origin;
+      a.grids[i].sy = v.sy;
+      a.grids[i].sz = v.sz;
+      for (int k = 0; k < 3; k++) a.grids[i].n[k] = v.n[k];
+      a.grids[i].type = cd->grid_type[i];
+    }
+    for (int i = 0; i < m.nparams; i++) a.params[i] = m.params[i];
+    a.error = r.d_error + 1;
+    a.device = r.device;
+    st = cd->launch(&a, (void *)s);
+    if (launches) (*launches)++;
+    for (int i = 0; i < m.ngrids; i++)
+      if (cd->emits[i] && m.grids[i]->layout == PSB_LAYOUT_PITCHED)
+        m.grids[i]->ghost_valid = PSB_BOUNDARY_NONE;
   } else {
     const GenericDesc *gd = generic_of(m.kernel_id);
     if (!gd) return set_status(PSB_ERR_INVALID);
@@ -400,6 +460,10 @@ static int kernel_ngrids(int kernel_id, int *nparams) {
     case PSB_KERNEL_DIFFUSION7_PERIODIC: *nparams = 7; return 2;
     case PSB_KERNEL_HIMENO19: *nparams = 1; return 14;
     default: {
+      if (const psb_compiled_stencil *cd = compiled_of(kernel_id)) {
+        *nparams = cd->nparams;
+        return cd->ngrids;
+      }
       const GenericDesc *gd = generic_of(kernel_id);
       *nparams = 0;
       return gd ? gd->host.ngrids : -1;
@@ -419,7 +483,18 @@ static PSStencil vmap(void *kernel, int color, va_list vl) {
   __PSGrid *grids[PSB_MAX_GRIDS];
   for (int i = 0; i < ng; i++) grids[i] = va_arg(vl, __PSGrid *);
   double params[PSB_MAX_PARAMS];
-  for (int i = 0; i < np; i++) params[i] = va_arg(vl, double);
+  // Varargs promote float to double; integer scalars of compiled stencils
+  // arrive as int / long.
+  const psb_compiled_stencil *cd = compiled_of(kid);
+  for (int i = 0; i < np; i++) {
+    const int t = cd ? cd->param_type[i] : PS_DOUBLE;
+    if (t == PS_INT)
+      params[i] = (double)va_arg(vl, int);
+    else if (t == PS_LONG)
+      params[i] = (double)va_arg(vl, long);
+    else
+      params[i] = va_arg(vl, double);
+  }
   PSStencil h = 0;
   psb_status s = make_map(kid, &dom, grids, ng, params, np, color, &h);
   if (s != PSB_OK) {
@@ -542,11 +617,30 @@ psb_status psb_stencil_map(int kernel_id, const __PSDomain *dom, __PSGrid *const
   return make_map(kernel_id, dom, grids, ngrids, params, nparams, -1, out);
 }
 
+psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_id) {
+  PSB_CHECK(ensure_init());
+  if (!desc || !kernel_id || !desc->launch) return set_status(PSB_ERR_INVALID);
+  const psb_compiled_stencil &d = *desc;
+  if (d.ndims < 1 || d.ndims > 3 || d.ngrids < 1 || d.ngrids > PSB_MAX_GRIDS || d.nparams < 0 ||
+      d.nparams > PSB_MAX_PARAMS)
+    return set_status(PSB_ERR_INVALID);
+  for (int i = 0; i < d.ngrids; i++)
+    if (type_size(d.grid_type[i]) == 0 || d.grid_ndims[i] < 1 || d.grid_ndims[i] > 3)
+      return set_status(PSB_ERR_INVALID);
+  for (int i = 0; i < d.nparams; i++)
+    if (type_size(d.param_type[i]) == 0) return set_status(PSB_ERR_INVALID);
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
+  r.compiled.push_back(d);
+  *kernel_id = PSB_KERNEL_FIRST_COMPILED + (int)r.compiled.size() - 1;
+  return PSB_OK;
+}
+
 psb_status psb_stencil_map_rb(int kernel_id, const __PSDomain *dom, __PSGrid *const *grids,
                               int ngrids, const double *params, int nparams, int color,
                               PSStencil *out) {
   if (color < 0 || color > 2) return set_status(PSB_ERR_INVALID);
-  if (!generic_of(kernel_id)) return set_status(PSB_ERR_UNSUPPORTED);
+  if (!generic_of(kernel_id) && !compiled_of(kernel_id)) return set_status(PSB_ERR_UNSUPPORTED);
   return make_map(kernel_id, dom, grids, ngrids, params, nparams, color, out);
 }
 

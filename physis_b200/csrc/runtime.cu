@@ -349,6 +349,13 @@ static psb_status check_device_error() {
     cudaMemset(rt().d_error, 0, sizeof(int));
     return set_status(PSB_ERR_TIMEOUT);
   }
+  // Word 1: a compiled stencil's read outside its grid.
+  e = cudaMemcpy(&err, rt().d_error + 1, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_status(e, "read error word");
+  if (err) {
+    cudaMemset(rt().d_error + 1, 0, sizeof(int));
+    return set_status(PSB_ERR_BOUNDS);
+  }
   return PSB_OK;
 }
 
@@ -705,6 +712,7 @@ const char *psb_status_string(psb_status s) {
     case PSB_ERR_UNSUPPORTED: return "unsupported";
     case PSB_ERR_CANCELLED: return "cancelled";
     case PSB_ERR_BUSY: return "busy";
+    case PSB_ERR_BOUNDS: return "read outside the grid";
   }
   return "unknown";
 }

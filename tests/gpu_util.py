@@ -7,15 +7,18 @@ from tests.golden import cases as C
 LAYOUTS = {"pitched": ps.LAYOUT_PITCHED, "dense": ps.LAYOUT_DENSE}
 
 
-def run_case_gpu(case, layout):
-    """Execute one system-test case on the GPU; returns the dumped array."""
+def run_case_gpu(case, layout, kernel_id=None, params=()):
+    """Execute one system-test case on the GPU with its generic descriptor
+    (or the given kernel and scalars); returns the dumped array."""
     grids = []
     for kind, (t, dims) in zip(case["init"], case["grids"]):
         g = ps.grid_new(t, dims, layout)
         ps.PSGridCopyin(g, C.init_array(kind, t, dims))
         grids.append(g)
-    d = case["desc"]
-    st = ps.GenericStencil(d["ndims"], d["grids"], d["out"], d["accum"], d["terms"], d.get("post"))
+    if kernel_id is None:
+        d = case["desc"]
+        kernel_id = ps.GenericStencil(d["ndims"], d["grids"], d["out"], d["accum"], d["terms"],
+                                      d.get("post")).kernel_id
     lo, hi = case["dom"]
     nd = len(lo)
     dom = [ps.PSDomain1DNew, ps.PSDomain2DNew, ps.PSDomain3DNew][nd - 1](
@@ -24,9 +27,9 @@ def run_case_gpu(case, layout):
     for slots, color in case["run"]:
         args = [grids[s] for s in slots]
         if color == 2:
-            maps.append(ps.PSStencilMapRedBlack(st.kernel_id, dom, *args))
+            maps.append(ps.PSStencilMapRedBlack(kernel_id, dom, *args, *params))
         else:
-            maps.append(ps.PSStencilMap(st.kernel_id, dom, *args))
+            maps.append(ps.PSStencilMap(kernel_id, dom, *args, *params))
     ps.PSStencilRun(*maps, case["iters"])
     out = ps.PSGridCopyout(grids[case["dump"]])
     for g in grids:

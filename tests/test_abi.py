@@ -80,8 +80,10 @@ def test_ctypes_structs_match_header(tmp_path):
     import physis_b200 as ps
     structs = {"psb_request": ps.Request, "psb_result": ps.Result,
                "psb_tune_config": ps.TuneConfig, "psb_generic_stencil": ps.GenericStencilStruct,
-               "psb_user_type": ps.UserType}
-    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "physis_b200.h"',
+               "psb_user_type": ps.UserType, "psb_grid_view": ps.GridViewStruct,
+               "psb_launch_args": ps.LaunchArgs, "psb_compiled_stencil": ps.CompiledStencilStruct}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include <stdint.h>',
+             '#include "physis_b200.h"',
              'int main(void) {']
     for cname, cls in structs.items():
         lines.append('printf("%s sizeof %%zu\\n", sizeof(%s));' % (cname, cname))

@@ -1,0 +1,111 @@
+"""The DSL front end on the CPU: translation, DSL rule checks and an sm_100a
+cross-compile of the generated kernels (nothing here needs a GPU)."""
+import ctypes
+import glob
+import os
+
+import pytest
+
+import physis_b200 as ps
+from physis_b200 import dsl
+from tests.golden import dsl_cases as D
+
+REF_TESTS = "/root/reference/tests/system_tests/test_cases"
+
+
+def _all_case_source():
+    seen, parts = set(), []
+    for src, fn, _ in D.dsl_cases().values():
+        if fn not in seen:
+            seen.add(fn)
+            parts.append(src)
+    return "\n".join(parts)
+
+
+def test_translation_metadata():
+    _, infos = dsl.translate(_all_case_source())
+    k = infos["sum7"]
+    assert k.ndims == 3 and k.grid_types == [ps.PS_FLOAT, ps.PS_FLOAT]
+    assert k.emits == [0, 1] and k.reads_offset == [1, 0]
+    n = infos["neumann7"]
+    assert [t for _, t in n.scalars] == [ps.PS_FLOAT] * 7
+    m = infos["weighted_planes"]
+    assert [nd for _, _, nd in m.grids] == [3, 3, 1, 2]
+    assert m.axes[2] == [0] and m.axes[3] == [1, 2]
+    assert infos["line3"].ndims == 1 and infos["plane9"].ndims == 2
+    rb = infos["rb7"]
+    assert rb.emits == [1] and rb.reads_offset == [1]
+    mix = infos["mixed_types"]
+    assert mix.grid_types == [ps.PS_FLOAT, ps.PS_DOUBLE, ps.PS_INT] and mix.emits == [0, 1, 0]
+
+
+def test_generated_code_keeps_c_semantics():
+    src = """
+    #define SCALE 0.5
+    void f(const int x, const int y, const int z, PSGrid3DFloat a, PSGrid3DFloat b, float t) {
+      float v = PSGridGet(a, x, y, z) / 7.0 * t;
+      PSGridEmit(b, sqrt(v) * SCALE + fabsf(v));
+    }
+    """
+    cu, infos = dsl.translate(src)
+    assert "sqrt((double) v)" in cu          # C promotes the float argument
+    assert "fabsf(v)" in cu                  # the float function stays as written
+    assert "0.5" in cu and "SCALE" not in cu  # the source's own macros are expanded
+    assert "__psb_emit(b, x, y, z" in cu
+
+
+@pytest.mark.parametrize("src, msg", [
+    ("void f(PSGrid3DFloat a, const int x) { }", "no stencil function"),
+    ("void f(const int x, PSGrid1DFloat a, float *p) { PSGridEmit(a, 0); }", "parameters must"),
+    ("void f(const int x, PSGrid1DFloat a, PSGrid1DFloat b) { float v = PSGridGet(3, x); }",
+     "grid parameter"),
+    ("void f(const int x, const int y, PSGrid2DFloat a, PSGrid1DFloat b) { PSGridEmit(b, 1); }",
+     "PSGridEmit into a 1-D grid"),
+    ("void f(const int x, PSGrid1DFloat a, PSGrid1DFloat b) { PSGridEmit(b, PSGridGet(a, x, x)); }",
+     "takes 1 indices"),
+    ("void f(const int x, PSGrid1DFloat a) { void *p = &a; }", "address of a grid"),
+    ("void f(const int x, PSGrid1DFloat a) { PSGridCopyin(a, 0); }", "not available"),
+    ("int f(const int x, PSGrid1DFloat a) { return 0; }", "return void"),
+    ("void f(const int x, PSGrid1DFloat a) { float v = ; }", "cannot parse"),
+])
+def test_dsl_rule_violations_are_reported(src, msg):
+    with pytest.raises(dsl.DSLError, match=msg):
+        dsl.translate(src)
+
+
+def test_generated_library_builds_for_sm100a(tmp_path):
+    """nvcc compiles every case's kernel; the library exports the launch and
+    describe functions of each stencil, and the descriptions match."""
+    cu, infos = dsl.translate(_all_case_source())
+    so = dsl.build_library(cu, str(tmp_path))
+    lib = ctypes.CDLL(so)
+    for name, info in infos.items():
+        assert hasattr(lib, "psb_dsl_launch_" + name)
+        d = ps.CompiledStencilStruct()
+        getattr(lib, "psb_dsl_describe_" + name)(ctypes.byref(d))
+        assert d.ndims == info.ndims and d.ngrids == len(info.grids)
+        assert list(d.grid_type)[:d.ngrids] == info.grid_types
+        assert list(d.emits)[:d.ngrids] == info.emits
+        assert list(d.reads_offset)[:d.ngrids] == info.reads_offset
+        assert d.nparams == len(info.scalars) and d.launch
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_TESTS), reason="reference sources not present")
+def test_reference_system_tests_translate():
+    """Every stencil function of the reference's system tests translates,
+    except the user-defined point types (struct grids, a separate API here)."""
+    done = 0
+    for f in sorted(glob.glob(os.path.join(REF_TESTS, "test_*.c"))):
+        if ".manual." in f:
+            continue
+        text = open(f).read()
+        if "PSGridEmit" not in text:
+            continue
+        if "DeclareGrid" in text:
+            with pytest.raises(dsl.DSLError):
+                dsl.translate(text)
+            continue
+        _, infos = dsl.translate(text)
+        assert infos, f
+        done += 1
+    assert done >= 25
