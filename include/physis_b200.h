@@ -455,13 +455,16 @@ psb_status psb_generic_register(const psb_generic_stencil *desc, int *kernel_id)
 
 /* Compiled stencils: a DSL stencil function (docs/programming.md:117-190 of
  * the reference: `const int` index parameters, grids, scalars;
- * PSGridGet / PSGridGetPeriodic / PSGridEmit / PSGridDim) translated by the
- * front end physis_b200/dsl.py into a CUDA kernel of its own shared library,
- * in place of the reference's translator (translator/cuda_translator.cc,
- * which needs ROSE). The library exports a launch function; registering it
- * gives a kernel id usable with PSStencilMap / PSStencilRun like a built-in.
- * At each application the runtime passes the domain, the bound grids' views
- * and the map's scalars; the kernel runs on the given stream. */
+ * PSGridGet / PSGridGetPeriodic / PSGridEmit / PSGridEmitUtype / PSGridDim)
+ * translated by the front end physis_b200/dsl.py into a CUDA kernel of its
+ * own shared library, in place of the reference's translator
+ * (translator/cuda_translator.cc, which needs ROSE). The library exports a
+ * launch function; registering it gives a kernel id usable with
+ * PSStencilMap / PSStencilRun like a built-in. At each application the
+ * runtime passes the domain, one view per scalar component of the bound
+ * grids (a grid of a user-defined point type gives one per component, in
+ * field order) and the map's scalars; the kernel runs on the given stream. */
+#define PSB_MAX_VIEWS 64
 typedef struct {
   void *origin;          /* element (0,0,0) */
   int64_t sy, sz;        /* element strides of y and z */
@@ -472,8 +475,8 @@ typedef struct {
 typedef struct {
   int lo[3], hi[3];      /* domain, half-open; unused dimensions [0, 1) */
   int color;             /* -1 every point; 0 / 1 red / black points */
-  int ngrids, nparams;
-  psb_grid_view grids[PSB_MAX_GRIDS];
+  int nviews, nparams;
+  psb_grid_view views[PSB_MAX_VIEWS];
   double params[PSB_MAX_PARAMS];
   int *error;            /* device word; a read outside its grid sets it to
                             PSB_ERR_BOUNDS (reported by psb_sync / copy-out) */
@@ -484,11 +487,15 @@ typedef psb_status (*psb_compiled_launch)(const psb_launch_args *args, void *cud
 
 typedef struct {
   int ndims;                          /* index parameters of the function */
-  int ngrids;
-  int grid_type[PSB_MAX_GRIDS];       /* element type of each grid parameter */
+  int ngrids;                         /* grid parameters */
+  int grid_type[PSB_MAX_GRIDS];       /* element type, PS_USER for a point type */
   int grid_ndims[PSB_MAX_GRIDS];
-  int emits[PSB_MAX_GRIDS];           /* 1 if the function emits into the grid */
-  int reads_offset[PSB_MAX_GRIDS];    /* 1 if it reads the grid off the point */
+  int grid_components[PSB_MAX_GRIDS]; /* views of the grid: 1, or the point
+                                         type's scalar components */
+  int nviews;
+  int view_type[PSB_MAX_VIEWS];       /* element type of each view */
+  int view_emits[PSB_MAX_VIEWS];      /* 1 if the function emits into the view */
+  int view_reads_offset[PSB_MAX_VIEWS]; /* 1 if it reads the view off the point */
   int nparams;                        /* scalar parameters after the grids */
   int param_type[PSB_MAX_PARAMS];     /* PS_FLOAT / PS_DOUBLE / PS_INT / PS_LONG
                                          (how PSStencilMap's varargs read them) */

@@ -98,11 +98,14 @@ class GridViewStruct(ctypes.Structure):
                 ("n", ctypes.c_int * 3), ("type", ctypes.c_int)]
 
 
+PSB_MAX_VIEWS = 64
+
+
 class LaunchArgs(ctypes.Structure):
     """psb_launch_args."""
     _fields_ = [("lo", ctypes.c_int * 3), ("hi", ctypes.c_int * 3), ("color", ctypes.c_int),
-                ("ngrids", ctypes.c_int), ("nparams", ctypes.c_int),
-                ("grids", GridViewStruct * PSB_MAX_GRIDS),
+                ("nviews", ctypes.c_int), ("nparams", ctypes.c_int),
+                ("views", GridViewStruct * PSB_MAX_VIEWS),
                 ("params", ctypes.c_double * PSB_MAX_PARAMS), ("error", ctypes.c_void_p),
                 ("device", ctypes.c_int)]
 
@@ -112,8 +115,10 @@ class CompiledStencilStruct(ctypes.Structure):
     _fields_ = [("ndims", ctypes.c_int), ("ngrids", ctypes.c_int),
                 ("grid_type", ctypes.c_int * PSB_MAX_GRIDS),
                 ("grid_ndims", ctypes.c_int * PSB_MAX_GRIDS),
-                ("emits", ctypes.c_int * PSB_MAX_GRIDS),
-                ("reads_offset", ctypes.c_int * PSB_MAX_GRIDS), ("nparams", ctypes.c_int),
+                ("grid_components", ctypes.c_int * PSB_MAX_GRIDS), ("nviews", ctypes.c_int),
+                ("view_type", ctypes.c_int * PSB_MAX_VIEWS),
+                ("view_emits", ctypes.c_int * PSB_MAX_VIEWS),
+                ("view_reads_offset", ctypes.c_int * PSB_MAX_VIEWS), ("nparams", ctypes.c_int),
                 ("param_type", ctypes.c_int * PSB_MAX_PARAMS), ("launch", ctypes.c_void_p)]
 
 

@@ -43,28 +43,54 @@ static const psb_compiled_stencil *compiled_of(int kernel_id) {
   return &rt().compiled[i];
 }
 
-// A map of a compiled stencil: grids of the declared types and ranks, a
-// domain inside every emitted grid (reads are bounds-checked in the kernel),
-// and no grid that is both emitted and read off the point unless red-black
-// ordering separates the two.
+// The grid behind each view of a compiled stencil's map: a primitive grid
+// gives one view, a grid of a user-defined point type one per component.
+static int compiled_views(const MapImpl &m, const psb_compiled_stencil &d,
+                          GridImpl **views) {
+  int v = 0;
+  for (int i = 0; i < m.ngrids; i++) {
+    GridImpl *g = m.grids[i];
+    if (d.grid_type[i] == PS_USER) {
+      if ((int)g->comps.size() != d.grid_components[i] || v + d.grid_components[i] > PSB_MAX_VIEWS)
+        return -1;
+      for (GridImpl *c : g->comps) views[v++] = c;
+    } else {
+      if (v >= PSB_MAX_VIEWS) return -1;
+      views[v++] = g;
+    }
+  }
+  return v;
+}
+
+// A map of a compiled stencil: grids of the declared types, ranks and
+// components, a domain inside every emitted view (reads are bounds-checked
+// in the kernel), and no grid that is both emitted and read off the point
+// unless red-black ordering separates the two.
 static psb_status check_compiled_map(const MapImpl &m, const psb_compiled_stencil &d) {
   if (m.ngrids != d.ngrids || m.nparams != d.nparams) return PSB_ERR_INVALID;
   for (int i = 0; i < d.ngrids; i++) {
     const GridImpl *g = m.grids[i];
-    if (type_size(d.grid_type[i]) != g->pub.elm_size || d.grid_ndims[i] != g->pub.num_dims)
-      return PSB_ERR_INVALID;
-    if (g->type >= 0 && g->type != d.grid_type[i]) return PSB_ERR_INVALID;
+    if (d.grid_ndims[i] != g->pub.num_dims) return PSB_ERR_INVALID;
+    // Grids of point types (psb_grid_new_user) carry their components.
+    if ((d.grid_type[i] == PS_USER) != !g->comps.empty()) return PSB_ERR_INVALID;
+  }
+  GridImpl *views[PSB_MAX_VIEWS];
+  if (compiled_views(m, d, views) != d.nviews) return PSB_ERR_INVALID;
+  for (int v = 0; v < d.nviews; v++) {
+    const GridImpl *g = views[v];
+    if (type_size(d.view_type[v]) != g->pub.elm_size) return PSB_ERR_INVALID;
+    if (g->type >= 0 && g->type != d.view_type[v]) return PSB_ERR_INVALID;
   }
   for (int k = 0; k < d.ndims; k++)
     if (m.dom.local_min[k] < 0 || m.dom.local_max[k] < m.dom.local_min[k]) return PSB_ERR_INVALID;
-  for (int i = 0; i < d.ngrids; i++) {
-    if (!d.emits[i]) continue;
-    const GridImpl *g = m.grids[i];
+  for (int v = 0; v < d.nviews; v++) {
+    if (!d.view_emits[v]) continue;
+    const GridImpl *g = views[v];
     for (int k = 0; k < d.ndims; k++)
       if (m.dom.local_max[k] > g->pub.dim[k]) return PSB_ERR_INVALID;
     if (m.color < 0)
-      for (int j = 0; j < d.ngrids; j++)
-        if (m.grids[j] == g && d.reads_offset[j]) return PSB_ERR_UNSUPPORTED;
+      for (int w = 0; w < d.nviews; w++)
+        if (views[w] == g && d.view_reads_offset[w]) return PSB_ERR_UNSUPPORTED;
   }
   return PSB_OK;
 }
@@ -197,6 +223,8 @@ psb_status launch_map(MapImpl &m, int color, int64_t *launches) {
       if (full) o->ghost_valid = PSB_BOUNDARY_PERIODIC;
     }
   } else if (const psb_compiled_stencil *cd = compiled_of(m.kernel_id)) {
+    GridImpl *views[PSB_MAX_VIEWS];
+    if (compiled_views(m, *cd, views) != cd->nviews) return set_status(PSB_ERR_INVALID);
     psb_launch_args a;
     memset(&a, 0, sizeof(a));
     for (int k = 0; k < 3; k++) {
@@ -204,24 +232,24 @@ psb_status launch_map(MapImpl &m, int color, int64_t *launches) {
       a.hi[k] = k < cd->ndims ? m.dom.local_max[k] : 1;
     }
     a.color = color;
-    a.ngrids = m.ngrids;
+    a.nviews = cd->nviews;
     a.nparams = m.nparams;
-    for (int i = 0; i < m.ngrids; i++) {
-      const GridView v = m.grids[i]->view();
-      a.grids[i].origin = v.origin;
-      a.grids[i].sy = v.sy;
-      a.grids[i].sz = v.sz;
-      for (int k = 0; k < 3; k++) a.grids[i].n[k] = v.n[k];
-      a.grids[i].type = cd->grid_type[i];
+    for (int v = 0; v < cd->nviews; v++) {
+      const GridView gv = views[v]->view();
+      a.views[v].origin = gv.origin;
+      a.views[v].sy = gv.sy;
+      a.views[v].sz = gv.sz;
+      for (int k = 0; k < 3; k++) a.views[v].n[k] = gv.n[k];
+      a.views[v].type = cd->view_type[v];
     }
     for (int i = 0; i < m.nparams; i++) a.params[i] = m.params[i];
     a.error = r.d_error + 1;
     a.device = r.device;
     st = cd->launch(&a, (void *)s);
     if (launches) (*launches)++;
-    for (int i = 0; i < m.ngrids; i++)
-      if (cd->emits[i] && m.grids[i]->layout == PSB_LAYOUT_PITCHED)
-        m.grids[i]->ghost_valid = PSB_BOUNDARY_NONE;
+    for (int v = 0; v < cd->nviews; v++)
+      if (cd->view_emits[v] && views[v]->layout == PSB_LAYOUT_PITCHED)
+        views[v]->ghost_valid = PSB_BOUNDARY_NONE;
   } else {
     const GenericDesc *gd = generic_of(m.kernel_id);
     if (!gd) return set_status(PSB_ERR_INVALID);
@@ -410,9 +438,13 @@ static psb_status make_map(int kernel_id, const __PSDomain *dom, __PSGrid *const
   m.kernel_id = kernel_id;
   m.dom = *dom;
   m.ngrids = ngrids;
+  // A grid of a point type (psb_grid_new_user) has no storage of its own:
+  // only compiled stencils bind it whole (other kernels take components).
+  const bool compiled = compiled_of(kernel_id) != nullptr;
   for (int i = 0; i < ngrids; i++) {
     m.grids[i] = as_impl(grids[i]);
-    if (!m.grids[i] || m.grids[i]->user_type) return set_status(PSB_ERR_INVALID);
+    if (!m.grids[i] || m.grids[i]->user_type || (!m.grids[i]->comps.empty() && !compiled))
+      return set_status(PSB_ERR_INVALID);
   }
   m.nparams = nparams;
   for (int i = 0; i < nparams; i++) m.params[i] = params[i];
@@ -624,9 +656,17 @@ psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_i
   if (d.ndims < 1 || d.ndims > 3 || d.ngrids < 1 || d.ngrids > PSB_MAX_GRIDS || d.nparams < 0 ||
       d.nparams > PSB_MAX_PARAMS)
     return set_status(PSB_ERR_INVALID);
-  for (int i = 0; i < d.ngrids; i++)
-    if (type_size(d.grid_type[i]) == 0 || d.grid_ndims[i] < 1 || d.grid_ndims[i] > 3)
+  int nv = 0;
+  for (int i = 0; i < d.ngrids; i++) {
+    const bool user = d.grid_type[i] == PS_USER;
+    if ((!user && (type_size(d.grid_type[i]) == 0 || d.grid_components[i] != 1)) ||
+        d.grid_components[i] < 1 || d.grid_ndims[i] < 1 || d.grid_ndims[i] > 3)
       return set_status(PSB_ERR_INVALID);
+    nv += d.grid_components[i];
+  }
+  if (nv != d.nviews || nv > PSB_MAX_VIEWS) return set_status(PSB_ERR_INVALID);
+  for (int v = 0; v < d.nviews; v++)
+    if (type_size(d.view_type[v]) == 0) return set_status(PSB_ERR_INVALID);
   for (int i = 0; i < d.nparams; i++)
     if (type_size(d.param_type[i]) == 0) return set_status(PSB_ERR_INVALID);
   Runtime &r = rt();
@@ -735,7 +775,8 @@ psb_status psb_last_run_stats(double *device_ms, int64_t *launches) {
 // ---------------------------------------------------------------------------
 
 static psb_status reduce_grid(GridImpl *g, int type, int op, const __PSDomain *dom, double *res) {
-  if (!g || g->user_type || op < PS_MAX || op > PS_PROD) return set_status(PSB_ERR_INVALID);
+  if (!g || g->user_type || !g->comps.empty() || op < PS_MAX || op > PS_PROD)
+    return set_status(PSB_ERR_INVALID);
   Dom3 d;
   for (int i = 0; i < 3; i++) {
     const int n = i < g->pub.num_dims ? g->pub.dim[i] : 1;
@@ -811,7 +852,8 @@ psb_status psb_reduce_map(int kernel_id, const __PSDomain *dom, __PSGrid *const 
   m.ngrids = ngrids;
   for (int i = 0; i < ngrids; i++) {
     m.grids[i] = as_impl(grids[i]);
-    if (!m.grids[i] || m.grids[i]->user_type) return set_status(PSB_ERR_INVALID);
+    if (!m.grids[i] || m.grids[i]->user_type || !m.grids[i]->comps.empty())
+      return set_status(PSB_ERR_INVALID);
   }
   m.nparams = nparams;
   for (int i = 0; i < nparams; i++) m.params[i] = params[i];

@@ -385,7 +385,7 @@ static EncodeTiledFn encode_fn() {
 }
 
 bool tma_eligible(const GridImpl *g) {
-  if (g->user_type || g->pub.num_dims != 3) return false;
+  if (g->user_type || !g->comps.empty() || g->pub.num_dims != 3) return false;
   if (g->pub.elm_size != 4 && g->pub.elm_size != 8) return false;
   if (((uintptr_t)g->alloc & 15) != 0) return false;
   if ((g->sy * g->pub.elm_size) % 16 != 0) return false;
@@ -602,7 +602,7 @@ static int64_t element_offset(GridImpl *g, va_list vl, bool *ok) {
 
 void __PSGridSet(__PSGrid *p, void *buf, ...) {
   GridImpl *g = as_impl(p);
-  if (!g || g->user_type) return;
+  if (!g || g->user_type || !g->comps.empty()) return;
   va_list vl;
   va_start(vl, buf);
   bool ok;
@@ -621,7 +621,7 @@ void __PSGridSet(__PSGrid *p, void *buf, ...) {
 
 void __PSGridGet(__PSGrid *p, void *buf, ...) {
   GridImpl *g = as_impl(p);
-  if (!g || g->user_type) return;
+  if (!g || g->user_type || !g->comps.empty()) return;
   va_list vl;
   va_start(vl, buf);
   bool ok;
@@ -827,7 +827,8 @@ psb_status psb_host_free(void *ptr) {
 
 psb_status psb_grid_copy(__PSGrid *pd, const __PSGrid *ps) {
   GridImpl *d = as_impl(pd), *s = as_impl(ps);
-  if (!d || !s || d->pub.elm_size != s->pub.elm_size || d->pub.num_dims != s->pub.num_dims)
+  if (!d || !s || d->pub.elm_size != s->pub.elm_size || d->pub.num_dims != s->pub.num_dims ||
+      !d->comps.empty() || !s->comps.empty() || d->user_type || s->user_type)
     return set_status(PSB_ERR_INVALID);
   for (int i = 0; i < d->pub.num_dims; i++)
     if (d->pub.dim[i] != s->pub.dim[i]) return set_status(PSB_ERR_INVALID);

@@ -244,7 +244,8 @@ using namespace psb;
 
 extern "C" psb_status psb_grid_fill(__PSGrid *p, int kind, uint64_t seed, double lo, double hi) {
   GridImpl *g = as_impl(p);
-  if (!g || g->user_type || kind < 0 || kind > 3) return set_status(PSB_ERR_INVALID);
+  if (!g || g->user_type || !g->comps.empty() || kind < 0 || kind > 3)
+    return set_status(PSB_ERR_INVALID);
   PSB_CHECK(ensure_init());
   Runtime &r = rt();
   GridView v = g->view();

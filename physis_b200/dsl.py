@@ -20,6 +20,14 @@ What is translated:
     expressions (normally an index parameter plus or minus a constant; a
     lower-rank grid names the index parameters of the axes it follows);
     PSGridEmit(g, v) (stores v at the current point); PSGridDim(g, d);
+  * grids of user-defined point types (`struct T {...}; DeclareGrid3D(Name,
+    struct T)`, members float/double/int/long scalars or fixed arrays):
+    PSGridGet(g, ...).member[i][j] reads one component, PSGridGet(g, ...) the
+    whole record, PSGridEmit(g, record) stores every member and
+    PSGridEmitUtype(g.member[i][j], v) one (translator/cuda_runtime_builder.cc
+    :319-1100 of the reference); on the device each component is its own
+    grid, so a stencil may update one member of a grid in place while
+    reading others around the point;
   * calls to other functions of the source (stencil functions or plain C
     helpers, emitted as device functions), and C math functions;
   * any other C statement (declarations, branches, loops), as written.
@@ -62,17 +70,21 @@ _MATH_DOUBLE = {"sqrt", "cbrt", "sin", "cos", "tan", "asin", "acos", "atan", "at
                 "cosh", "tanh", "exp", "exp2", "expm1", "log", "log2", "log10", "log1p", "pow",
                 "fabs", "floor", "ceil", "round", "trunc", "fmod", "fmin", "fmax", "hypot",
                 "erf", "erfc"}
-_INTRINSICS = {"PSGridGet", "PSGridGetPeriodic", "PSGridEmit", "PSGridDim"}
 
 
 class DSLError(ValueError):
     """The source breaks a DSL rule or cannot be translated."""
 
 
+_DECLARE = re.compile(r"\bDeclareGrid([123])D\s*\(\s*(\w+)\s*,\s*struct\s+(\w+)\s*\)\s*;?")
+
+
 def _preprocess(source):
     """Expand the source's own macros with the C preprocessor; #include lines
     are dropped first (the DSL headers only declare what this module knows,
-    and pycparser parses plain C without system headers)."""
+    and pycparser parses plain C without system headers). Grid types of
+    user-defined point types, `DeclareGrid3D(Name, struct T)`, become
+    typedefs; returns (text, {grid type name: (rank, struct name)})."""
     lines = []
     for line in source.split("\n"):
         lines.append("" if re.match(r"\s*#\s*include\b", line) else line)
@@ -80,7 +92,13 @@ def _preprocess(source):
                        capture_output=True, text=True)
     if r.returncode != 0:
         raise DSLError("the C preprocessor failed on the stencil source:\n" + r.stderr)
-    return r.stdout
+    user = {}
+
+    def declare(m):
+        user["PSGrid%sD%s" % (m.group(1), m.group(2))] = (int(m.group(1)), m.group(3))
+        return "typedef int PSGrid%sD%s;" % (m.group(1), m.group(2))
+
+    return _DECLARE.sub(declare, r.stdout), user
 
 
 def _prelude():
@@ -89,30 +107,117 @@ def _prelude():
     return "".join("typedef int %s;\n" % n for n in names)
 
 
+class _Field:
+    def __init__(self, name, ctype, dims, first):
+        self.name, self.ctype, self.dims, self.first = name, ctype, dims, first
+
+    @property
+    def count(self):
+        n = 1
+        for d in self.dims:
+            n *= d
+        return n
+
+
+class _Struct:
+    """A point type: its scalar fields (arrays flattened row-major) in order."""
+
+    def __init__(self, name, fields):
+        self.name = name
+        self.fields = fields
+        self.count = sum(f.count for f in fields)
+
+    def field(self, name):
+        for f in self.fields:
+            if f.name == name:
+                return f
+        return None
+
+
+def _struct_defs(ast):
+    """Point types defined at file scope: struct name -> _Struct (only those
+    whose members are float/double/int/long scalars or arrays of them)."""
+    out = {}
+    for n in ast.ext:
+        t = getattr(n, "type", None)
+        if isinstance(n, c_ast.Decl) and isinstance(t, c_ast.Struct) and t.decls:
+            fields, first, ok = [], 0, True
+            for d in t.decls:
+                ty, dims = d.type, []
+                while isinstance(ty, c_ast.ArrayDecl):
+                    c = _const_int(ty.dim) if ty.dim is not None else None
+                    if c is None or c <= 0:
+                        ok = False
+                        break
+                    dims.append(c)
+                    ty = ty.type
+                if not ok or not isinstance(ty, c_ast.TypeDecl) or \
+                        not isinstance(ty.type, c_ast.IdentifierType):
+                    ok = False
+                    break
+                tn = " ".join(ty.type.names)
+                if tn not in _SCALAR_TYPES and tn != "long int":
+                    ok = False
+                    break
+                f = _Field(d.name, _SCALAR_TYPES.get(tn, ps.PS_LONG), dims, first)
+                fields.append(f)
+                first += f.count
+            if ok:
+                out[t.name] = _Struct(t.name, fields)
+    return out
+
+
 class _Param:
-    def __init__(self, name, kind, ctype=None, nd=0):
-        self.name, self.kind, self.ctype, self.nd = name, kind, ctype, nd
+    def __init__(self, name, kind, ctype=None, nd=0, struct=None):
+        self.name, self.kind, self.ctype, self.nd, self.struct = name, kind, ctype, nd, struct
+
+    @property
+    def nviews(self):
+        return self.struct.count if self.struct else 1
 
 
 class StencilInfo:
     """What the front end learned about one stencil function."""
 
-    def __init__(self, name, ndims, index_names, grids, scalars):
+    def __init__(self, name, ndims, index_names, gparams, scalars):
         self.name = name
         self.ndims = ndims
         self.index_names = index_names
-        self.grids = grids          # [(name, type, nd)]
+        self.gparams = gparams      # [_Param] of the grid parameters
+        self.grids = [(p.name, p.ctype if not p.struct else ps.PS_USER, p.nd) for p in gparams]
         self.scalars = scalars      # [(name, type)]
-        self.emits = [0] * len(grids)
-        self.reads_offset = [0] * len(grids)
-        self.axes = [None] * len(grids)
+        self.base = []              # first view of each grid parameter
+        self.view_type = []
+        for p in gparams:
+            self.base.append(len(self.view_type))
+            if p.struct:
+                for f in p.struct.fields:
+                    self.view_type += [f.ctype] * f.count
+            else:
+                self.view_type.append(p.ctype)
+        self.view_emits = [0] * len(self.view_type)
+        self.view_reads_offset = [0] * len(self.view_type)
+        self.axes = [None] * len(gparams)
 
     @property
     def grid_types(self):
         return [t for _, t, _ in self.grids]
 
+    def _per_grid(self, per_view):
+        return [int(any(per_view[self.base[i]:self.base[i] + p.nviews]))
+                for i, p in enumerate(self.gparams)]
 
-def _params_of(fd):
+    @property
+    def emits(self):
+        """1 for each grid parameter that has an emitted view."""
+        return self._per_grid(self.view_emits)
+
+    @property
+    def reads_offset(self):
+        return self._per_grid(self.view_reads_offset)
+
+
+def _params_of(fd, user):
     args = fd.decl.type.args
     out = []
     if args is None:
@@ -131,6 +236,9 @@ def _params_of(fd):
         if tn in _GRID_TYPES:
             nd, typ = _GRID_TYPES[tn]
             out.append(_Param(p.name, "grid", typ, nd))
+        elif tn in user:
+            nd, st = user[tn]
+            out.append(_Param(p.name, "grid", None, nd, st))
         elif tn == "int" and "const" in p.quals:
             out.append(_Param(p.name, "index", ps.PS_INT))
         elif tn in _SCALAR_TYPES or tn == "long int":
@@ -167,13 +275,34 @@ def _index_form(node, index_names):
     return None
 
 
+def _member_chain(node):
+    """(base, field name, [subscripts]) of `base.field[a][b]`, else None."""
+    subs = []
+    while isinstance(node, c_ast.ArrayRef):
+        subs.append(node.subscript)
+        node = node.name
+    if isinstance(node, c_ast.StructRef) and node.type == "." and \
+            isinstance(node.field, c_ast.ID):
+        return node.name, node.field.name, subs[::-1]
+    return None
+
+
+def _field_var(gname, fname):
+    return "%s__%s" % (gname, fname)
+
+
+def _int(v):
+    return c_ast.Constant("int", str(v))
+
+
 class _Rewriter:
     """Rewrites the intrinsics of one function body in place."""
 
     def __init__(self, fname, params, info, functions):
         self.fname = fname
         self.index_names = [p.name for p in params if p.kind == "index"]
-        self.grids = {p.name: (i, p) for i, p in enumerate(p for p in params if p.kind == "grid")}
+        gp = [p for p in params if p.kind == "grid"]
+        self.grids = {p.name: (i, p) for i, p in enumerate(gp)}
         self.info = info
         self.functions = functions
 
@@ -188,7 +317,74 @@ class _Rewriter:
             self.fail(call, "the first argument of %s must be a grid parameter" % call.name.name)
         return self.grids[node.name]
 
+    # -- views -----------------------------------------------------------
+    def _mark(self, slot, lo, n, what):
+        if self.info is None:
+            return
+        arr = self.info.view_emits if what == "emit" else self.info.view_reads_offset
+        b = self.info.base[slot]
+        for v in range(b + lo, b + lo + n):
+            arr[v] = 1
+
+    def _component(self, node, p, fname, subs):
+        """(array variable, index expression, first component, components
+        it may be) of member `fname[subs]` of a user-type grid."""
+        f = p.struct.field(fname)
+        if f is None:
+            self.fail(node, "struct %s has no member %s" % (p.struct.name, fname))
+        if len(subs) != len(f.dims):
+            self.fail(node, "member %s of struct %s is read as an array: give all %d subscripts"
+                      % (fname, p.struct.name, len(f.dims)))
+        consts = [_const_int(e) for e in subs]
+        if all(c is not None for c in consts):
+            flat = 0
+            for c, d in zip(consts, f.dims):
+                if not 0 <= c < d:
+                    self.fail(node, "subscript of %s out of its bounds" % fname)
+                flat = flat * d + c
+            return _field_var(p.name, fname), _int(flat), f.first + flat, 1
+        expr = None
+        for e, d in zip(subs, f.dims):
+            expr = e if expr is None else c_ast.BinaryOp(
+                "+", c_ast.BinaryOp("*", expr, _int(d)), e)
+        return _field_var(p.name, fname), expr, f.first, f.count
+
+    def _indices(self, node, p, idx):
+        if len(idx) != p.nd:
+            self.fail(node, "%s of a %d-D grid takes %d indices" % (node.name.name, p.nd, p.nd))
+        # The reference's translator wants `index parameter +- constant`
+        # (for its halo analysis, docs/programming.md:161-171); here any
+        # integer expression is read (reads are bounds-checked), and a read
+        # that is not at the point itself marks the view as read off the
+        # point (no in-place update without red-black order).
+        forms = [_index_form(e, self.index_names) for e in idx]
+        at_point = len(idx) == len(self.index_names) and all(
+            f is not None and f == (k, 0) for k, f in enumerate(forms))
+        return forms, at_point
+
+    def _record_axes(self, slot, forms):
+        if self.info is not None and all(f is not None for f in forms) and \
+                self.info.axes[slot] is None:
+            self.info.axes[slot] = [f[0] for f in forms]
+
+    def _point(self):
+        return [c_ast.ID(n) for n in self.index_names] + [_int(0)] * (3 - len(self.index_names))
+
     def visit(self, node):
+        ch = _member_chain(node)
+        if ch is not None:
+            base, fname, subs = ch
+            if isinstance(base, c_ast.FuncCall) and isinstance(base.name, c_ast.ID) and \
+                    base.name.name in ("PSGridGet", "PSGridGetPeriodic"):
+                args = base.args.exprs if base.args else []
+                slot, p = self.grid_arg(base, args[0] if args else None)
+                if p.struct is not None:
+                    return self.member_get(base, slot, p, args[1:], fname, subs)
+            if isinstance(base, c_ast.ID) and base.name in self.grids:
+                self.fail(node, "a member of a grid is only written by PSGridEmitUtype")
+        if isinstance(node, c_ast.FuncCall) and isinstance(node.name, c_ast.ID) and \
+                node.name.name == "PSGridEmitUtype":
+            return self.emit_member(node)
         for name, child in list(node.children()):
             new = self.visit(child)
             if new is not child:
@@ -204,30 +400,57 @@ class _Rewriter:
             self.fail(node, "taking the address of a grid is not allowed")
         return node
 
+    def member_get(self, call, slot, p, idx, fname, subs):
+        idx = [self.visit(e) for e in idx]
+        subs = [self.visit(e) for e in subs]
+        forms, at_point = self._indices(call, p, idx)
+        self._record_axes(slot, forms)
+        var, sub, first, n = self._component(call, p, fname, subs)
+        if not at_point:
+            self._mark(slot, first, n, "read")
+        helper = "__psb_getp" if call.name.name == "PSGridGetPeriodic" else "__psb_get"
+        return c_ast.FuncCall(c_ast.ID(helper), c_ast.ExprList(
+            [c_ast.ArrayRef(c_ast.ID(var), sub)] + idx), call.coord)
+
+    def emit_member(self, node):
+        args = node.args.exprs if node.args else []
+        if len(args) != 2:
+            self.fail(node, "PSGridEmitUtype takes a grid member and a value")
+        ch = _member_chain(args[0])
+        if ch is None or not isinstance(ch[0], c_ast.ID) or ch[0].name not in self.grids or \
+                self.grids[ch[0].name][1].struct is None:
+            self.fail(node, "the first argument of PSGridEmitUtype must be a member of a grid "
+                            "of a user-defined point type")
+        slot, p = self.grids[ch[0].name]
+        if p.nd != len(self.index_names):
+            self.fail(node, "PSGridEmitUtype into a %d-D grid from a %d-D stencil" %
+                      (p.nd, len(self.index_names)))
+        subs = [self.visit(e) for e in ch[2]]
+        value = self.visit(args[1])
+        var, sub, first, n = self._component(node, p, ch[1], subs)
+        self._mark(slot, first, n, "emit")
+        return c_ast.FuncCall(c_ast.ID("__psb_emit"), c_ast.ExprList(
+            [c_ast.ArrayRef(c_ast.ID(var), sub)] + self._point() + [value]), node.coord)
+
+    def _field_args(self, p):
+        return [c_ast.ID(_field_var(p.name, f.name)) for f in p.struct.fields]
+
     def call(self, node):
         fn = node.name.name
         args = node.args.exprs if node.args else []
         if fn in ("PSGridGet", "PSGridGetPeriodic"):
             slot, p = self.grid_arg(node, args[0] if args else None)
             idx = args[1:]
-            if len(idx) != p.nd:
-                self.fail(node, "%s of a %d-D grid takes %d indices" % (fn, p.nd, p.nd))
-            # The reference's translator wants `index parameter +- constant`
-            # (for its halo analysis, docs/programming.md:161-171); here any
-            # integer expression is read (reads are bounds-checked), and a
-            # read that is not at the point itself marks the grid as read
-            # off the point (no in-place update without red-black order).
-            forms = [_index_form(e, self.index_names) for e in idx]
-            at_point = len(idx) == len(self.index_names) and all(
-                f is not None and f == (k, 0) for k, f in enumerate(forms))
-            if self.info is not None:
-                if not at_point:
-                    self.info.reads_offset[slot] = 1
-                if all(f is not None for f in forms):
-                    axes = [f[0] for f in forms]
-                    if self.info.axes[slot] is None:
-                        self.info.axes[slot] = axes
-            helper = "__psb_getp" if fn == "PSGridGetPeriodic" else "__psb_get"
+            forms, at_point = self._indices(node, p, idx)
+            self._record_axes(slot, forms)
+            if not at_point:
+                self._mark(slot, 0, p.nviews, "read")
+            per = fn == "PSGridGetPeriodic"
+            if p.struct is not None:   # the whole record
+                helper = "__psb_load%s_%s" % ("p" if per else "", p.struct.name)
+                return c_ast.FuncCall(c_ast.ID(helper), c_ast.ExprList(
+                    self._field_args(p) + idx), node.coord)
+            helper = "__psb_getp" if per else "__psb_get"
             return c_ast.FuncCall(c_ast.ID(helper), c_ast.ExprList([c_ast.ID(p.name)] + idx),
                                   node.coord)
         if fn == "PSGridEmit":
@@ -237,19 +460,34 @@ class _Rewriter:
             if p.nd != len(self.index_names):
                 self.fail(node, "PSGridEmit into a %d-D grid from a %d-D stencil" %
                           (p.nd, len(self.index_names)))
-            if self.info is not None:
-                self.info.emits[slot] = 1
-            pos = [c_ast.ID(n) for n in self.index_names]
-            return c_ast.FuncCall(c_ast.ID("__psb_emit"),
-                                  c_ast.ExprList([c_ast.ID(p.name)] + pos + [args[1]]), node.coord)
+            self._mark(slot, 0, p.nviews, "emit")
+            if p.struct is not None:
+                return c_ast.FuncCall(c_ast.ID("__psb_store_" + p.struct.name), c_ast.ExprList(
+                    self._field_args(p) + self._point() + [args[1]]), node.coord)
+            return c_ast.FuncCall(c_ast.ID("__psb_emit"), c_ast.ExprList(
+                [c_ast.ID(p.name)] + self._point() + [args[1]]), node.coord)
         if fn == "PSGridDim":
             if len(args) != 2:
                 self.fail(node, "PSGridDim takes a grid and a dimension")
-            self.grid_arg(node, args[0])
-            return c_ast.FuncCall(c_ast.ID("__psb_dim"), c_ast.ExprList(list(args)), node.coord)
+            slot, p = self.grid_arg(node, args[0])
+            g = c_ast.ID(p.name) if p.struct is None else c_ast.ArrayRef(
+                c_ast.ID(_field_var(p.name, p.struct.fields[0].name)), _int(0))
+            return c_ast.FuncCall(c_ast.ID("__psb_dim"), c_ast.ExprList([g, args[1]]), node.coord)
         if fn.startswith("PS"):
             self.fail(node, "%s is not available inside a stencil function" % fn)
-        if fn in _MATH_DOUBLE and fn not in self.functions:
+        if fn in self.functions:
+            # A grid of a point type is passed on as its field arrays.
+            out = []
+            for a in args:
+                if isinstance(a, c_ast.ID) and a.name in self.grids and \
+                        self.grids[a.name][1].struct is not None:
+                    out += self._field_args(self.grids[a.name][1])
+                else:
+                    out.append(a)
+            if node.args:
+                node.args.exprs = out
+            return node
+        if fn in _MATH_DOUBLE:
             dargs = [c_ast.Cast(c_ast.Typename(None, [], None, c_ast.TypeDecl(
                 None, [], None, c_ast.IdentifierType(["double"]))), a) for a in args]
             return c_ast.FuncCall(c_ast.ID(fn), c_ast.ExprList(dargs), node.coord)
@@ -300,14 +538,7 @@ __device__ __forceinline__ T __psb_getp(const __psb_grid<T> &g, int i, int j = 0
   return g.p[__psb_wrap(i, g.n0) + __psb_wrap(j, g.n1) * g.sy + __psb_wrap(k, g.n2) * g.sz];
 }
 
-template <typename T, typename V>
-__device__ __forceinline__ void __psb_emit(const __psb_grid<T> &g, int i, V v) {
-  g.p[i] = (T)v;
-}
-template <typename T, typename V>
-__device__ __forceinline__ void __psb_emit(const __psb_grid<T> &g, int i, int j, V v) {
-  g.p[i + j * g.sy] = (T)v;
-}
+// Stores at the current point (unused index parameters are 0).
 template <typename T, typename V>
 __device__ __forceinline__ void __psb_emit(const __psb_grid<T> &g, int i, int j, int k, V v) {
   g.p[i + j * g.sy + k * g.sz] = (T)v;
@@ -320,11 +551,46 @@ __device__ __forceinline__ int __psb_dim(const __psb_grid<T> &g, int d) {
 """
 
 
+def _struct_helpers(st):
+    """Whole-record load (plain and periodic) and store of a point type."""
+    params = ", ".join("const __psb_grid<%s> *f_%s" % (_CTYPE[f.ctype], f.name)
+                       for f in st.fields)
+    out = []
+    for per in (False, True):
+        body = []
+        for f in st.fields:
+            for flat in range(f.count):
+                sub, r = "", flat
+                for d in reversed(f.dims):
+                    sub = "[%d]" % (r % d) + sub
+                    r //= d
+                body.append("  v.%s%s = %s(f_%s[%d], i, j, k);" % (
+                    f.name, sub, "__psb_getp" if per else "__psb_get", f.name, flat))
+        out.append("__device__ __forceinline__ struct %s __psb_load%s_%s(%s, int i, int j = 0, "
+                   "int k = 0) {\n  struct %s v;\n%s\n  return v;\n}" % (
+                       st.name, "p" if per else "", st.name, params, st.name, "\n".join(body)))
+    body = []
+    for f in st.fields:
+        for flat in range(f.count):
+            sub, r = "", flat
+            for d in reversed(f.dims):
+                sub = "[%d]" % (r % d) + sub
+                r //= d
+            body.append("  __psb_emit(f_%s[%d], i, j, k, v.%s%s);" % (f.name, flat, f.name, sub))
+    out.append("__device__ __forceinline__ void __psb_store_%s(%s, int i, int j, int k, "
+               "const struct %s &v) {\n%s\n}" % (st.name, params, st.name, "\n".join(body)))
+    return "\n\n".join(out)
+
+
 def _signature(fname, params):
     out = []
     for p in params:
         if p.kind == "index":
             out.append("const int %s" % p.name)
+        elif p.kind == "grid" and p.struct is not None:
+            for f in p.struct.fields:
+                out.append("const __psb_grid<%s> *%s" % (_CTYPE[f.ctype],
+                                                          _field_var(p.name, f.name)))
         elif p.kind == "grid":
             out.append("const __psb_grid<%s> %s" % (_CTYPE[p.ctype], p.name))
         elif p.kind == "scalar":
@@ -342,11 +608,11 @@ class _Calls(c_ast.NodeVisitor):
         self.generic_visit(node)
 
 
-def _reachable(funcs):
+def _reachable(funcs, user):
     """The stencil functions and the functions they call (directly or not),
     in source order; the rest of the program (main, I/O) is host code."""
     by_name = {f.decl.name: f for f in funcs}
-    todo = [f.decl.name for f in funcs if _is_stencil(_params_of(f))]
+    todo = [f.decl.name for f in funcs if _is_stencil(_params_of(f, user))]
     keep = set()
     while todo:
         n = todo.pop()
@@ -363,25 +629,43 @@ def translate(source):
     """Translate every stencil function of `source`.
 
     Returns (cuda_source, {name: StencilInfo}). Runs on the CPU only."""
-    text = _prelude() + _preprocess(source)
+    text, user_decl = _preprocess(source)
     try:
-        ast = c_parser.CParser().parse(text, filename="<dsl>")
+        ast = c_parser.CParser().parse(_prelude() + text, filename="<dsl>")
     except Exception as e:  # pycparser raises ParseError with a location
         raise DSLError("cannot parse the stencil source: %s" % e) from None
     gen = c_generator.CGenerator()
+    structs = _struct_defs(ast)
+    user = {}
+    for tname, (nd, sname) in user_decl.items():
+        if sname not in structs:
+            raise DSLError("%s: struct %s is not defined with float/double/int/long members "
+                           "of fixed size" % (tname, sname))
+        user[tname] = (nd, structs[sname])
     funcs = [n for n in ast.ext if isinstance(n, c_ast.FuncDef)]
     names = {f.decl.name for f in funcs}
-    funcs = _reachable(funcs)
+    funcs = _reachable(funcs, user)
     infos = {}
     parts = [_HELPERS]
-    # Declarations first, so functions may call each other in any order.
+    # Point types and their record helpers, then declarations first, so
+    # functions may call each other in any order.
+    used = []
+    for nd, st in user.values():
+        if st not in used:
+            used.append(st)
+    for n in ast.ext:
+        if isinstance(n, c_ast.Decl) and isinstance(getattr(n, "type", None), c_ast.Struct) \
+                and n.type.decls:
+            parts.append(gen.visit(n) + ";")
+    for st in used:
+        parts.append(_struct_helpers(st))
     decls = []
     bodies = []
     for fd in funcs:
         fname = fd.decl.name
         if fname == "main":
             continue
-        params = _params_of(fd)
+        params = _params_of(fd, user)
         if _is_stencil(params):
             ret = fd.decl.type.type
             if not (isinstance(ret, c_ast.TypeDecl) and ret.type.names == ["void"]):
@@ -395,15 +679,16 @@ def translate(source):
             if any(k == "other" for k in kinds):
                 raise DSLError("%s: parameters must be grids or float/double/int/long scalars" %
                                fname)
-            grids = [(p.name, p.ctype, p.nd) for p in params if p.kind == "grid"]
+            gparams = [p for p in params if p.kind == "grid"]
             scalars = [(p.name, p.ctype) for p in params if p.kind == "scalar"]
-            if len(grids) > ps.PSB_MAX_GRIDS or len(scalars) > ps.PSB_MAX_PARAMS:
-                raise DSLError("%s: too many grid or scalar parameters" % fname)
-            info = StencilInfo(fname, nidx, [p.name for p in params[:nidx]], grids, scalars)
+            info = StencilInfo(fname, nidx, [p.name for p in params[:nidx]], gparams, scalars)
+            if len(gparams) > ps.PSB_MAX_GRIDS or len(scalars) > ps.PSB_MAX_PARAMS or \
+                    len(info.view_type) > ps.PSB_MAX_VIEWS:
+                raise DSLError("%s: too many grid, component or scalar parameters" % fname)
             _Rewriter(fname, params, info, names).visit(fd.body)
-            for slot, (gname, _, nd) in enumerate(grids):
-                if info.emits[slot] and info.axes[slot] is None:
-                    info.axes[slot] = list(range(nd))
+            for slot, p in enumerate(gparams):
+                if info.axes[slot] is None:
+                    info.axes[slot] = list(range(p.nd))
             infos[fname] = info
             sig = _signature(fname, params)
         else:
@@ -425,17 +710,28 @@ def _entry(info):
     n = info.name
     binds = []
     args = ["x", "y", "z"][:info.ndims]
-    for slot, (gname, t, nd) in enumerate(info.grids):
-        binds.append("  const __psb_grid<%s> g%d = __psb_bind<%s>(A.grids[%d], A.error);" %
-                     (_CTYPE[t], slot, _CTYPE[t], slot))
-        args.append("g%d" % slot)
+    for slot, p in enumerate(info.gparams):
+        b = info.base[slot]
+        if p.struct is None:
+            t = _CTYPE[p.ctype]
+            binds.append("  const __psb_grid<%s> g%d = __psb_bind<%s>(A.views[%d], A.error);" %
+                         (t, slot, t, b))
+            args.append("g%d" % slot)
+            continue
+        for f in p.struct.fields:
+            t = _CTYPE[f.ctype]
+            items = ", ".join("__psb_bind<%s>(A.views[%d], A.error)" % (t, b + f.first + k)
+                              for k in range(f.count))
+            binds.append("  const __psb_grid<%s> g%d__%s[%d] = {%s};" % (t, slot, f.name, f.count,
+                                                                          items))
+            args.append("g%d__%s" % (slot, f.name))
     for k, (sname, t) in enumerate(info.scalars):
         args.append("(%s)A.params[%d]" % (_CTYPE[t], k))
-    gt = ", ".join(str(t) for t in info.grid_types)
-    gn = ", ".join(str(nd) for _, _, nd in info.grids)
-    em = ", ".join(str(e) for e in info.emits)
-    ro = ", ".join(str(r) for r in info.reads_offset)
-    pt = ", ".join(str(t) for _, t in info.scalars) or "0"
+
+    def arr(vals):
+        return ", ".join(str(v) for v in vals) or "0"
+
+    comps = [p.nviews for p in info.gparams]
     return """
 extern "C" __global__ void __launch_bounds__(256) __psb_kernel_{n}(const psb_launch_args A) {{
   // One thread per (x, y) point of the domain, a loop over z.
@@ -462,21 +758,30 @@ extern "C" psb_status psb_dsl_launch_{n}(const psb_launch_args *a, void *stream)
 }}
 
 extern "C" void psb_dsl_describe_{n}(psb_compiled_stencil *d) {{
-  const int gt[] = {{{gt}}}, gn[] = {{{gn}}}, em[] = {{{em}}}, ro[] = {{{ro}}}, pt[] = {{{pt}}};
+  const int gt[] = {{{gt}}}, gn[] = {{{gn}}}, gc[] = {{{gc}}};
+  const int vt[] = {{{vt}}}, ve[] = {{{ve}}}, vr[] = {{{vr}}}, pt[] = {{{pt}}};
   d->ndims = {nd};
   d->ngrids = {ng};
   for (int i = 0; i < {ng}; i++) {{
     d->grid_type[i] = gt[i];
     d->grid_ndims[i] = gn[i];
-    d->emits[i] = em[i];
-    d->reads_offset[i] = ro[i];
+    d->grid_components[i] = gc[i];
+  }}
+  d->nviews = {nv};
+  for (int v = 0; v < {nv}; v++) {{
+    d->view_type[v] = vt[v];
+    d->view_emits[v] = ve[v];
+    d->view_reads_offset[v] = vr[v];
   }}
   d->nparams = {np};
   for (int i = 0; i < {np}; i++) d->param_type[i] = pt[i];
   d->launch = psb_dsl_launch_{n};
 }}
-""".format(n=n, binds="\n".join(binds), args=", ".join(args), gt=gt, gn=gn, em=em, ro=ro, pt=pt,
-           nd=info.ndims, ng=len(info.grids), np=len(info.scalars))
+""".format(n=n, binds="\n".join(binds), args=", ".join(args), gt=arr(info.grid_types),
+           gn=arr(nd for _, _, nd in info.grids), gc=arr(comps), vt=arr(info.view_type),
+           ve=arr(info.view_emits), vr=arr(info.view_reads_offset),
+           pt=arr(t for _, t in info.scalars), nd=info.ndims, ng=len(info.grids),
+           nv=len(info.view_type), np=len(info.scalars))
 
 
 def build_library(cuda_source, cache_dir=None):

@@ -142,6 +142,160 @@ void lopsided(const int x, const int y, const int z, PSGrid3DFloat p, PSGrid3DFl
 """
 
 
+_BRANCHES = """
+/* Reads under data-independent conditions (x at the faces, x parity). */
+void branches(const int x, const int y, const int z, PSGrid3DFloat in, PSGrid3DFloat out) {
+  const float mid = PSGridGet(in, x, y, z);
+  float acc = 0.0f;
+  if (x > 0) acc = PSGridGet(in, x - 1, y, z);
+  acc += x > 0 ? PSGridGet(in, x - 1, y, z) : PSGridGet(in, x, y, z);
+  acc += x > 0 ? PSGridGet(in, x - 1, y, z) : mid;
+  if (x > 0 && x < PSGridDim(in, 0) - 1)
+    acc += PSGridGet(in, x - 1, y, z) + PSGridGet(in, x + 1, y, z);
+  else
+    acc += PSGridGet(in, x, y, z);
+  if ((x & 1) == 0) acc += PSGridGet(in, x, y, z);
+  PSGridEmit(out, mid + acc);
+}
+"""
+
+
+# Point-type cases: (DSL source, [(function, grid slots)] applied in order each
+# iteration, iterations, numpy record dtype, initial values per component as
+# `i + offset` (None: 0), grids, dumped grid, dumped components (field, flat
+# index)). The domain is the interior [1, N-1) in every case.
+_VEC3 = """
+struct Vec3 { float a; float b; float c; };
+DeclareGrid3D(Vec3, struct Vec3);
+
+void smooth3(const int x, const int y, const int z, PSGrid3DVec3 src, PSGrid3DVec3 dst) {
+  float sa = (PSGridGet(src, x, y, z).a + PSGridGet(src, x + 1, y, z).a
+              + PSGridGet(src, x - 1, y, z).a) / 3.3f;
+  float sb = (PSGridGet(src, x, y, z).b + PSGridGet(src, x, y + 1, z).b
+              + PSGridGet(src, x, y - 1, z).b + PSGridGet(src, x, y, z + 1).b
+              + PSGridGet(src, x, y, z - 1).b) / 5.5f;
+  float sc = (PSGridGet(src, x, y, z).c + PSGridGet(src, x, y, z + 1).c
+              + PSGridGet(src, x, y, z - 1).c) / 3.3f;
+  struct Vec3 out = {sa, sb, sc};
+  PSGridEmit(dst, out);
+}
+"""
+
+_TRIPLE = """
+struct Triple { float u; float v; float w; };
+DeclareGrid3D(Triple, struct Triple);
+
+void gather_w(const int x, const int y, const int z, PSGrid3DTriple t) {
+  float s = PSGridGet(t, x, y, z).u + PSGridGet(t, x + 1, y, z).u
+      + PSGridGet(t, x - 1, y, z).u + PSGridGet(t, x, y + 1, z).u
+      + PSGridGet(t, x, y - 1, z).u + PSGridGet(t, x, y, z + 1).u
+      + PSGridGet(t, x, y, z - 1).u + PSGridGet(t, x, y, z).v
+      + PSGridGet(t, x + 1, y, z).v + PSGridGet(t, x - 1, y, z).v
+      + PSGridGet(t, x, y + 1, z).v + PSGridGet(t, x, y - 1, z).v
+      + PSGridGet(t, x, y, z + 1).v + PSGridGet(t, x, y, z - 1).v;
+  PSGridEmitUtype(t.w, s / 14.3);
+}
+
+void relax_uv(const int x, const int y, const int z, PSGrid3DTriple t) {
+  PSGridEmitUtype(t.u, (PSGridGet(t, x, y, z).u + PSGridGet(t, x, y, z).w) * 0.5);
+  PSGridEmitUtype(t.v, (PSGridGet(t, x, y, z).v + PSGridGet(t, x, y, z).w) * 0.5);
+}
+"""
+
+_PAIR = """
+struct Pair { float h[2]; };
+DeclareGrid3D(Pair, struct Pair);
+
+void spread(const int x, const int y, const int z, PSGrid3DPair g) {
+  float s = PSGridGet(g, x, y, z).h[0] + PSGridGet(g, x - 1, y, z).h[0]
+      + PSGridGet(g, x + 1, y, z).h[0] + PSGridGet(g, x, y - 1, z).h[0]
+      + PSGridGet(g, x, y + 1, z).h[0] + PSGridGet(g, x, y, z - 1).h[0]
+      + PSGridGet(g, x, y, z + 1).h[0];
+  PSGridEmitUtype(g.h[1], s);
+}
+"""
+
+_MULTI = """
+struct Cell { float s[2]; float m; float out; };
+DeclareGrid3D(Cell, struct Cell);
+
+#define STAR(G, F) (PSGridGet(G, x, y, z).F + PSGridGet(G, x - 1, y, z).F \\
+    + PSGridGet(G, x + 1, y, z).F + PSGridGet(G, x, y - 1, z).F \\
+    + PSGridGet(G, x, y + 1, z).F + PSGridGet(G, x, y, z - 1).F \\
+    + PSGridGet(G, x, y, z + 1).F)
+
+void three_sums(const int x, const int y, const int z, PSGrid3DCell g) {
+  float first = STAR(g, s[0]);
+  float second = STAR(g, s[1]);
+  float third = STAR(g, m);
+  PSGridEmitUtype(g.out, first + second + third);
+}
+"""
+
+_MATRIX = """
+struct Mat { float e[3][2]; };
+DeclareGrid3D(Mat, struct Mat);
+
+static float star_of(float c, float w, float e, float n, float s, float b, float t) {
+  return c + w + e + n + s + b + t;
+}
+
+void corners(const int x, const int y, const int z, PSGrid3DMat g) {
+  float lo = star_of(PSGridGet(g, x, y, z).e[0][0], PSGridGet(g, x - 1, y, z).e[0][0],
+                     PSGridGet(g, x + 1, y, z).e[0][0], PSGridGet(g, x, y - 1, z).e[0][0],
+                     PSGridGet(g, x, y + 1, z).e[0][0], PSGridGet(g, x, y, z - 1).e[0][0],
+                     PSGridGet(g, x, y, z + 1).e[0][0]);
+  float hi = star_of(PSGridGet(g, x, y, z).e[2][1], PSGridGet(g, x - 1, y, z).e[2][1],
+                     PSGridGet(g, x + 1, y, z).e[2][1], PSGridGet(g, x, y - 1, z).e[2][1],
+                     PSGridGet(g, x, y + 1, z).e[2][1], PSGridGet(g, x, y, z - 1).e[2][1],
+                     PSGridGet(g, x, y, z + 1).e[2][1]);
+  PSGridEmitUtype(g.e[1][0], lo + hi);
+}
+"""
+
+
+def user_cases():
+    """name -> dict(src, steps, iters, dtype, init, grids, dump, comps)."""
+    import numpy as np
+    f4 = np.float32
+    return {
+        "user-defined-type1": dict(
+            src=_VEC3, steps=[("smooth3", [0, 1]), ("smooth3", [1, 0])], iters=5,
+            dtype=np.dtype([("a", f4), ("b", f4), ("c", f4)]),
+            init=[("a", 0, 0), ("b", 0, 1), ("c", 0, 2)], grids=2, dump=0,
+            comps=[("a", 0), ("b", 0), ("c", 0)]),
+        "user-defined-type3": dict(
+            src=_TRIPLE, steps=[("gather_w", [0]), ("relax_uv", [0])], iters=10,
+            dtype=np.dtype([("u", f4), ("v", f4), ("w", f4)]),
+            init=[("u", 0, 0), ("v", 0, 1), ("w", 0, None)], grids=1, dump=0,
+            comps=[("u", 0), ("v", 0), ("w", 0)]),
+        "user-defined-type5": dict(
+            src=_PAIR, steps=[("spread", [0])], iters=1,
+            dtype=np.dtype([("h", f4, (2,))]), init=[("h", 0, 0), ("h", 1, None)], grids=1,
+            dump=0, comps=[("h", 1)]),
+        "user-defined-type-multi-members": dict(
+            src=_MULTI, steps=[("three_sums", [0])], iters=1,
+            dtype=np.dtype([("s", f4, (2,)), ("m", f4), ("out", f4)]),
+            init=[("s", 0, 0), ("s", 1, 1), ("m", 0, 2), ("out", 0, None)], grids=1, dump=0,
+            comps=[("out", 0)]),
+        "user-defined-type-multi-dim-member": dict(
+            src=_MATRIX, steps=[("corners", [0])], iters=1,
+            dtype=np.dtype([("e", f4, (3, 2))]),
+            init=[("e", j * 2 + k, j + k) for j in range(3) for k in range(2)], grids=1, dump=0,
+            comps=[("e", 2)]),
+    }
+
+
+def extra_cases():
+    """Known-answer cases that only the front end runs (not flat sums, so no
+    generic descriptor): name -> case dict in the form of cases.py."""
+    n = C.N
+    return {
+        "15": dict(grids=[(C.PS_FLOAT, (n, n, n))] * 2, init=["ramp", "ramp"],
+                   dom=([0, 0, 0], [n, n, n]), run=[([0, 1], -1)], iters=1, dump=1, fmt="%f"),
+    }
+
+
 def _order27():
     out = []
     for dz in (-1, 0, 1):
@@ -183,5 +337,6 @@ def dsl_cases():
         "mixed-dim3": (_MIXED3, "weighted_planes", []),
         "redblack": (_inplace_stencil("rb7", _O7, False), "rb7", []),
         "redblack-periodic": (_inplace_stencil("rb7p", _O7, True), "rb7p", []),
+        "15": (_BRANCHES, "branches", []),
     }
     return out

@@ -20,7 +20,9 @@ ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
 NAMES = ["7-pt", "7-pt-multi-iterations", "7-pt-neumann-cond", "7-pt-periodic",
          "7-pt-double-type", "7-pt-type-mix", "7-pt-int-type", "27-pt", "27-pt-periodic",
          "asymmetric", "asymmetric-periodic", "stencil-hole", "16", "3-pt-1d", "3-pt-periodic",
-         "9-pt-2d", "mixed-dim", "mixed-dim2", "mixed-dim3", "redblack", "redblack-periodic"]
+         "9-pt-2d", "mixed-dim", "mixed-dim2", "mixed-dim3", "redblack", "redblack-periodic",
+         "15", "user-defined-type1", "user-defined-type3", "user-defined-type5",
+         "user-defined-type-multi-members", "user-defined-type-multi-dim-member"]
 
 
 def main():

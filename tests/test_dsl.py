@@ -85,15 +85,17 @@ def test_generated_library_builds_for_sm100a(tmp_path):
         getattr(lib, "psb_dsl_describe_" + name)(ctypes.byref(d))
         assert d.ndims == info.ndims and d.ngrids == len(info.grids)
         assert list(d.grid_type)[:d.ngrids] == info.grid_types
-        assert list(d.emits)[:d.ngrids] == info.emits
-        assert list(d.reads_offset)[:d.ngrids] == info.reads_offset
+        assert d.nviews == len(info.view_type)
+        assert list(d.view_type)[:d.nviews] == info.view_type
+        assert list(d.view_emits)[:d.nviews] == info.view_emits
+        assert list(d.view_reads_offset)[:d.nviews] == info.view_reads_offset
         assert d.nparams == len(info.scalars) and d.launch
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_TESTS), reason="reference sources not present")
 def test_reference_system_tests_translate():
     """Every stencil function of the reference's system tests translates,
-    except the user-defined point types (struct grids, a separate API here)."""
+    the user-defined point types included."""
     done = 0
     for f in sorted(glob.glob(os.path.join(REF_TESTS, "test_*.c"))):
         if ".manual." in f:
@@ -101,11 +103,7 @@ def test_reference_system_tests_translate():
         text = open(f).read()
         if "PSGridEmit" not in text:
             continue
-        if "DeclareGrid" in text:
-            with pytest.raises(dsl.DSLError):
-                dsl.translate(text)
-            continue
         _, infos = dsl.translate(text)
         assert infos, f
         done += 1
-    assert done >= 25
+    assert done >= 33

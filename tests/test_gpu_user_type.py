@@ -107,3 +107,34 @@ def test_invalid_types_are_refused():
         ps.grid_new_user((4, 4, 4), [(ps.PS_DOUBLE, 1, 4)], 16)  # misaligned double
     with pytest.raises(ps.PhysisError):
         ps.grid_new_user((4, 4, 4), [(ps.PS_FLOAT, 5, 0)], 16)   # field past the record
+
+
+def test_whole_point_grid_is_refused_where_it_has_no_storage():
+    """A point-type grid keeps its data in its components: calls that would
+    touch the grid's own storage (fill, reduce, built-in or generic maps,
+    grid copy) refuse it up front, before any device work."""
+    dims = (8, 8, 8)
+    g, h = _point_grid(dims), _point_grid(dims)
+    f = ps.grid_new(ps.PS_FLOAT, dims)
+    try:
+        codes = []
+        codes.append(ps.lib.psb_grid_fill(g.ptr, ps.FILL_CONST, 0, 1.0, 1.0))
+        codes.append(ps.lib.psb_grid_copy(g.ptr, h.ptr))
+        dom = ps.PSDomain3DNew(1, 7, 1, 7, 1, 7)
+        for k, gs in ((ps.DIFFUSION7, [g, f]), (ps.DIFFUSION7, [f, g])):
+            with pytest.raises(ps.PhysisError) as e:
+                ps.PSStencilMap(k, dom, *gs, *([0.1] * 7))
+            codes.append(e.value.status)
+        st = ps.GenericStencil(3, [(ps.PS_FLOAT, (0, 1, 2))] * 2, 1, ps.PS_FLOAT,
+                               [ps.get(0, (0, 0, 0))])
+        with pytest.raises(ps.PhysisError) as e:
+            ps.PSStencilMap(st.kernel_id, dom, g, f)
+        codes.append(e.value.status)
+        with pytest.raises(ps.PhysisError) as e:
+            ps.PSReduce(ps.PS_SUM, g)
+        codes.append(e.value.status)
+        assert codes == [ps.PSB_ERR_INVALID] * len(codes)
+        ps.sync()
+    finally:
+        for x in (g, h, f):
+            ps.PSGridFree(x)

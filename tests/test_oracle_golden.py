@@ -24,6 +24,7 @@ def test_golden_manifest_digests():
     import os
     with open(os.path.join(C.HERE, "manifest.json")) as f:
         man = json.load(f)
-    assert set(man) == set(CASES)
+    from tests.golden import dsl_cases
+    assert set(man) == set(CASES) | set(dsl_cases.extra_cases()) | set(dsl_cases.user_cases())
     for name, rec in man.items():
         assert hashlib.sha256(C.golden_text(name).encode()).hexdigest() == rec["sha256"]
