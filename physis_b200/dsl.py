@@ -692,6 +692,9 @@ def translate(source):
             infos[fname] = info
             sig = _signature(fname, params)
         else:
+            if any(p.kind == "grid" for p in params):
+                raise DSLError("%s: a function that takes grids is a stencil function and "
+                               "begins with its `const int` index parameters" % fname)
             _Rewriter(fname, params, None, names).visit(fd.body)
             sig = "__device__ " + gen.visit(fd.decl).rstrip(";")
         decls.append(sig + ";")
@@ -784,12 +787,21 @@ extern "C" void psb_dsl_describe_{n}(psb_compiled_stencil *d) {{
            nv=len(info.view_type), np=len(info.scalars))
 
 
+_NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
+               "-fmad=false", "-Xcompiler", "-fPIC", "-shared"]
+
+
 def build_library(cuda_source, cache_dir=None):
-    """Compile generated source for sm_100a into a shared library (cached by
-    the hash of the source); returns its path."""
+    """Compile generated source for sm_100a into a shared library; returns
+    its path. Libraries are cached by a hash of the source, the ABI header
+    they are compiled against (the launch arguments' layout) and the flags."""
     cache_dir = cache_dir or DEFAULT_CACHE
     os.makedirs(cache_dir, exist_ok=True)
-    key = hashlib.sha256(cuda_source.encode()).hexdigest()[:20]
+    h = hashlib.sha256(cuda_source.encode())
+    with open(os.path.join(INCLUDE, "physis_b200.h"), "rb") as f:
+        h.update(f.read())
+    h.update(" ".join(_NVCC_FLAGS).encode())
+    key = h.hexdigest()[:20]
     so = os.path.join(cache_dir, "libpsb_dsl_%s.so" % key)
     if os.path.exists(so):
         return so
@@ -797,8 +809,7 @@ def build_library(cuda_source, cache_dir=None):
     with open(cu, "w") as f:
         f.write(cuda_source)
     tmp = so + ".tmp%d" % os.getpid()
-    cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-           "-fmad=false", "-Xcompiler", "-fPIC", "-shared", "-I" + INCLUDE, cu, "-o", tmp]
+    cmd = [NVCC] + _NVCC_FLAGS + ["-I" + INCLUDE, cu, "-o", tmp]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise DSLError("nvcc failed on the generated kernel:\n" + r.stdout + r.stderr)

@@ -63,6 +63,15 @@ def test_generated_code_keeps_c_semantics():
      "PSGridEmit into a 1-D grid"),
     ("void f(const int x, PSGrid1DFloat a, PSGrid1DFloat b) { PSGridEmit(b, PSGridGet(a, x, x)); }",
      "takes 1 indices"),
+    ("float h(PSGrid1DFloat a, int i) { return 0; }\n"
+     "void f(const int x, PSGrid1DFloat a, PSGrid1DFloat b) { PSGridEmit(b, h(a, x)); }",
+     "begins with its `const int` index"),
+    ("struct P { float u; };\nDeclareGrid1D(P, struct P);\n"
+     "void f(const int x, PSGrid1DP a) { PSGridEmitUtype(a.v, 1.0f); }", "has no member v"),
+    ("struct P { float u[2]; };\nDeclareGrid1D(P, struct P);\n"
+     "void f(const int x, PSGrid1DP a) { PSGridEmitUtype(a.u, 1.0f); }", "give all 1 subscripts"),
+    ("struct P { float u; };\nDeclareGrid1D(P, struct P);\n"
+     "void f(const int x, PSGrid1DP a) { float v = a.u; }", "only written by PSGridEmitUtype"),
     ("void f(const int x, PSGrid1DFloat a) { void *p = &a; }", "address of a grid"),
     ("void f(const int x, PSGrid1DFloat a) { PSGridCopyin(a, 0); }", "not available"),
     ("int f(const int x, PSGrid1DFloat a) { return 0; }", "return void"),
@@ -107,3 +116,16 @@ def test_reference_system_tests_translate():
         assert infos, f
         done += 1
     assert done >= 33
+
+
+def test_point_type_views():
+    """A grid of a point type is one view per scalar component (fields in
+    order, arrays row-major); reads and emits are tracked per component."""
+    _, infos = dsl.translate(D.user_cases()["user-defined-type-multi-dim-member"]["src"])
+    k = infos["corners"]
+    assert k.grid_types == [ps.PS_USER] and k.view_type == [ps.PS_FLOAT] * 6
+    assert k.view_emits == [0, 0, 1, 0, 0, 0]           # e[1][0]
+    assert k.view_reads_offset == [1, 0, 0, 0, 0, 1]    # e[0][0] and e[2][1]
+    _, infos = dsl.translate(D.user_cases()["user-defined-type1"]["src"])
+    k = infos["smooth3"]
+    assert k.view_emits == [0, 0, 0, 1, 1, 1] and k.view_reads_offset == [1, 1, 1, 0, 0, 0]
