@@ -109,7 +109,8 @@ struct BMember {
   TmaGeom dg;
   HimenoGeom hg;
   double *partials;  // [2][ntiles][kBWarps][2]
-  unsigned *done;    // (ntiles * kBWarps + 1) units per step
+  unsigned *step_cnt;   // [steps] warps done in the local step, +1 once it is released
+  unsigned *tile_done;  // [ntiles] warps done on the tile, over all steps
   int *stop;         // local steps completed when converged, or -1
   double *res;       // [0] a or gosa, [1] b, [2] gosa of the first check, [3] check count
 };
@@ -157,8 +158,25 @@ __device__ __forceinline__ int ld_acquire_int(const int *p) {
   return v;
 }
 
-__device__ __forceinline__ unsigned step_unit(const BMember &M) {
-  return (unsigned)M.ntiles * kBWarps + 1u;
+// Members with at least this many tiles per step wait for the tiles around
+// an item of the previous step; smaller ones for the whole previous step.
+constexpr int kWaveTiles = 128;
+
+// Warp completions of one step of a member (the last one also releases it).
+__device__ __forceinline__ unsigned step_full(const BMember &M) {
+  return (unsigned)M.ntiles * kBWarps;
+}
+
+// Whether global step gstep measures the residual (and may stop the member).
+template <int GROUP>
+__device__ __forceinline__ bool is_check_step(const BMember &M, int gstep) {
+  return M.check_every > 0 && ((gstep + 1) % M.check_every == 0 || (GROUP == 1 && gstep == 0));
+}
+
+__device__ __forceinline__ unsigned ld_relaxed(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
 }
 
 // Output column and planes of item (m, s, t).
@@ -214,18 +232,79 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, const 
       m = __ldg(B.order + k);
       t = (int)(local - __ldg(B.tile_prefix + k));
       M = &B.members[m];
-      // Every tile of step s-1 of this member, and its convergence decision.
-      const unsigned need = (unsigned)s * step_unit(*M);
-      if (ld_acquire(M->done) < need) {
+      // Dependencies on step s-1 of the member. After a step that measures
+      // the residual: all of it and its convergence decision. Otherwise the
+      // tiles this item's planes read (its own and the 26 around it,
+      // wrapping for periodic members, whose edge tiles also write the
+      // opposite halo), which are also every tile that read the planes it
+      // overwrites: consecutive steps of one member overlap like a
+      // wavefront instead of meeting at a barrier. Every dependency is an
+      // item earlier in the list, so the earliest unfinished item can always
+      // run.
+      if (s > 0) {
+        const unsigned full = step_full(*M);
+        const bool after_check = is_check_step<GROUP>(*M, M->step0 + s - 1);
+        const unsigned *cnt = M->step_cnt + (s - 1);
         const long long t0 = clock64();
         unsigned sleep = 32;
-        while (ld_acquire(M->done) < need) {
-          if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) {
-            ok = false;
-            break;
+        if (after_check) {
+          while (ld_acquire(cnt) < full + 1u) {
+            if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) {
+              ok = false;
+              break;
+            }
+            __nanosleep(sleep);
+            if (sleep < 2048) sleep <<= 1;
           }
-          __nanosleep(sleep);
-          if (sleep < 2048) sleep <<= 1;
+        } else if (M->ntiles < kWaveTiles) {
+          // Small members: their steps are short and end almost together;
+          // waiting for the whole step costs one counter.
+          while (ld_acquire(cnt) < full) {
+            if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) {
+              ok = false;
+              break;
+            }
+            __nanosleep(sleep);
+            if (sleep < 2048) sleep <<= 1;
+          }
+        } else if (ld_acquire(cnt) < full) {
+          const int tx = M->tiles_x, ty = M->tiles_y, tz = M->nzc;
+          const int cx = t % tx, cy = (t / tx) % ty, cz = t / (tx * ty);
+          const bool wrap = GROUP == 0 && M->kind == BK_DIFF7P;
+          const unsigned need = (unsigned)s * kBWarps;
+          // The 27 counters are read together (independent loads in flight
+          // at once), then only the ones not yet reached are polled.
+          const unsigned *nb[27];
+#pragma unroll
+          for (int k = 0; k < 27; k++) {
+            int x = cx + k % 3 - 1, y = cy + (k / 3) % 3 - 1, z = cz + k / 9 - 1;
+            bool in = true;
+            if (x < 0 || x >= tx) { in = wrap; x = (x + tx) % tx; }
+            if (y < 0 || y >= ty) { in = in && wrap; y = (y + ty) % ty; }
+            if (z < 0 || z >= tz) { in = in && wrap; z = (z + tz) % tz; }
+            nb[k] = in ? M->tile_done + (x + tx * (y + ty * z)) : nullptr;
+          }
+          unsigned v[27];
+#pragma unroll
+          for (int k = 0; k < 27; k++) v[k] = nb[k] ? ld_relaxed(nb[k]) : need;
+          unsigned pending = 0;
+#pragma unroll
+          for (int k = 0; k < 27; k++)
+            if (v[k] < need) pending |= 1u << k;
+          while (pending) {
+            if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) {
+              ok = false;
+              break;
+            }
+            __nanosleep(sleep);
+            if (sleep < 2048) sleep <<= 1;
+            if (ld_relaxed(cnt) >= full) break;  // the whole step is done
+#pragma unroll
+            for (int k = 0; k < 27; k++)
+              if ((pending >> k & 1u) && ld_relaxed(nb[k]) >= need) pending &= ~(1u << k);
+          }
+          // Acquire what the relaxed reads observed.
+          asm volatile("fence.acq_rel.gpu;" ::: "memory");
         }
       }
       if (!ok) {
@@ -288,10 +367,11 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, const 
 }
 
 // Completion of an item by one consumer warp: its FP64 residual partial
-// (when the step is checked), then one unit of the member's step counter.
-// The warp that completes the step's last unit combines the partials in
-// index order (deterministic: the same whatever else is in the batch),
-// decides convergence, and only then releases the member's next step.
+// (when the step is checked), then one unit of the tile's and of the step's
+// counter. The warp that completes the step's last unit combines the
+// partials in index order (deterministic: the same whatever else is in the
+// batch), decides convergence, and only then releases the step (the next
+// step of a checked one waits for that).
 template <int GROUP>
 __device__ __forceinline__ void item_done(const BMember &M, int s, int t, int warp, int lane,
                                           bool check, bool contrib, double a, double b) {
@@ -312,8 +392,9 @@ __device__ __forceinline__ void item_done(const BMember &M, int s, int t, int wa
   unsigned last = 0;
   if (lane == 0) {
     __threadfence();
-    const unsigned old = atomicAdd(M.done, 1u);
-    last = old + 1 == (unsigned)s * step_unit(M) + (unsigned)M.ntiles * kBWarps;
+    atomicAdd(M.tile_done + t, 1u);
+    const unsigned old = atomicAdd(M.step_cnt + s, 1u);
+    last = old + 1 == step_full(M);
   }
   last = __shfl_sync(0xffffffffu, last, 0);
   if (!last) return;
@@ -347,7 +428,7 @@ __device__ __forceinline__ void item_done(const BMember &M, int s, int t, int wa
   }
   if (lane == 0) {
     __threadfence();
-    atomicAdd(M.done, 1u);
+    atomicAdd(M.step_cnt + s, 1u);
   }
 }
 
@@ -376,9 +457,7 @@ __device__ void batch_consume(const BatchDev &B, const Ring &R, const Ring &RC, 
     const int par = (M.step0 + ds) & 1;
     __syncwarp();
     if (lane == 0) mbar_arrive(&qempty[q]);
-    const int gstep = M.step0 + ds;
-    const bool check = M.check_every > 0 &&
-                       ((gstep + 1) % M.check_every == 0 || (GROUP == 1 && gstep == 0));
+    const bool check = is_check_step<GROUP>(M, M.step0 + ds);
     double a = 0, b = 0;
     if (!skip) {
       const ItemGeom g = item_geom<GROUP>(M, dt);
@@ -481,7 +560,8 @@ struct psb_batch {
   BMember *d_members = nullptr;
   CUtensorMap *d_tmaps = nullptr;
   double *d_partials = nullptr;
-  unsigned *d_done = nullptr;
+  unsigned *d_done = nullptr;  // per member: step counters, then tile counters
+  int64_t n_counters = 1;
   int *d_stop = nullptr;
   double *d_res = nullptr;
   size_t cap_members = 0, cap_tmaps = 0, cap_partials = 0, cap_done = 0, cap_stop = 0,
@@ -738,14 +818,17 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
                      cudaMemcpyHostToDevice));
   PSB_CHECK(dev_reserve(&b->d_partials, &b->cap_partials,
                         sizeof(double) * std::max<int64_t>(1, partial_slots)));
-  PSB_CHECK(dev_reserve(&b->d_done, &b->cap_done, sizeof(unsigned) * std::max(1, n)));
+  int64_t counters = 0;
+  for (int i = 0; i < n; i++) counters += std::max(0, steps[i]) + b->members[i].ntiles;
+  b->n_counters = std::max<int64_t>(1, counters);
+  PSB_CHECK(dev_reserve(&b->d_done, &b->cap_done, sizeof(unsigned) * b->n_counters));
   PSB_CHECK(dev_reserve(&b->d_stop, &b->cap_stop, sizeof(int) * std::max(1, n)));
   PSB_CHECK(dev_reserve(&b->d_res, &b->cap_res, sizeof(double) * 4 * std::max(1, n)));
   if ((int)b->res_init.size() == 4 * n && n > 0)
     PSB_TRY(cudaMemcpy(b->d_res, b->res_init.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice));
   else
     PSB_TRY(cudaMemset(b->d_res, 0, sizeof(double) * 4 * std::max(1, n)));
-  int64_t off = 0;
+  int64_t off = 0, coff = 0;
   for (int i = 0; i < n; i++) {
     BMember &M = b->members[i];
     M.tmap[0] = b->d_tmaps + 2 * i;
@@ -753,7 +836,10 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     M.tcoef = coef_map[i] >= 0 ? b->d_tmaps + coef_map[i] : nullptr;
     M.partials = b->d_partials + off;
     off += 2 * 2 * kBWarps * (int64_t)M.ntiles;
-    M.done = b->d_done + i;
+    M.step_cnt = b->d_done + coff;
+    coff += std::max(0, steps[i]);
+    M.tile_done = b->d_done + coff;
+    coff += M.ntiles;
     M.stop = b->d_stop + i;
     M.res = b->d_res + 4 * i;
   }
@@ -827,7 +913,7 @@ psb_status batch_read_state(psb_batch *b, std::vector<int> &stop, std::vector<do
 
 psb_status batch_reset_counters(psb_batch *b, cudaStream_t s) {
   const int n = (int)b->hm.size();
-  PSB_TRY(cudaMemsetAsync(b->d_done, 0, sizeof(unsigned) * std::max(1, n), s));
+  PSB_TRY(cudaMemsetAsync(b->d_done, 0, sizeof(unsigned) * b->n_counters, s));
   PSB_TRY(cudaMemsetAsync(b->d_stop, 0xff, sizeof(int) * std::max(1, n), s));
   for (auto &g : b->grp) PSB_TRY(cudaMemsetAsync(g.d_cursor, 0, sizeof(unsigned long long), s));
   return PSB_OK;

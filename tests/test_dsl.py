@@ -10,7 +10,10 @@ import physis_b200 as ps
 from physis_b200 import dsl
 from tests.golden import dsl_cases as D
 
-REF_TESTS = "/root/reference/tests/system_tests/test_cases"
+# The reference's system tests, where the reference tree is present (this
+# CPU test is skipped elsewhere).
+REF_TESTS = os.path.join(os.environ.get("PHYSIS_REFERENCE", "/root/reference"),
+                         "tests", "system_tests", "test_cases")
 
 
 def _all_case_source():
