@@ -10,10 +10,12 @@
 //
 // Mode 0 (persistent): one launch per kind with one CTA per resident slot.
 // In each CTA a producer thread takes items from the list with an atomic
-// cursor, waits until the item's member has completed the previous step (a
-// per-member counter, acquire load, bounded wait), passes the item to the
-// consumer warps through a small descriptor queue in shared memory and
-// streams its input planes by TMA into a ring of stages. The ring is not
+// cursor, waits for the item's dependencies in the member's previous step
+// (the whole step after a residual check or for a small member; otherwise
+// the 27 tiles around the item, so a large member's steps overlap like a
+// wavefront; acquire loads, bounded waits), passes the item to the consumer
+// warps through a small descriptor queue in shared memory and streams its
+// input planes by TMA into a ring of stages. The ring is not
 // drained between items: the producer runs ahead into the next item's planes
 // while the consumers finish the current one, and consumer warps never meet
 // at a CTA-wide barrier, so a CTA moves from item to item without a bubble.
