@@ -504,6 +504,16 @@ typedef struct {
 
 psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_id);
 
+/* Register stencil function `name` of a kernel library made by the front end
+ * (which exports psb_dsl_describe_<name>); *status_out gets the status. */
+#define PSB_DSL_REGISTER(name, kernel_id_ptr, status_out)            \
+  do {                                                                \
+    extern void psb_dsl_describe_##name(psb_compiled_stencil *);     \
+    psb_compiled_stencil psb_d__;                                     \
+    psb_dsl_describe_##name(&psb_d__);                                \
+    *(status_out) = psb_compiled_register(&psb_d__, (kernel_id_ptr)); \
+  } while (0)
+
 /* Non-varargs map and run. grids: ngrids grid pointers in the kernel's
  * order; params: nparams scalars (converted to the kernel's type). */
 psb_status psb_stencil_map(int kernel_id, const __PSDomain *dom, __PSGrid *const *grids,

@@ -1,22 +1,20 @@
 /* The user program of user_diffusion.c with its stencil written in the DSL
- * (dsl_kernels.c) and compiled by the front end: the kernel library's
- * describe function fills a psb_compiled_stencil, psb_compiled_register gives
- * the id PSStencilMap takes. Usage: dsl_diffusion nx ny nz count in out */
+ * (dsl_kernels.c) and compiled by the front end: PSB_DSL_REGISTER fills a
+ * psb_compiled_stencil from the kernel library and registers it, giving the
+ * id PSStencilMap takes. Usage: dsl_diffusion nx ny nz count in out */
 #include <stdio.h>
 #include <stdlib.h>
 
 #include "physis_b200.h"
 
-void psb_dsl_describe_diffuse(psb_compiled_stencil *d);
-
 int main(int argc, char *argv[]) {
   PSInit(&argc, &argv, 3, 0, 0, 0);
   if (argc < 7) return 2;
   int nx = atoi(argv[1]), ny = atoi(argv[2]), nz = atoi(argv[3]), count = atoi(argv[4]);
-  psb_compiled_stencil desc;
   int diffuse = 0;
-  psb_dsl_describe_diffuse(&desc);
-  if (psb_compiled_register(&desc, &diffuse) != PSB_OK) return 4;
+  psb_status st;
+  PSB_DSL_REGISTER(diffuse, &diffuse, &st);
+  if (st != PSB_OK) return 4;
   size_t n = (size_t)nx * ny * nz;
   float *buf = (float *)malloc(n * sizeof(float));
   FILE *f = fopen(argv[5], "rb");

@@ -38,7 +38,7 @@ def declared_functions():
         text = open(os.path.join(ROOT, "include", hdr)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         text = _strip_inline_bodies(text)
-        text = re.sub(r"#[^\n]*(\\\n[^\n]*)*", "", text)
+        text = re.sub(r"#(?:\\\n|[^\n])*", "", text)  # directives, with continuations
         for m in re.finditer(r"([A-Za-z_][A-Za-z_0-9]*)\s*\(([^;{}]*)\)\s*;", text):
             name = m.group(1)
             pre = text[max(0, m.start() - 200):m.start()]
