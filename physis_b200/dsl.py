@@ -409,8 +409,12 @@ class _Rewriter:
         if not at_point:
             self._mark(slot, first, n, "read")
         helper = "__psb_getp" if call.name.name == "PSGridGetPeriodic" else "__psb_get"
-        return c_ast.FuncCall(c_ast.ID(helper), c_ast.ExprList(
-            [c_ast.ArrayRef(c_ast.ID(var), sub)] + idx), call.coord)
+        if n == 1:
+            return c_ast.FuncCall(c_ast.ID(helper), c_ast.ExprList(
+                [c_ast.ArrayRef(c_ast.ID(var), sub)] + idx), call.coord)
+        # A subscript computed at run time is checked against the member.
+        return c_ast.FuncCall(c_ast.ID(helper + "_c"), c_ast.ExprList(
+            [c_ast.ID(var), _int(n), sub] + idx), call.coord)
 
     def emit_member(self, node):
         args = node.args.exprs if node.args else []
@@ -429,8 +433,11 @@ class _Rewriter:
         value = self.visit(args[1])
         var, sub, first, n = self._component(node, p, ch[1], subs)
         self._mark(slot, first, n, "emit")
-        return c_ast.FuncCall(c_ast.ID("__psb_emit"), c_ast.ExprList(
-            [c_ast.ArrayRef(c_ast.ID(var), sub)] + self._point() + [value]), node.coord)
+        if n == 1:
+            return c_ast.FuncCall(c_ast.ID("__psb_emit"), c_ast.ExprList(
+                [c_ast.ArrayRef(c_ast.ID(var), sub)] + self._point() + [value]), node.coord)
+        return c_ast.FuncCall(c_ast.ID("__psb_emit_c"), c_ast.ExprList(
+            [c_ast.ID(var), _int(n), sub] + self._point() + [value]), node.coord)
 
     def _field_args(self, p):
         return [c_ast.ID(_field_var(p.name, f.name)) for f in p.struct.fields]
@@ -542,6 +549,36 @@ __device__ __forceinline__ T __psb_getp(const __psb_grid<T> &g, int i, int j = 0
 template <typename T, typename V>
 __device__ __forceinline__ void __psb_emit(const __psb_grid<T> &g, int i, int j, int k, V v) {
   g.p[i + j * g.sy + k * g.sz] = (T)v;
+}
+
+// Members of point types indexed at run time: a subscript outside the member
+// reads 0 / stores nothing and sets PSB_ERR_BOUNDS.
+template <typename T>
+__device__ __forceinline__ T __psb_get_c(const __psb_grid<T> *f, int n, int c, int i, int j = 0,
+                                         int k = 0) {
+  if ((unsigned)c >= (unsigned)n) {
+    atomicExch(f[0].err, (int)PSB_ERR_BOUNDS);
+    return T(0);
+  }
+  return __psb_get(f[c], i, j, k);
+}
+template <typename T>
+__device__ __forceinline__ T __psb_getp_c(const __psb_grid<T> *f, int n, int c, int i, int j = 0,
+                                          int k = 0) {
+  if ((unsigned)c >= (unsigned)n) {
+    atomicExch(f[0].err, (int)PSB_ERR_BOUNDS);
+    return T(0);
+  }
+  return __psb_getp(f[c], i, j, k);
+}
+template <typename T, typename V>
+__device__ __forceinline__ void __psb_emit_c(const __psb_grid<T> *f, int n, int c, int i, int j,
+                                             int k, V v) {
+  if ((unsigned)c >= (unsigned)n) {
+    atomicExch(f[0].err, (int)PSB_ERR_BOUNDS);
+    return;
+  }
+  __psb_emit(f[c], i, j, k, v);
 }
 
 template <typename T>

@@ -132,3 +132,24 @@ def test_point_type_views():
     _, infos = dsl.translate(D.user_cases()["user-defined-type1"]["src"])
     k = infos["smooth3"]
     assert k.view_emits == [0, 0, 0, 1, 1, 1] and k.view_reads_offset == [1, 1, 1, 0, 0, 0]
+
+
+def test_run_time_member_subscripts_are_checked():
+    """A member subscript computed at run time (a loop over a matrix member)
+    goes through the checked helpers: outside the member it reads 0 or
+    stores nothing and reports PSB_ERR_BOUNDS instead of indexing past the
+    member's component list."""
+    src = """
+    struct M { float p[3][3]; };
+    DeclareGrid3D(M, struct M);
+    void transpose(const int x, const int y, const int z, PSGrid3DM a, PSGrid3DM b) {
+      int i, j;
+      for (i = 0; i < 3; i++)
+        for (j = 0; j < 3; j++)
+          PSGridEmitUtype(b.p[j][i], PSGridGet(a, x, y, z).p[i][j]);
+    }
+    """
+    cu, infos = dsl.translate(src)
+    assert "__psb_emit_c(b__p, 9, (j * 3) + i" in cu and "__psb_get_c(a__p, 9, (i * 3) + j" in cu
+    k = infos["transpose"]
+    assert k.view_emits == [0] * 9 + [1] * 9 and k.view_reads_offset == [0] * 18

@@ -160,3 +160,35 @@ def test_compiled_matches_builtin_diffusion_in_graph_loop(kernels, tmp_path):
     assert np.array_equal(out, ref)
     for x in g:
         ps.PSGridFree(x)
+
+
+@pytest.mark.gpu
+def test_point_type_transpose_with_loop_subscripts(tmp_path):
+    """Members indexed by loop variables: b.p[j][i] = a(x, y, z).p[i][j]."""
+    from physis_b200 import dsl
+    k = dsl.compile_stencils("""
+    struct M { float p[3][3]; };
+    DeclareGrid3D(M, struct M);
+    void transpose(const int x, const int y, const int z, PSGrid3DM a, PSGrid3DM b) {
+      int i, j;
+      for (i = 0; i < 3; i++)
+        for (j = 0; j < 3; j++)
+          PSGridEmitUtype(b.p[j][i], PSGridGet(a, x, y, z).p[i][j]);
+    }""", str(tmp_path))["transpose"]
+    dims = (12, 10, 8)
+    dt = np.dtype([("p", np.float32, (3, 3))])
+    recs = np.zeros(dims[::-1], dt)
+    recs["p"] = np.random.default_rng(5).random(dims[::-1] + (3, 3), dtype=np.float32)
+    a = ps.grid_new_user(dims, [(ps.PS_FLOAT, 9, 0)], dt.itemsize)
+    b = ps.grid_new_user(dims, [(ps.PS_FLOAT, 9, 0)], dt.itemsize)
+    try:
+        ps.user_copyin(a, recs)
+        dom = ps.PSDomain3DNew(0, dims[0], 0, dims[1], 0, dims[2])
+        ps.PSStencilRun(ps.PSStencilMap(k.kernel_id, dom, a, b), 1)
+        ps.sync()
+        out = np.zeros_like(recs)
+        ps.user_copyout(b, out)
+    finally:
+        ps.PSGridFree(a)
+        ps.PSGridFree(b)
+    assert np.array_equal(out["p"], np.swapaxes(recs["p"], -1, -2))
