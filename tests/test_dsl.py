@@ -153,3 +153,20 @@ def test_run_time_member_subscripts_are_checked():
     assert "__psb_emit_c(b__p, 9, (j * 3) + i" in cu and "__psb_get_c(a__p, 9, (i * 3) + j" in cu
     k = infos["transpose"]
     assert k.view_emits == [0] * 9 + [1] * 9 and k.view_reads_offset == [0] * 18
+
+
+def test_command_line_translation(tmp_path):
+    """`python -m physis_b200.dsl src -o out.cu` writes the generated CUDA
+    (translation only, no nvcc) and lists the stencil functions found."""
+    import subprocess
+    import sys
+    src = tmp_path / "k.c"
+    src.write_text(D.dsl_cases()["7-pt"][0])
+    out = tmp_path / "k.cu"
+    r = subprocess.run([sys.executable, "-m", "physis_b200.dsl", str(src), "-o", str(out)],
+                       capture_output=True, text=True,
+                       cwd=os.path.abspath(os.path.join(os.path.dirname(__file__), "..")))
+    assert r.returncode == 0, r.stderr
+    assert "sum7: 3-D" in r.stdout
+    text = out.read_text()
+    assert "__global__" in text and "psb_dsl_describe_sum7" in text
