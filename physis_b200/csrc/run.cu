@@ -434,6 +434,8 @@ static psb_status make_map(int kernel_id, const __PSDomain *dom, __PSGrid *const
   if (!dom || !out || ngrids < 1 || ngrids > PSB_MAX_GRIDS || nparams < 0 ||
       nparams > PSB_MAX_PARAMS)
     return set_status(PSB_ERR_INVALID);
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
   MapImpl m;
   m.kernel_id = kernel_id;
   m.dom = *dom;
@@ -451,8 +453,6 @@ static psb_status make_map(int kernel_id, const __PSDomain *dom, __PSGrid *const
   m.color = color;
   m.live = true;
   PSB_CHECK(check_map(m));
-  Runtime &r = rt();
-  std::lock_guard<std::recursive_mutex> lk(r.mu);
   // The same closure bound again (a map call inside the user's time loop)
   // returns the existing handle instead of growing the table.
   for (int i = 0; i < (int)r.maps.size(); i++) {
@@ -504,10 +504,12 @@ static int kernel_ngrids(int kernel_id, int *nparams) {
 }
 
 static PSStencil vmap(void *kernel, int color, va_list vl) {
+  std::unique_lock<std::recursive_mutex> lk(rt().mu);
   int kid = (int)(intptr_t)kernel;
   int np = 0;
   int ng = kernel_ngrids(kid, &np);
   if (ng < 0) {
+    lk.unlock();
     fprintf(stderr, "physis_b200: PSStencilMap: unknown kernel %d\n", kid);
     exit(EXIT_FAILURE);
   }
@@ -529,6 +531,7 @@ static PSStencil vmap(void *kernel, int color, va_list vl) {
   }
   PSStencil h = 0;
   psb_status s = make_map(kid, &dom, grids, ng, params, np, color, &h);
+  lk.unlock();
   if (s != PSB_OK) {
     fprintf(stderr, "physis_b200: PSStencilMap failed: %s\n", psb_status_string(s));
     exit(EXIT_FAILURE);
@@ -593,6 +596,7 @@ void __PSStencilRunN(int nargs, ...) {
   va_start(vl, nargs);
   PSStencil hs[PSB_B200_MAX_RUN_MAPS];
   int nm = 0, iter = 1;
+  std::unique_lock<std::recursive_mutex> lk(rt().mu);
   for (int i = 0; i < nargs; i++) {
     int v = va_arg(vl, int);
     if (map_of(v) && nm < PSB_B200_MAX_RUN_MAPS) {
@@ -600,12 +604,14 @@ void __PSStencilRunN(int nargs, ...) {
     } else if (i == nargs - 1) {
       iter = v;
     } else {
+      lk.unlock();
       fprintf(stderr, "physis_b200: PSStencilRun: argument %d is not a stencil map\n", i);
       exit(EXIT_FAILURE);
     }
   }
   va_end(vl);
   psb_status s = psb_stencil_run(hs, nm, iter);
+  lk.unlock();
   if (s != PSB_OK) {
     fprintf(stderr, "physis_b200: PSStencilRun failed: %s\n", psb_status_string(s));
     exit(EXIT_FAILURE);
@@ -680,6 +686,7 @@ psb_status psb_stencil_map_rb(int kernel_id, const __PSDomain *dom, __PSGrid *co
                               int ngrids, const double *params, int nparams, int color,
                               PSStencil *out) {
   if (color < 0 || color > 2) return set_status(PSB_ERR_INVALID);
+  std::lock_guard<std::recursive_mutex> lk(rt().mu);
   if (!generic_of(kernel_id) && !compiled_of(kernel_id)) return set_status(PSB_ERR_UNSUPPORTED);
   return make_map(kernel_id, dom, grids, ngrids, params, nparams, color, out);
 }
@@ -687,19 +694,21 @@ psb_status psb_stencil_map_rb(int kernel_id, const __PSDomain *dom, __PSGrid *co
 psb_status psb_stencil_run(const PSStencil *maps, int nmaps, int iter) {
   PSB_CHECK(ensure_init());
   if (nmaps < 1 || nmaps > PSB_B200_MAX_RUN_MAPS || !maps) return set_status(PSB_ERR_INVALID);
+  // Map and kernel tables grow under the runtime lock; entries are only
+  // looked up and used while holding it.
+  std::lock_guard<std::recursive_mutex> lk(rt().mu);
   MapImpl *ms[PSB_B200_MAX_RUN_MAPS];
   for (int i = 0; i < nmaps; i++) {
     ms[i] = map_of(maps[i]);
     if (!ms[i]) return set_status(PSB_ERR_INVALID);
   }
-  std::lock_guard<std::recursive_mutex> lk(rt().mu);
   return run_maps(ms, nmaps, iter);
 }
 
 psb_status psb_stencil_free(PSStencil s) {
+  std::lock_guard<std::recursive_mutex> lk(rt().mu);
   MapImpl *m = map_of(s);
   if (!m) return set_status(PSB_ERR_INVALID);
-  std::lock_guard<std::recursive_mutex> lk(rt().mu);
   cudaStreamSynchronize(rt().stream);
   drop_graphs();
   if (m->d_partials) cudaFree(m->d_partials);
@@ -725,10 +734,10 @@ psb_status psb_set_graph(int enable) {
 }
 
 psb_status psb_himeno_residual_enable(PSStencil h, int history_len) {
+  std::lock_guard<std::recursive_mutex> lk(rt().mu);
   MapImpl *m = map_of(h);
   if (!m || m->kernel_id != PSB_KERNEL_HIMENO19 || history_len < 0)
     return set_status(PSB_ERR_INVALID);
-  std::lock_guard<std::recursive_mutex> lk(rt().mu);
   drop_graphs();
   if (history_len == 0) {
     m->residual_len = 0;
@@ -748,12 +757,14 @@ psb_status psb_himeno_residual_enable(PSStencil h, int history_len) {
 }
 
 psb_status psb_himeno_residual(PSStencil h, double *gosa) {
+  std::lock_guard<std::recursive_mutex> lk(rt().mu);
   MapImpl *m = map_of(h);
   if (!m || !gosa) return set_status(PSB_ERR_INVALID);
   return fetch_history(*m, gosa, 1);
 }
 
 psb_status psb_himeno_residual_history(PSStencil h, double *out, int n) {
+  std::lock_guard<std::recursive_mutex> lk(rt().mu);
   MapImpl *m = map_of(h);
   if (!m || !out || n < 1 || n > m->residual_len) return set_status(PSB_ERR_INVALID);
   return fetch_history(*m, out, n);
@@ -843,6 +854,8 @@ psb_status psb_reduce_map(int kernel_id, const __PSDomain *dom, __PSGrid *const 
   if (!dom || !grids || !result || op < PS_MAX || op > PS_PROD || ngrids < 1 ||
       ngrids > PSB_MAX_GRIDS || nparams < 0 || nparams > PSB_MAX_PARAMS)
     return set_status(PSB_ERR_INVALID);
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
   const GenericDesc *gd = generic_of(kernel_id);
   if (!gd) return set_status(kernel_id < PSB_KERNEL_FIRST_GENERIC ? PSB_ERR_UNSUPPORTED
                                                                   : PSB_ERR_INVALID);
@@ -858,8 +871,6 @@ psb_status psb_reduce_map(int kernel_id, const __PSDomain *dom, __PSGrid *const 
   m.nparams = nparams;
   for (int i = 0; i < nparams; i++) m.params[i] = params[i];
   PSB_CHECK(check_map(m, false));
-  Runtime &r = rt();
-  std::lock_guard<std::recursive_mutex> lk(r.mu);
   legacy_join_in();
   PSB_CHECK(generic_reduce(m, *gd, op, result, r.stream));
   legacy_join_out();
