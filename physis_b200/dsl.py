@@ -46,6 +46,7 @@ import hashlib
 import os
 import re
 import subprocess
+import threading
 
 from pycparser import c_ast, c_generator, c_parser
 
@@ -842,10 +843,13 @@ def build_library(cuda_source, cache_dir=None):
     so = os.path.join(cache_dir, "libpsb_dsl_%s.so" % key)
     if os.path.exists(so):
         return so
-    cu = os.path.join(cache_dir, "psb_dsl_%s.cu" % key)
+    # Unique names per build: the same source may be built by several
+    # threads or processes at once; the finished library is renamed in place.
+    tag = "%d.%d" % (os.getpid(), threading.get_ident())
+    cu = os.path.join(cache_dir, "psb_dsl_%s.%s.cu" % (key, tag))
     with open(cu, "w") as f:
         f.write(cuda_source)
-    tmp = so + ".tmp%d" % os.getpid()
+    tmp = so + ".tmp" + tag
     cmd = [NVCC] + _NVCC_FLAGS + ["-I" + INCLUDE, cu, "-o", tmp]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

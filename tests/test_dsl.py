@@ -121,6 +121,23 @@ def test_reference_system_tests_translate():
     assert done >= 33
 
 
+@pytest.mark.skipif(not os.path.isdir(REF_TESTS), reason="reference sources not present")
+def test_reference_system_tests_compile_for_sm100a(tmp_path):
+    """The translation of every reference system test with a stencil builds
+    with nvcc for sm_100a (host cross-compile, no GPU)."""
+    import concurrent.futures
+    files = [f for f in sorted(glob.glob(os.path.join(REF_TESTS, "test_*.c")))
+             if ".manual." not in f and "PSGridEmit" in open(f).read()]
+
+    def build(f):
+        cu, _ = dsl.translate(open(f).read())
+        return dsl.build_library(cu, str(tmp_path))
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=8) as ex:
+        libs = list(ex.map(build, files))
+    assert len(libs) == len(files) >= 33 and all(os.path.exists(p) for p in libs)
+
+
 def test_point_type_views():
     """A grid of a point type is one view per scalar component (fields in
     order, arrays row-major); reads and emits are tracked per component."""
