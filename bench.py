@@ -92,7 +92,7 @@ def c2_field(dims, dtype, seed=2024):
 
 
 def himeno_fields(dims, seed=77):
-    from tests.gpu_util import himeno_inputs
+    from physis_b200.workloads import himeno_inputs
     nx, ny, nz = dims
     return himeno_inputs((nz, ny, nx), seed)
 

@@ -568,9 +568,13 @@ psb_status psb_reduce_map(int kernel_id, const __PSDomain *dom, __PSGrid *const 
  *   data    device pointer to element (0,0,0) of the array
  *   type    PS_FLOAT, PS_DOUBLE, PS_INT or PS_LONG; op a PSReduceOp
  *   extent  nx, ny, nz, each in [1, PSB_NOALLOC_MAX_EXTENT] (else PSB_ERR_INVALID)
- *   stride  elements between rows (>= nx) and between planes (>= stride[0]*ny)
- *   stream  a cudaStream_t, or NULL for the legacy default stream
- *   result  host pointer; the call returns once it is written (FP64 value)
+ *   stride  elements between rows (>= nx) and between planes (>= stride[0]*ny),
+ *           with stride[1] * nz <= INT64_MAX / 8 (else PSB_ERR_INVALID)
+ *   stream  a cudaStream_t, or NULL for the legacy default stream; the data
+ *           is read in that stream's order, so order it after whatever last
+ *           wrote `data` (the runtime works on its own non-blocking stream:
+ *           call psb_sync() first when `data` is a runtime grid)
+ *   result  host pointer; the call blocks until it is written (FP64 value)
  * The first call on each device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current: make it before any stream
  * capture. All calls share the array and it keeps the last call's contents;

@@ -37,7 +37,9 @@ __global__ void __launch_bounds__(256) k_reduce(GridView g, Dom3 d, int op, Redu
     const int y = d.lo[1] + (int)(r % ry);
     const int z = d.lo[2] + (int)(r / ry);
     const T *row = base + (int64_t)y * g.sy + (int64_t)z * g.sz + d.lo[0];
-    for (int x = lane; x < rx; x += 32) racc_add(op, a, (double)row[x]);
+    // 64-bit column index: a row may be up to 2^31-1 elements long, and a
+    // 32-bit x + 32 would overflow past it.
+    for (int64_t x = lane; x < rx; x += 32) racc_add(op, a, (double)row[x]);
   }
   RAcc b = racc_block(op, a, scratch);
   if (threadIdx.x == 0) {
@@ -119,8 +121,14 @@ psb_status reduce_view(const GridView &v, int type, int op, const Dom3 &dom, dou
 //    overlap on the GPU (other streams, other host threads) race on it.
 //  * The launch never uses more CTAs than the array has partial slots, so
 //    the array does not bound the input; extents are bounded by the
-//    kernel's 32-bit indices (PSB_NOALLOC_MAX_EXTENT per dimension) and
-//    larger ones are rejected.
+//    kernel's 32-bit coordinates (PSB_NOALLOC_MAX_EXTENT per dimension; the
+//    column index within a row is 64-bit, so a row of that length does not
+//    overflow it) and larger ones are rejected, as are strides whose last
+//    element would lie beyond INT64_MAX / 8 elements.
+//  * The call blocks: it returns once the result is in host memory. It
+//    reads `data` in stream order on `stream`, so the caller orders that
+//    stream after whatever last wrote `data` (the runtime's own work runs
+//    on a non-blocking stream: psb_sync() before a NULL-stream call).
 // ===========================================================================
 }  // namespace psb
 
@@ -170,8 +178,17 @@ extern "C" psb_status psb_reduce_noalloc(const void *data, int type, int op,
       return set_status(PSB_ERR_INVALID);
     }
   }
-  if (stride[0] < extent[0] || stride[1] < stride[0] * extent[1]) {
+  // Rows and planes must not overlap: stride[0] >= nx and stride[1] >=
+  // stride[0] * ny, the latter tested as stride[1] / ny >= stride[0] (the
+  // same for positive integers) so that no product can overflow. The last
+  // element's offset is below nz * stride[1]; bounding that by INT64_MAX / 8
+  // keeps every element offset and byte offset representable.
+  if (stride[0] < extent[0] || stride[1] / extent[1] < stride[0]) {
     fprintf(stderr, "psb_reduce_noalloc: strides must not overlap rows or planes\n");
+    return set_status(PSB_ERR_INVALID);
+  }
+  if (stride[1] > (INT64_MAX / 8) / extent[2]) {
+    fprintf(stderr, "psb_reduce_noalloc: stride[1] * extent[2] exceeds the addressable range\n");
     return set_status(PSB_ERR_INVALID);
   }
   void *scratch = nullptr;
