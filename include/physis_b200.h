@@ -632,6 +632,18 @@ psb_status psb_batch_set_stop(psb_batch *b, int member, double tol, int check_ev
  * (0 or 1). */
 psb_status psb_batch_member_result(psb_batch *b, int member, int *steps_done, double *residual,
                                    int *result_grid);
+/* How the last mode-0/1 run cut a member into work items (no counterpart in
+ * the reference, which has no batching): the points of an item in x and y,
+ * its planes in z, the items of one step, and whether consecutive steps of
+ * the member overlapped as a wavefront (1: an item waited only for the 27
+ * items around it in the previous step; 0: for the whole previous step).
+ * PSB_ERR_INVALID before the batch has run in mode 0 or 1. */
+typedef struct {
+  int tile_x, tile_y, z_chunk;
+  int tiles;
+  int wavefront;
+} psb_batch_layout;
+psb_status psb_batch_member_layout(psb_batch *b, int member, psb_batch_layout *layout);
 psb_status psb_batch_free(psb_batch *b);
 
 /* ------------------------------------------------------------------------ */
@@ -678,6 +690,8 @@ typedef struct {
   int steps_done;
   double residual;        /* last relative residual, -1 if never checked */
   double submit_s, start_s, finish_s;  /* host steady clock, seconds */
+  int wave_rounds;        /* rounds in which its steps overlapped as a wavefront
+                             (psb_batch_layout.wavefront) */
 } psb_result;
 /* max_slots: requests advanced at once (0: no limit). The budget covers
  * every resident grid, including those of finished requests whose results

@@ -155,7 +155,14 @@ class Result(ctypes.Structure):
     """psb_result."""
     _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int), ("steps_done", ctypes.c_int),
                 ("residual", ctypes.c_double), ("submit_s", ctypes.c_double),
-                ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double)]
+                ("start_s", ctypes.c_double), ("finish_s", ctypes.c_double),
+                ("wave_rounds", ctypes.c_int)]
+
+
+class BatchLayout(ctypes.Structure):
+    """psb_batch_layout."""
+    _fields_ = [("tile_x", ctypes.c_int), ("tile_y", ctypes.c_int), ("z_chunk", ctypes.c_int),
+                ("tiles", ctypes.c_int), ("wavefront", ctypes.c_int)]
 
 
 # ---------------------------------------------------------------------------
@@ -240,6 +247,7 @@ def _load():
         "psb_batch_member_result": (S, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_int)]),
+        "psb_batch_member_layout": (S, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchLayout)]),
         "psb_server_create": (S, [ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
         "psb_server_submit": (S, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]),
         "psb_server_cancel": (S, [ctypes.c_void_p, ctypes.c_int64]),
@@ -719,6 +727,14 @@ class Batch:
                                           ctypes.byref(which)), "psb_batch_member_result")
         return st.value, res.value, self.members[member][which.value]
 
+    def layout(self, member):
+        """How the last mode-0/1 run cut the member into items (dict of
+        psb_batch_layout)."""
+        lay = BatchLayout()
+        check(lib.psb_batch_member_layout(self.ptr, member, ctypes.byref(lay)),
+              "psb_batch_member_layout")
+        return {k: getattr(lay, k) for k, _ in lay._fields_}
+
     def free(self):
         if self.ptr:
             check(lib.psb_batch_free(self.ptr), "psb_batch_free")
@@ -801,7 +817,7 @@ class Server:
         self._keep.pop(r.id, None)
         return {"id": r.id, "status": r.status, "steps_done": r.steps_done,
                 "residual": r.residual, "submit_s": r.submit_s, "start_s": r.start_s,
-                "finish_s": r.finish_s}
+                "finish_s": r.finish_s, "wave_rounds": r.wave_rounds}
 
     def stats(self):
         c, rd, la = ctypes.c_int64(), ctypes.c_int64(), ctypes.c_int64()

@@ -901,6 +901,13 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
   return PSB_OK;
 }
 
+// Whether the steps of member i overlap as a wavefront in the prepared
+// launch (the producer's per-tile dependency path).
+bool batch_member_wavefront(const psb_batch *b, int i) {
+  return b->built && i >= 0 && i < (int)b->members.size() &&
+         b->members[i].ntiles >= kWaveTiles && b->members[i].steps > 1;
+}
+
 // After a run: per member, local steps completed when it converged (-1 if
 // it did not) and its residual state (4 doubles).
 psb_status batch_read_state(psb_batch *b, std::vector<int> &stop, std::vector<double> &res) {
@@ -1245,6 +1252,19 @@ psb_status psb_batch_member_result(psb_batch *b, int member, int *steps_done, do
   if (steps_done) *steps_done = done;
   if (residual) *residual = res;
   if (result_grid) *result_grid = done & 1;
+  return PSB_OK;
+}
+
+psb_status psb_batch_member_layout(psb_batch *b, int member, psb_batch_layout *layout) {
+  if (!b || !layout || member < 0 || member >= (int)b->hm.size() || !b->built)
+    return set_status(PSB_ERR_INVALID);
+  const BMember &M = b->members[member];
+  const bool him = M.kind == BK_HIMENO;
+  layout->tile_x = (him ? M.hg.tx_threads : M.dg.tx_threads) * 4;
+  layout->tile_y = him ? M.hg.ty_threads : M.dg.ty_threads * kVY;
+  layout->z_chunk = him ? M.hg.zchunk : M.dg.zchunk;
+  layout->tiles = M.ntiles;
+  layout->wavefront = batch_member_wavefront(b, member) ? 1 : 0;
   return PSB_OK;
 }
 

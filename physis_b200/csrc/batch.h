@@ -32,6 +32,7 @@ psb_status batch_launch_persistent(psb_batch *b, cudaStream_t s, int64_t *launch
 psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches);
 psb_status batch_add_member(psb_batch *b, const BatchMemberHost &m);
 psb_status batch_read_state(psb_batch *b, std::vector<int> &stop, std::vector<double> &res);
+bool batch_member_wavefront(const psb_batch *b, int i);
 // Server access to a batch's member list (replaced every round).
 psb_batch *batch_new();
 void batch_set_members(psb_batch *b, const std::vector<BatchMemberHost> &m,

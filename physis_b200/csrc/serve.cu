@@ -60,6 +60,7 @@ struct SReq {
   std::atomic<bool> cancel{false};
   bool complete = false;
   int skipped = 0;  // consecutive rounds this admitted request was left out of
+  int wave_rounds = 0;  // rounds in which its steps overlapped as a wavefront
   BatchMemberHost h;
   double res[4] = {0, 0, 0, 0};
   cudaEvent_t copied = nullptr;
@@ -387,6 +388,8 @@ static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
   const double t0 = now_s();
   batch_set_members(S->batch, hm, res_init);
   PSB_CHECK(batch_prepare(S->batch, steps, step0));
+  for (int i = 0; i < n; i++)
+    if (batch_member_wavefront(S->batch, i)) round_reqs[i]->wave_rounds++;
   const double t1 = now_s();
   // Results of the previous round: packed now, copied out while this round runs.
   const int nretire = (int)finished.size();
@@ -785,6 +788,7 @@ psb_status psb_server_wait(psb_server *S, int64_t id, double timeout_s, psb_resu
         res->status = q->status;
         res->steps_done = q->steps_done;
         res->residual = q->residual;
+        res->wave_rounds = q->wave_rounds;
         res->submit_s = q->submit_s;
         res->start_s = q->start_s;
         res->finish_s = q->finish_s;

@@ -1,9 +1,15 @@
 import os
 import sys
+import tempfile
 
 ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
+
+# The autotuner's user cache: a per-session file, so that tests neither read
+# nor change the caches of whoever runs them. The shipped table still loads.
+os.environ.setdefault("PHYSIS_B200_TUNE_CACHE",
+                      os.path.join(tempfile.mkdtemp(prefix="physis_b200_tune_"), "tune.json"))
 
 
 def pytest_configure(config):

@@ -162,3 +162,80 @@ def test_grid_fill_matches_host_restatement(kind):
             assert U.bits_equal(got, want)
         finally:
             ps.PSGridFree(g)
+
+
+# Members large enough (>= 128 items per step) that an item waits only for
+# the 27 items around it in the member's previous step, so consecutive steps
+# overlap as a wavefront: clamped and periodic 7-point (a periodic member
+# one tile wide in x, whose dependencies wrap onto itself) and Himeno.
+WAVE_MEMBERS = [
+    ("diff", (192, 192, 192), 24),
+    ("diffp", (160, 160, 160), 30),
+    ("him", (160, 160, 160), 20),
+    ("diffp", (64, 48, 512), 25),
+    ("him", (300, 40, 130), 16),
+]
+
+_WANT_CACHE = {}
+
+
+def _want_cached(i, kind, data, steps):
+    key = (i, kind, steps)
+    if key not in _WANT_CACHE:
+        _WANT_CACHE[key] = _want(kind, data, steps)
+    return _WANT_CACHE[key]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mix", ["alone", "mixed"])
+def test_batch_wavefront_members_bit_exact(mix):
+    """Large members take the per-tile (wavefront) dependency path; each is
+    bit-exact against the oracle whether it runs alone or with every other
+    large member and the small members of MEMBERS."""
+    spec = WAVE_MEMBERS + (MEMBERS if mix == "mixed" else [])
+    M = Members(spec)
+    try:
+        groups = [[i] for i in range(len(WAVE_MEMBERS))] if mix == "alone" else [list(range(len(spec)))]
+        for ids in groups:
+            sub = Members.__new__(Members)
+            sub.spec = [spec[i] for i in ids]
+            sub.data = [M.data[i] for i in ids]
+            sub.grids = [M.grids[i] for i in ids]
+            b = sub.batch()
+            b.run(0)
+            for j, i in enumerate(ids):
+                kind, dims, steps = spec[i]
+                lay = b.layout(j)
+                done, _, g = b.result(j)
+                assert done == steps
+                if i < len(WAVE_MEMBERS):
+                    assert lay["wavefront"] == 1 and lay["tiles"] >= 128, (i, lay)
+                else:
+                    assert lay["wavefront"] == 0, (i, lay)
+                want = (_want_cached(i, kind, M.data[i], steps) if i < len(WAVE_MEMBERS)
+                        else _want(kind, M.data[i], steps))
+                assert U.bits_equal(ps.PSGridCopyout(g), want), (mix, i, kind, dims, lay)
+            b.free()
+    finally:
+        M.free()
+
+
+@pytest.mark.gpu
+def test_batch_wavefront_with_residual_checks():
+    """Wavefront members with residual checks: the step after a check waits
+    for the whole step and its decision; stop steps and fields equal the
+    oracle's after that many steps."""
+    spec = [("diff", (192, 160, 96), 60), ("him", (160, 128, 96), 40)]
+    stop = lambda i: ((3e-3, 7), (0.5, 5))[i]
+    M = Members(spec)
+    try:
+        b = M.batch(stop)
+        b.run(0)
+        for i, (kind, dims, steps) in enumerate(spec):
+            assert b.layout(i)["wavefront"] == 1
+            done, res, g = b.result(i)
+            assert 0 < done <= steps
+            assert U.bits_equal(ps.PSGridCopyout(g), _want(kind, M.data[i], done)), (i, done)
+        b.free()
+    finally:
+        M.free()

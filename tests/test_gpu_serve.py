@@ -216,3 +216,36 @@ def test_continuous_admission_overlaps_requests():
         assert s.stats()["rounds"] >= 2
     finally:
         s.destroy()
+
+
+def test_large_requests_take_the_wavefront_path():
+    """Requests large enough for the batched kernel's per-tile dependencies
+    (their steps overlap as a wavefront): a 200^3 clamped diffusion and a
+    176x160x144 Himeno solve with a residual stop, served together with the
+    small mix. Each equals the oracle, and equals itself served alone."""
+    nd = (200, 200, 200)
+    u0 = np.random.default_rng(23).random(tuple(reversed(nd)), dtype=np.float32)
+    hd = (176, 160, 144)
+    p, coef = himeno_inputs(tuple(reversed(hd)), 21)
+    ce, max_steps = 5, 40
+    _, gosa = O.himeno(p, coef, 0.8, max_steps)
+    checks = [1] + list(range(ce, max_steps + 1, ce))
+    res = {n: float(np.sqrt(gosa[n - 1] / gosa[0])) for n in checks}
+    tol = float(np.sqrt(res[checks[3]] * res[checks[4]]))
+    stop = next(n for n in checks if res[n] <= tol)
+    big = [dict(kernel=ps.DIFFUSION7, dims=nd, params=list(COEF), max_steps=36, init=u0),
+           dict(kernel=ps.HIMENO19, dims=hd, params=[0.8], max_steps=max_steps, tol=tol,
+                check_every=ce, init=np.ascontiguousarray(p),
+                coef=np.ascontiguousarray(np.stack(coef)))]
+    recs, outs, _ = _serve(big + _mix())
+    want = [O.diffusion7(u0, 36, np.asarray(COEF, np.float32)), O.himeno(p, coef, 0.8, stop)[0]]
+    assert recs[0]["steps_done"] == 36
+    assert recs[1]["steps_done"] == stop
+    assert recs[1]["residual"] == pytest.approx(res[stop], rel=1e-9)
+    for i in range(2):
+        assert recs[i]["wave_rounds"] >= 1, recs[i]
+        assert bits_equal(outs[i], want[i]), i
+        alone_recs, alone_outs, _ = _serve([big[i]])
+        assert alone_recs[0]["steps_done"] == recs[i]["steps_done"]
+        assert alone_recs[0]["wave_rounds"] >= 1
+        assert bits_equal(alone_outs[0], want[i]), i

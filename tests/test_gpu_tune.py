@@ -1,0 +1,90 @@
+"""The autotuner (psb_autotune) on the GPU: it times the candidate tile
+configurations of a (kernel, type, shape) key, keeps the fastest, caches it
+in the JSON file and makes PSStencilRun use it. The chosen configuration
+must be one of the candidates, survive a reload of the cache, and the run
+with it must stay bit-exact against the oracle (the reference tunes at
+translation time by trial, translator/reference_translator.cc:749-1223)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import physis_b200 as ps
+from oracle import oracle
+from tests import gpu_util as U
+
+pytestmark = pytest.mark.gpu
+
+COEF = [0.1, 0.1, 0.1, 0.1, 0.1, 0.1, 0.4]
+CASES = [(ps.DIFFUSION7, ps.PS_FLOAT, (96, 80, 40)),
+         (ps.DIFFUSION7_PERIODIC, ps.PS_FLOAT, (64, 48, 32)),
+         (ps.DIFFUSION7, ps.PS_DOUBLE, (64, 40, 36)),
+         (ps.HIMENO19, ps.PS_FLOAT, (65, 49, 33))]
+
+
+def _valid(kernel, type_, dims, c):
+    if c["impl"] == ps.IMPL_PLAIN:
+        return True
+    if c["impl"] != ps.IMPL_TMA or c["stages"] not in (4, 6, 8):
+        return False
+    if c["t_depth"] == 2:
+        return kernel == ps.DIFFUSION7 and type_ == ps.PS_FLOAT and c["z_chunk"] in (32, 64, 128)
+    txs = (16, 32, 64) if type_ == ps.PS_DOUBLE else (32, 64, 128)
+    tys = (4, 8, 16) if kernel == ps.HIMENO19 else (4, 8, 16, 32)
+    return (c["t_depth"] == 1 and c["tile_x"] in txs and c["tile_y"] in tys
+            and c["z_chunk"] in (2, 4, 8, 16, 32, 64, 128) and c["z_chunk"] <= 2 * dims[2])
+
+
+@pytest.mark.parametrize("kernel,type_,dims", CASES)
+def test_autotune_picks_a_candidate_and_stays_bit_exact(kernel, type_, dims):
+    ps.PSInit()
+    cfg = ps.autotune(kernel, type_, dims, force=True)
+    assert _valid(kernel, type_, dims, cfg), cfg
+    assert ps.tune_get(kernel, type_, dims) == cfg
+    # The choice is in the cache file under its key.
+    with open(os.environ["PHYSIS_B200_TUNE_CACHE"]) as f:
+        entries = json.load(f)
+    hit = [e for e in entries if e["kernel"] == kernel and e["type"] == type_
+           and e["n"] == list(dims)]
+    assert len(hit) == 1
+    assert {k: hit[0][k] for k in cfg} == cfg
+    # Not forced: the cached entry comes back without tuning again.
+    assert ps.autotune(kernel, type_, dims) == cfg
+    nx, ny, nz = dims
+    if kernel == ps.HIMENO19:
+        p, coef = U.himeno_inputs((nz, ny, nx), 3)
+        got, gosa = U.himeno_gpu(p, coef, 0.8, 6)
+        want, wgosa = oracle.himeno(p, coef, 0.8, 6)
+        assert U.bits_equal(got, want)
+        assert np.allclose(gosa, wgosa, rtol=1e-12, atol=0)
+    else:
+        dt = np.float32 if type_ == ps.PS_FLOAT else np.float64
+        f = np.random.default_rng(4).random((nz, ny, nx)).astype(dt)
+        periodic = kernel == ps.DIFFUSION7_PERIODIC
+        got = U.diffusion_gpu(f, 10, COEF, periodic=periodic)
+        want = oracle.diffusion7(f, 10, np.asarray(COEF, dt), periodic=periodic)
+        assert U.bits_equal(got, want)
+
+
+def test_tune_set_overrides_and_every_candidate_shape_runs():
+    """psb_tune_set installs a configuration that PSStencilRun then uses; a
+    sweep of explicit shapes (all bit-exact) covers the tuner's candidate
+    space beyond the one it picked."""
+    ps.PSInit()
+    dims = (72, 40, 24)
+    f = np.random.default_rng(8).random(tuple(reversed(dims)), dtype=np.float32)
+    want = oracle.diffusion7(f, 4, np.asarray(COEF, np.float32))
+    try:
+        for tx in (32, 64, 128):
+            for ty in (4, 8, 16, 32):
+                for zc, st in ((2, 4), (16, 6), (64, 8)):
+                    cfg = dict(impl=ps.IMPL_TMA, tile_x=tx, tile_y=ty, z_chunk=zc, stages=st,
+                               t_depth=1)
+                    ps.tune_set(ps.DIFFUSION7, ps.PS_FLOAT, dims, **cfg)
+                    assert ps.tune_get(ps.DIFFUSION7, ps.PS_FLOAT, dims) == cfg
+                    got = U.diffusion_gpu(f, 4, COEF)
+                    assert U.bits_equal(got, want), cfg
+    finally:
+        ps.tune_set(ps.DIFFUSION7, ps.PS_FLOAT, dims, impl=ps.IMPL_PLAIN, tile_x=32, tile_y=16,
+                    z_chunk=16, stages=6, t_depth=1)
