@@ -250,6 +250,112 @@ def cpu_baseline_sample(wl, field=None):
             "sample": sample + "; " + who + "; run loop only, copies excluded"}
 
 
+# ---------------------------------------------------------------------------
+# Numerics: every run states its error against the FP64 oracle
+# ---------------------------------------------------------------------------
+NUMERICS_SIDE = 96       # the full-length solve is checked at this size
+NUMERICS_FULL_STEPS = 2  # the full-size grid is checked after this many steps
+
+
+def _coef_sum(dt):
+    return float(sum(np.float64(np.asarray(COEF, dt))))
+
+
+def numerics_diffusion(ps, dt, dims, tsteps, grids, m1, m2, host, mass0, mass1, steps_done):
+    """Error of the 7-point path against the oracle, outside the timed
+    region: (1) the full-size grid after NUMERICS_FULL_STEPS steps from the
+    workload's field, against the oracle port (the reference CPU target bit
+    for bit: `bit_exact_vs_reference`) and the FP64 oracle; (2) a full-length
+    solve (tsteps steps) of the same field formula at NUMERICS_SIDE^3,
+    likewise; (3) the timed solves themselves: the clamped scheme conserves
+    sum(u) * (sum of coefficients)^steps exactly, so the drift of the device
+    sum (FP64 reduction) from that value is the rounding of every step run."""
+    from oracle import oracle
+    coef = np.asarray(COEF, dt)
+    out = {"vs": "FP64 oracle (the reference's algorithm and term order in double from the "
+                 "same inputs); bit_exact_vs_reference: equality with the oracle port, which "
+                 "equals the reference CPU target bit for bit"}
+    # (3) mass after every warm-up and timed step
+    expect = mass0 * _coef_sum(dt) ** steps_done
+    out["timed_solves_mass"] = {"steps": steps_done, "sum_initial": mass0, "sum_final": mass1,
+                                "sum_expected": expect, "rel_drift": abs(mass1 - expect) / abs(expect)}
+    # (1) full size, a few steps
+    ps.PSGridCopyin(grids[0], host)
+    ps.PSStencilRun(m1, m2, NUMERICS_FULL_STEPS // 2)
+    got = ps.PSGridCopyout(grids[0])
+    want = oracle.diffusion7(host, NUMERICS_FULL_STEPS, coef)
+    ref64 = oracle.diffusion7_fp64(host, NUMERICS_FULL_STEPS, coef)
+    full = {"sample": "%dx%dx%d after %d steps" % (dims + (NUMERICS_FULL_STEPS,)),
+            "bit_exact_vs_reference": bool(np.array_equal(got.view(np.uint8), want.view(np.uint8)))}
+    full.update(oracle.error_norms(got, ref64))
+    full["max_ulp_vs_reference"] = oracle.error_norms(got, want)["max_ulp_err"]
+    del got, want, ref64
+    out["full_size"] = full
+    # (2) full-length solve, smaller grid
+    n = NUMERICS_SIDE
+    f = c2_field((n, n, n), dt)
+    g = [ps.grid_new(ps.PS_FLOAT if dt == np.float32 else ps.PS_DOUBLE, (n, n, n))
+         for _ in range(2)]
+    ps.PSGridCopyin(g[0], f)
+    d = ps.PSDomain3DNew(0, n, 0, n, 0, n)
+    a = ps.PSStencilMap(ps.DIFFUSION7, d, g[0], g[1], *COEF)
+    b = ps.PSStencilMap(ps.DIFFUSION7, d, g[1], g[0], *COEF)
+    ps.PSStencilRun(a, b, tsteps // 2)
+    got = ps.PSGridCopyout(g[0])
+    for x in g:
+        ps.PSGridFree(x)
+    want = oracle.diffusion7(f, tsteps, coef)
+    ref64 = oracle.diffusion7_fp64(f, tsteps, coef)
+    solve = {"sample": "%d^3, %d steps (the full solve length), same field formula" % (n, tsteps),
+             "bit_exact_vs_reference": bool(np.array_equal(got.view(np.uint8), want.view(np.uint8)))}
+    solve.update(oracle.error_norms(got, ref64))
+    solve["reference_vs_fp64"] = oracle.error_norms(want, ref64)
+    solve["max_ulp_vs_reference"] = oracle.error_norms(got, want)["max_ulp_err"]
+    out["full_solve"] = solve
+    out["bit_exact_vs_reference"] = full["bit_exact_vs_reference"] and solve["bit_exact_vs_reference"]
+    out["max_abs_err"] = max(full["max_abs_err"], solve["max_abs_err"])
+    out["rms_err"] = solve["rms_err"]
+    return out
+
+
+def numerics_himeno(ps, dims, tsteps, grids, m1, m2, p, coef):
+    """Error of the Himeno path: the full-size grids after 2 sweeps and a
+    full-length run (tsteps sweeps) at 65x65x129, each against the oracle
+    port (bit-exact check, per-sweep residuals) and the FP64 oracle."""
+    from oracle import oracle
+    from physis_b200.workloads import himeno_gpu, himeno_inputs
+    out = {"vs": "FP64 oracle (the reference's algorithm and term order in double from the "
+                 "same inputs); bit_exact_vs_reference: equality with the oracle port, which "
+                 "equals the reference CPU target bit for bit"}
+    ps.PSGridCopyin(grids[0], p)
+    ps.PSGridCopyin(grids[1], p)
+    ps.PSStencilRun(m1, m2, 1)
+    got = ps.PSGridCopyout(grids[0])
+    want, wg = oracle.himeno(p, coef, 0.8, 2)
+    ref64, g64 = oracle.himeno_fp64(p, coef, 0.8, 2)
+    full = {"sample": "%dx%dx%d after 2 sweeps" % dims,
+            "bit_exact_vs_reference": bool(np.array_equal(got.view(np.uint8), want.view(np.uint8)))}
+    full.update(oracle.error_norms(got, ref64))
+    del got, want, ref64
+    out["full_size"] = full
+    shape = (129, 65, 65)
+    ps_, cf = himeno_inputs(shape, 5)
+    got, gg = himeno_gpu(ps_, cf, 0.8, tsteps)
+    want, wg = oracle.himeno(ps_, cf, 0.8, tsteps)
+    ref64, g64 = oracle.himeno_fp64(ps_, cf, 0.8, tsteps)
+    solve = {"sample": "65x65x129, %d sweeps (the full run length)" % tsteps,
+             "bit_exact_vs_reference": bool(np.array_equal(got.view(np.uint8), want.view(np.uint8)))}
+    solve.update(oracle.error_norms(got, ref64))
+    gg = np.asarray(gg)
+    solve["gosa_max_rel_diff_vs_reference"] = float(np.max(np.abs(gg - wg) / np.abs(wg)))
+    solve["gosa_max_rel_err_vs_fp64"] = float(np.max(np.abs(gg - g64) / np.abs(g64)))
+    out["full_solve"] = solve
+    out["bit_exact_vs_reference"] = full["bit_exact_vs_reference"] and solve["bit_exact_vs_reference"]
+    out["max_abs_err"] = max(full["max_abs_err"], solve["max_abs_err"])
+    out["rms_err"] = solve["rms_err"]
+    return out
+
+
 def run_ours(args):
     dist = Dist(args.gpus)
     os.environ["PHYSIS_B200_DEVICE"] = str(dist.local)
@@ -263,6 +369,7 @@ def run_ours(args):
     tune = ps.autotune(kernel, ptype, dims) if args.tune else ps.tune_get(kernel, ptype, dims)
     if args.plain:
         ps.set_impl(ps.IMPL_PLAIN)
+    ps.set_fp_mode(ps.FP_FMA if args.fp_mode == "fma" else ps.FP_EXACT)
 
     # Inputs, pinned host buffers for the end-to-end leg.
     if kname == "himeno":
@@ -296,6 +403,7 @@ def run_ours(args):
         return ps.last_run_stats()
 
     # ---- device-resident timing ------------------------------------------
+    mass0 = ps.reduce64(ps.PS_SUM, g_io) if kname != "himeno" else None
     for _ in range(args.warmup):
         solve()
     ps.sync()
@@ -313,6 +421,7 @@ def run_ours(args):
     wall = time.perf_counter() - t0
     clocks = sampler.stop()
     dist.barrier()
+    mass1 = ps.reduce64(ps.PS_SUM, g_io) if kname != "himeno" else None
     dev_s = sum(ms_list) / 1e3
     dev_s_max = dist.max(dev_s)
     total_pts = dist.sum(pts_per_step * args.steps)
@@ -351,6 +460,13 @@ def run_ours(args):
         e2e_value = dist.sum(pts_per_step * e2e_steps) / e2e_s / 1e9
     ps.check(ps.lib.psb_host_free(hp), "psb_host_free")
 
+    numerics = None
+    if dist.rank == 0 and not args.no_numerics:
+        if kname == "himeno":
+            numerics = numerics_himeno(ps, dims, tsteps, grids, m1, m2, p, coef)
+        else:
+            numerics = numerics_diffusion(ps, dt, dims, tsteps, grids, m1, m2, host, mass0, mass1,
+                                          (args.warmup + args.steps) * tsteps)
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(wl, host if kname != "himeno" else None)
@@ -374,6 +490,11 @@ def run_ours(args):
             "inputs_vs_l2": "%.0f MB per grid > 126 MB L2; no flush needed" % (host.nbytes / 1e6),
             "parallelism": "replicas (one independent solve per GPU, no exchange)",
             "impl": "plain" if args.plain else "autotuned",
+            "fp_mode": ("exact: every product and sum rounded in the reference's term order "
+                        "(bit-identical to the reference CPU target)" if args.fp_mode == "exact"
+                        or args.plain or kname != "diffusion7" else
+                        "fma: the reference's term order with fused multiply-adds (one rounding "
+                        "per term; within 4 ulp of the reference per step)"),
             "tune": tune,
             "hbm_gbs_effective": value * bpl,
             "wall_s_timed": wall,
@@ -395,6 +516,7 @@ def run_ours(args):
         "gpu_launches": int(launches),
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "numerics": numerics,
     }
     for g in grids:
         ps.PSGridFree(g)
@@ -517,6 +639,89 @@ def c4_e2e(ps, members, grids, b, lups, dist, reps=2):
             "h2d_bytes_per_step": n_in * 4, "d2h_bytes_per_step": n_out * 4}
 
 
+C4_HIMENO_RANGES = [(0.9, 1.1)] * 3 + [(0.95 / 6, 1.05 / 6)] + [(-0.01, 0.01)] * 3 + [(0.9, 1.1)] * 3
+
+
+def c4_host_inputs(ps, kind, dims, i):
+    """Host copies of member i's seeded inputs (the host restatement of the
+    device fills of c4_build, equal to them bit for bit)."""
+    if kind == "diffp":
+        return ps.fill_reference(dims, ps.FILL_UNIFORM, 1000 + i, 0.0, 1.0), None
+    p = ps.fill_reference(dims, ps.FILL_ZPROFILE)
+    coef = [ps.fill_reference(dims, ps.FILL_UNIFORM, 100000 * (i + 1) + k, lo, hi)
+            for k, (lo, hi) in enumerate(C4_HIMENO_RANGES)]
+    coef += [ps.fill_reference(dims, ps.FILL_BND), np.zeros(tuple(reversed(dims)), np.float32)]
+    return p, coef
+
+
+def member_numerics(kind, data, steps, got):
+    """One solve against the oracle port (bit-exact check) and the FP64
+    oracle (error norms). kind: "diff", "diffp" or "him"."""
+    from oracle import oracle
+    f, coef = data
+    if kind == "him":
+        want = oracle.himeno(f, coef, 0.8, steps)[0]
+        ref64 = oracle.himeno_fp64(f, coef, 0.8, steps)[0]
+    else:
+        per = kind == "diffp"
+        want = oracle.diffusion7(f, steps, np.asarray(COEF, np.float32), periodic=per)
+        ref64 = oracle.diffusion7_fp64(f, steps, COEF, periodic=per)
+    out = {"bit_exact_vs_reference": bool(np.array_equal(got.view(np.uint8), want.view(np.uint8)))}
+    out.update(oracle.error_norms(got, ref64))
+    return out
+
+
+def summarize_numerics(recs, what):
+    return {"vs": "FP64 oracle (the reference's algorithm and term order in double from the "
+                  "same inputs); bit_exact_vs_reference: equality with the oracle port, which "
+                  "equals the reference CPU target bit for bit",
+            "sample": what, "solves_checked": len(recs),
+            "bit_exact_vs_reference": all(r["bit_exact_vs_reference"] for r in recs),
+            "max_abs_err": max(r["max_abs_err"] for r in recs),
+            "rms_err": float(np.sqrt(np.mean([r["rms_err"] ** 2 for r in recs]))),
+            "max_rel_err": max(r["max_rel_err"] for r in recs),
+            "per_solve": recs}
+
+
+def c4_numerics(ps, members, grids, b, max_work=3e8):
+    """After the timed runs: the sampled members' inputs are regenerated,
+    the whole batch runs once more (mode 0), and each sampled member is
+    compared with the oracle. Sample: the five cheapest members of each kind
+    and the cheapest member of each kind that took the wavefront path."""
+    def work(i):
+        k, d, st = members[i]
+        return d[0] * d[1] * d[2] * st
+    sample = []
+    for kind in ("diffp", "him"):
+        ids = sorted((i for i, m in enumerate(members) if m[0] == kind), key=work)
+        sample += ids[:5]
+        wave = [i for i in ids if b.layout(i)["wavefront"] and work(i) <= max_work]
+        if wave:
+            sample.append(wave[0])
+    for i in sample:
+        kind, dims, steps = members[i]
+        g = grids[i]
+        if kind == "diffp":
+            ps.grid_fill(g[0], ps.FILL_UNIFORM, 1000 + i, 0.0, 1.0)
+        else:
+            ps.grid_fill(g[0], ps.FILL_ZPROFILE)
+            ps.grid_fill(g[1], ps.FILL_ZPROFILE)
+    ps.sync()
+    b.run(0)
+    recs = []
+    for i in sample:
+        kind, dims, steps = members[i]
+        done, _, g = b.result(i)
+        got = ps.PSGridCopyout(g)
+        r = member_numerics(kind, c4_host_inputs(ps, kind, dims, i), done, got)
+        r.update({"member": i, "kind": kind, "dims": list(dims), "steps": done,
+                  "wavefront": bool(b.layout(i)["wavefront"])})
+        recs.append(r)
+    return summarize_numerics(recs, "the five cheapest members of each kind and the cheapest "
+                                    "wavefront-path member of each kind (<= %.0e updates), "
+                                    "rerun from their seeded inputs in the whole batch" % max_work)
+
+
 def run_c4(args, dist):
     os.environ["PHYSIS_B200_DEVICE"] = str(dist.local)
     import physis_b200 as ps
@@ -554,6 +759,9 @@ def run_c4(args, dist):
     loop_tuned = timed(3, 1, 0)[0] if not args.skip_loops else float("nan")
     per_run_s = dev_s / args.steps
     e2e = None if args.no_e2e else c4_e2e(ps, members, grids, b, lups, dist)
+    numerics = None
+    if dist.rank == 0 and not args.no_numerics:
+        numerics = c4_numerics(ps, members, grids, b)
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
         rate_d, rate_h, kind, sample = cpu_rates(periodic=True)
@@ -592,6 +800,7 @@ def run_c4(args, dist):
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "numerics": numerics,
     }
     b.free()
     for g in grids:
@@ -692,7 +901,45 @@ def serve_trace(ps, trace, mode, shared_init, out_arena):
             "mean_steps": float(np.mean([r["steps_done"] for r in recs])),
             "converged": int(sum(r["steps_done"] < C5_MAX_STEPS for r in recs)),
             "lattice_updates": lups, "alg_bytes": alg, "h2d": h2d, "d2h": d2h,
-            "steps_done": {index[r["id"]]: r["steps_done"] for r in recs}, **stats}
+            "steps_done": {index[r["id"]]: r["steps_done"] for r in recs},
+            "wave_rounds": {index[r["id"]]: r["wave_rounds"] for r in recs}, **stats}
+
+
+def c5_numerics(ps, trace, served, shared, arena, max_work=5e8):
+    """Served results against the oracle: the four smallest requests of each
+    kind and the cheapest one of each kind that ran on the wavefront path
+    (<= max_work updates), each compared after the steps it was served."""
+    offs = np.cumsum([0] + [side ** 3 for _, _, side, _ in trace])
+    steps = served["steps_done"]
+    waves = served["wave_rounds"]
+    sample = []
+    for kind in ("diff", "him"):
+        ids = sorted((i for i, t in enumerate(trace) if t[1] == kind), key=lambda i: trace[i][2])
+        sample += ids[:4]
+        wave = [i for i in sorted(ids, key=lambda i: trace[i][2] ** 3 * steps[i])
+                if waves[i] > 0 and trace[i][2] ** 3 * steps[i] <= max_work]
+        if wave:
+            sample.append(wave[0])
+    recs = []
+    for i in sample:
+        _, kind, side, seed = trace[i]
+        dims = (side, side, side)
+        got = np.array(arena[offs[i]:offs[i + 1]]).reshape(side, side, side)
+        if kind == "diff":
+            data = (np.array(shared[:side ** 3]).reshape(side, side, side), None)
+        else:
+            p = ps.fill_reference(dims, ps.FILL_ZPROFILE)
+            coef = [ps.fill_reference(dims, ps.FILL_UNIFORM, seed * 16 + 1 + k, lo, hi)
+                    for k, (lo, hi) in enumerate(C4_HIMENO_RANGES)]
+            coef += [ps.fill_reference(dims, ps.FILL_BND), np.zeros((side,) * 3, np.float32)]
+            data = (p, coef)
+        r = member_numerics(kind, data, steps[i], got)
+        r.update({"request": i, "kind": kind, "side": side, "steps": steps[i],
+                  "wave_rounds": waves[i]})
+        recs.append(r)
+    return summarize_numerics(recs, "the four smallest requests of each kind and the cheapest "
+                                    "wavefront-path request of each kind (<= %.0e updates), "
+                                    "after the steps each was served" % max_work)
 
 
 def run_c5(args, dist):
@@ -719,6 +966,9 @@ def run_c5(args, dist):
     sampler.start()
     ours = serve_trace(ps, trace, ps.SERVE_BATCHED, shared, arena)
     clocks = sampler.stop()
+    numerics = None
+    if dist.rank == 0 and not args.no_numerics:
+        numerics = c5_numerics(ps, trace, ours, shared, arena)
     fifo = None if args.c5_skip_fifo else serve_trace(ps, trace, ps.SERVE_FIFO, shared, arena)
     for hp in (hp_in, hp_out):
         ps.check(ps.lib.psb_host_free(hp), "psb_host_free")
@@ -768,6 +1018,7 @@ def run_c5(args, dist):
         "gpu_launches": ours["launches"],
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "numerics": numerics,
     }
     dist.close()
     if dist.rank == 0:
@@ -918,12 +1169,16 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--tune", action="store_true", help="autotune before timing")
     ap.add_argument("--plain", action="store_true", help="time the plain one-launch kernel")
+    ap.add_argument("--fp-mode", default="exact", choices=["exact", "fma"],
+                    help="arithmetic of the 7-point TMA kernel")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-procs", type=int, default=64)
     ap.add_argument("--dims", default=None, help="override grid extents nx,ny,nz (profiling)")
     ap.add_argument("--time-steps", type=int, default=None,
                     help="override time steps per solve (profiling)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-numerics", action="store_true",
+                    help="skip the error report against the oracle (profiling runs)")
     ap.add_argument("--no-residual", action="store_true", help="c3: skip the fused residual")
     ap.add_argument("--members", type=int, default=256, help="c4: batch members (profiling)")
     ap.add_argument("--skip-loops", action="store_true", help="c4: skip the per-grid loops")

@@ -57,6 +57,8 @@ def port():
             f.argtypes = [I, I, I, P, P, I, P, I, P, P]
         lib.orc_himeno_f32.restype = None
         lib.orc_himeno_f32.argtypes = [I, I, I, P, P, P, ctypes.c_float, I, P]
+        lib.orc_himeno_f64.restype = None
+        lib.orc_himeno_f64.argtypes = [I, I, I, P, P, P, ctypes.c_double, I, P]
         lib.orc_generic_apply.restype = None
         lib.orc_generic_apply.argtypes = [P, P, P, P, P, I]
         lib.orc_fold_f32.restype = None
@@ -133,6 +135,46 @@ def himeno(p, coef, omega, sweeps):
     port().orc_himeno_f32(nx, ny, nz, _ptr(a), _ptr(b), ctypes.cast(arr, ctypes.c_void_p),
                           ctypes.c_float(omega), sweeps, _ptr(gosa))
     return (a if sweeps % 2 == 0 else b), gosa[:sweeps]
+
+
+# ---------------------------------------------------------------------------
+# FP64 oracle: the same algorithms, term order and inputs, in double
+# ---------------------------------------------------------------------------
+def diffusion7_fp64(field, steps, coef, periodic=False):
+    """The 7-point run of diffusion7() in double from the same inputs: the
+    field and the coefficients are the fp32 (or fp64) values, widened."""
+    c = np.asarray(coef, dtype=field.dtype).astype(np.float64)
+    return diffusion7(np.asarray(field).astype(np.float64), steps, c, periodic=periodic)
+
+
+def himeno_fp64(p, coef, omega, sweeps):
+    """himeno() in double from the same fp32 inputs (omega as the float the
+    kernel uses). Returns (p after the sweeps, gosa per sweep)."""
+    a = np.array(p, dtype=np.float64, copy=True)
+    b = a.copy()
+    cs = [np.ascontiguousarray(c, dtype=np.float64) for c in coef]
+    arr = (ctypes.c_void_p * 12)(*[c.ctypes.data for c in cs])
+    gosa = np.zeros(max(1, sweeps), dtype=np.float64)
+    nz, ny, nx = a.shape
+    port().orc_himeno_f64(nx, ny, nz, _ptr(a), _ptr(b), ctypes.cast(arr, ctypes.c_void_p),
+                          float(np.float32(omega)), sweeps, _ptr(gosa))
+    return (a if sweeps % 2 == 0 else b), gosa[:sweeps]
+
+
+def error_norms(got, ref):
+    """Max and RMS absolute error of `got` against the FP64 oracle `ref`, the
+    max error relative to max |ref|, and the largest error in units of the
+    last place of got's type at the reference value."""
+    g = np.asarray(got, dtype=np.float64).ravel()
+    r = np.asarray(ref, dtype=np.float64).ravel()
+    d = np.abs(g - r)
+    scale = float(np.max(np.abs(r))) if r.size else 0.0
+    ulp = np.spacing(np.abs(r).astype(np.asarray(got).dtype)).astype(np.float64)
+    ulp[ulp == 0] = np.finfo(np.asarray(got).dtype).tiny
+    return {"max_abs_err": float(d.max()) if d.size else 0.0,
+            "rms_err": float(np.sqrt(np.mean(d * d))) if d.size else 0.0,
+            "max_rel_err": float(d.max() / scale) if d.size and scale > 0 else 0.0,
+            "max_ulp_err": float(np.max(d / ulp)) if d.size else 0.0}
 
 
 def generic_apply(desc, arrays, lo, hi, color=-1):

@@ -93,50 +93,56 @@ DEFINE_DIFFUSION7(orc_diffusion7_f64, double)
 /* loop order -- the residual of the original Himeno (gosa += ss*ss) carried */
 /* in FP64.                                                                   */
 /* ------------------------------------------------------------------------ */
-void orc_himeno_f32(int nx, int ny, int nz, float *p0, float *p1,
-                    const float *const *coef, float omega, int sweeps,
-                    double *gosa) {
-  const float *a0 = coef[0], *a1 = coef[1], *a2 = coef[2], *a3 = coef[3];
-  const float *b0 = coef[4], *b1 = coef[5], *b2 = coef[6];
-  const float *c0 = coef[7], *c1 = coef[8], *c2 = coef[9];
-  const float *bnd = coef[10], *wrk1 = coef[11];
-  float *src = p0, *dst = p1;
-#define P(i, j, k) src[IDX3(i, j, k, nx, ny)]
-  for (int it = 0; it < sweeps; it++) {
-    /* gosa with Neumaier compensation so the checker is accurate to a few
-       ulp whatever the summation order of the implementation under test */
-    double g = 0.0, gc = 0.0;
-    for (int k = 1; k < nz - 1; k++)
-      for (int j = 1; j < ny - 1; j++)
-        for (int i = 1; i < nx - 1; i++) {
-          int64_t o = IDX3(i, j, k, nx, ny);
-          float s0 = a0[o] * P(i, j, k + 1) + a1[o] * P(i, j + 1, k) +
-                     a2[o] * P(i + 1, j, k) +
-                     b0[o] * (P(i, j + 1, k + 1) - P(i, j - 1, k + 1) -
-                              P(i, j + 1, k - 1) + P(i, j - 1, k - 1)) +
-                     b1[o] * (P(i + 1, j + 1, k) - P(i + 1, j - 1, k) -
-                              P(i - 1, j + 1, k) + P(i - 1, j - 1, k)) +
-                     b2[o] * (P(i + 1, j, k + 1) - P(i + 1, j, k - 1) -
-                              P(i - 1, j, k + 1) + P(i - 1, j, k - 1)) +
-                     c0[o] * P(i, j, k - 1) + c1[o] * P(i, j - 1, k) +
-                     c2[o] * P(i - 1, j, k) + wrk1[o];
-          float ss = (s0 * a3[o] - P(i, j, k)) * bnd[o];
-          float v = P(i, j, k) + omega * ss;
-          dst[o] = v;
-          double q = (double)ss * (double)ss;
-          double t = g + q;
-          if (fabs(g) >= fabs(q)) gc += (g - t) + q; else gc += (q - t) + g;
-          g = t;
-        }
-    if (gosa) gosa[it] = g + gc;
-    float *t = src;
-    src = dst;
-    dst = t;
+/* The same sweep in REAL arithmetic: orc_himeno_f32 is the restatement of
+ * the fp32 kernel; orc_himeno_f64 runs the identical expression tree in
+ * double from inputs widened to double, the FP64 oracle against which the
+ * error of an fp32 run is measured. */
+#define DEFINE_HIMENO(NAME, REAL)                                              \
+  void NAME(int nx, int ny, int nz, REAL *p0, REAL *p1,                        \
+            const REAL *const *coef, REAL omega, int sweeps, double *gosa) {   \
+    const REAL *a0 = coef[0], *a1 = coef[1], *a2 = coef[2], *a3 = coef[3];     \
+    const REAL *b0 = coef[4], *b1 = coef[5], *b2 = coef[6];                    \
+    const REAL *c0 = coef[7], *c1 = coef[8], *c2 = coef[9];                    \
+    const REAL *bnd = coef[10], *wrk1 = coef[11];                              \
+    REAL *src = p0, *dst = p1;                                                 \
+    for (int it = 0; it < sweeps; it++) {                                      \
+      /* gosa with Neumaier compensation so the checker is accurate to a few  \
+         ulp whatever the summation order of the implementation under test */ \
+      double g = 0.0, gc = 0.0;                                                \
+      for (int k = 1; k < nz - 1; k++)                                         \
+        for (int j = 1; j < ny - 1; j++)                                       \
+          for (int i = 1; i < nx - 1; i++) {                                   \
+            int64_t o = IDX3(i, j, k, nx, ny);                                 \
+            REAL s0 = a0[o] * HP(i, j, k + 1) + a1[o] * HP(i, j + 1, k) +      \
+                      a2[o] * HP(i + 1, j, k) +                                \
+                      b0[o] * (HP(i, j + 1, k + 1) - HP(i, j - 1, k + 1) -     \
+                               HP(i, j + 1, k - 1) + HP(i, j - 1, k - 1)) +    \
+                      b1[o] * (HP(i + 1, j + 1, k) - HP(i + 1, j - 1, k) -     \
+                               HP(i - 1, j + 1, k) + HP(i - 1, j - 1, k)) +    \
+                      b2[o] * (HP(i + 1, j, k + 1) - HP(i + 1, j, k - 1) -     \
+                               HP(i - 1, j, k + 1) + HP(i - 1, j, k - 1)) +    \
+                      c0[o] * HP(i, j, k - 1) + c1[o] * HP(i, j - 1, k) +      \
+                      c2[o] * HP(i - 1, j, k) + wrk1[o];                       \
+            REAL ss = (s0 * a3[o] - HP(i, j, k)) * bnd[o];                     \
+            REAL v = HP(i, j, k) + omega * ss;                                 \
+            dst[o] = v;                                                        \
+            double q = (double)ss * (double)ss;                                \
+            double t = g + q;                                                  \
+            if (fabs(g) >= fabs(q)) gc += (g - t) + q; else gc += (q - t) + g; \
+            g = t;                                                             \
+          }                                                                    \
+      if (gosa) gosa[it] = g + gc;                                             \
+      REAL *t = src;                                                           \
+      src = dst;                                                               \
+      dst = t;                                                                 \
+    }                                                                          \
+    /* After an even number of sweeps the result is back in p0 (as in the    \
+       reference's PSStencilRun(map(p0->p1), map(p1->p0), nn/2)). */         \
   }
-#undef P
-  /* After an even number of sweeps the result is back in p0 (as in the
-     reference's PSStencilRun(map(p0->p1), map(p1->p0), nn/2)). */
-}
+#define HP(i, j, k) src[IDX3(i, j, k, nx, ny)]
+DEFINE_HIMENO(orc_himeno_f32, float)
+DEFINE_HIMENO(orc_himeno_f64, double)
+#undef HP
 
 /* ------------------------------------------------------------------------ */
 /* Generic flat linear stencil (the descriptor of physis_b200.h).            */

@@ -247,6 +247,8 @@ def _load():
         "psb_batch_member_result": (S, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                         ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_int)]),
+        "psb_set_fp_mode": (S, [ctypes.c_int]),
+        "psb_get_fp_mode": (S, [ctypes.POINTER(ctypes.c_int)]),
         "psb_batch_member_layout": (S, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchLayout)]),
         "psb_server_create": (S, [ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
         "psb_server_submit": (S, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]),
@@ -578,6 +580,21 @@ def reduce64(op, g, dom=None):
 
 def set_impl(impl):
     check(lib.psb_set_impl(impl), "psb_set_impl")
+
+
+FP_EXACT, FP_FMA = 0, 1
+
+
+def set_fp_mode(mode):
+    """Arithmetic of the 7-point TMA kernels: FP_EXACT (the reference's
+    roundings, default) or FP_FMA (fused multiply-adds, within 4 ulp)."""
+    check(lib.psb_set_fp_mode(mode), "psb_set_fp_mode")
+
+
+def get_fp_mode():
+    m = ctypes.c_int()
+    check(lib.psb_get_fp_mode(ctypes.byref(m)), "psb_get_fp_mode")
+    return m.value
 
 
 def set_graph(enable):

@@ -115,6 +115,7 @@ struct Runtime {
   psb_status last_status = PSB_OK;
   char last_error[256] = {0};  // text of the last CUDA failure
   int impl = PSB_IMPL_AUTO;
+  int fp_mode = PSB_FP_EXACT;
   bool use_graph = true;
   double last_ms = 0.0;
   int64_t last_launches = 0;

@@ -63,8 +63,14 @@ __global__ void __launch_bounds__(256) k_diff7_plain(GridView in, GridView out, 
   }
 }
 
-template <typename T, bool PERIODIC>
-__global__ void __launch_bounds__(544) k_diff7_tma(const __grid_constant__ CUtensorMap tin,
+#ifndef PSB_D7_MAXT
+#define PSB_D7_MAXT 544
+#endif
+#ifndef PSB_D7_MINB
+#define PSB_D7_MINB 1
+#endif
+template <typename T, bool PERIODIC, bool FAST>
+__global__ void __launch_bounds__(PSB_D7_MAXT, PSB_D7_MINB) k_diff7_tma(const __grid_constant__ CUtensorMap tin,
                                                    GridView out, int nx, int ny, int nz, Dom3 d,
                                                    C7<T> k, TmaGeom geo, int images, int *err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -76,8 +82,8 @@ __global__ void __launch_bounds__(544) k_diff7_tma(const __grid_constant__ CUten
   b /= geo.tiles_x;
   const int tile_y = b % geo.tiles_y;
   const int zc = b / geo.tiles_y;
-  diff7_tile<T, PERIODIC, false>(&tin, out, nx, ny, nz, d, k, geo, tile_x, tile_y, zc, images,
-                                 err, smem, nullptr);
+  diff7_tile<T, PERIODIC, false, FAST>(&tin, out, nx, ny, nz, d, k, geo, tile_x, tile_y, zc,
+                                       images, err, smem, nullptr);
 }
 
 // --------------------------------------------------------------------------
@@ -122,7 +128,7 @@ static psb_status launch_plain(MapImpl &m, cudaStream_t s, int64_t *launches) {
   return PSB_OK;
 }
 
-template <typename T, bool PERIODIC>
+template <typename T, bool PERIODIC, bool FAST>
 static psb_status launch_tma(MapImpl &m, const psb_tune_config &cfg, cudaStream_t s,
                              int64_t *launches) {
   constexpr int V = 16 / sizeof(T);
@@ -153,9 +159,9 @@ static psb_status launch_tma(MapImpl &m, const psb_tune_config &cfg, cudaStream_
   geo.stages = std::min(std::max(3, cfg.stages), 32);
   geo.stage_bytes = (geo.bx * geo.by * (int)sizeof(T) + 127) / 128 * 128;
   size_t smem = 128 + 512 + (size_t)geo.stages * geo.stage_bytes;
-  auto kern = k_diff7_tma<T, PERIODIC>;
-  static size_t configured[2][2] = {{0, 0}, {0, 0}};
-  size_t &conf = configured[sizeof(T) == 8][PERIODIC];
+  auto kern = k_diff7_tma<T, PERIODIC, FAST>;
+  static size_t configured[2][2][2] = {};
+  size_t &conf = configured[sizeof(T) == 8][PERIODIC][FAST];
   if (conf == 0) {
     // Prefer the largest shared-memory carve-out: several CTAs' rings then
     // fit on one SM, which keeps more planes in flight.
@@ -314,10 +320,20 @@ psb_status diffusion7_launch(MapImpl &m, const psb_tune_config &cfg, cudaStream_
       if (gi->pub.dim[i] < gi->halo) tma = false;
   }
   if (tma) {
-    psb_status st = dbl ? (periodic ? launch_tma<double, true>(m, cfg, s, launches)
-                                    : launch_tma<double, false>(m, cfg, s, launches))
-                        : (periodic ? launch_tma<float, true>(m, cfg, s, launches)
-                                    : launch_tma<float, false>(m, cfg, s, launches));
+    // The contracted (FMA) arithmetic is a runtime choice (psb_set_fp_mode)
+    // of the TMA kernels; the plain kernel always keeps the reference's.
+    const bool fast = rt().fp_mode == PSB_FP_FMA;
+    psb_status st;
+    if (fast)
+      st = dbl ? (periodic ? launch_tma<double, true, true>(m, cfg, s, launches)
+                           : launch_tma<double, false, true>(m, cfg, s, launches))
+               : (periodic ? launch_tma<float, true, true>(m, cfg, s, launches)
+                           : launch_tma<float, false, true>(m, cfg, s, launches));
+    else
+      st = dbl ? (periodic ? launch_tma<double, true, false>(m, cfg, s, launches)
+                           : launch_tma<double, false, false>(m, cfg, s, launches))
+               : (periodic ? launch_tma<float, true, false>(m, cfg, s, launches)
+                           : launch_tma<float, false, false>(m, cfg, s, launches));
     if (st != PSB_ERR_UNSUPPORTED) return st;
   }
   return dbl ? (periodic ? launch_plain<double, true>(m, s, launches)

@@ -11,15 +11,34 @@ struct C7 {
   T ce, cw, cn, cs, ct, cb, cc;
 };
 
-template <typename T>
+// FAST = false: the reference's roundings (every product and sum rounded).
+// FAST = true: the contracted form of the same term order -- the first
+// product rounded, then each further term added by one fused multiply-add
+// (one rounding per term instead of two). It is no longer bit-identical to
+// the reference CPU target; on the C2 field and on random inputs in [0, 1)
+// one step differs from it by at most 4 ulp, and its error against an FP64
+// evaluation is no larger than the exact form's.
+__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+template <typename T, bool FAST = false>
 __device__ __forceinline__ T diff7_point(const C7<T> &k, T c, T w, T e, T n, T s, T b, T t) {
   T v = xmul(k.cc, c);
-  v = xadd(v, xmul(k.cw, w));
-  v = xadd(v, xmul(k.ce, e));
-  v = xadd(v, xmul(k.cs, s));
-  v = xadd(v, xmul(k.cn, n));
-  v = xadd(v, xmul(k.cb, b));
-  v = xadd(v, xmul(k.ct, t));
+  if constexpr (FAST) {
+    v = xfma(k.cw, w, v);
+    v = xfma(k.ce, e, v);
+    v = xfma(k.cs, s, v);
+    v = xfma(k.cn, n, v);
+    v = xfma(k.cb, b, v);
+    v = xfma(k.ct, t, v);
+  } else {
+    v = xadd(v, xmul(k.cw, w));
+    v = xadd(v, xmul(k.ce, e));
+    v = xadd(v, xmul(k.cs, s));
+    v = xadd(v, xmul(k.cn, n));
+    v = xadd(v, xmul(k.cb, b));
+    v = xadd(v, xmul(k.ct, t));
+  }
   return v;
 }
 
@@ -72,12 +91,63 @@ __device__ __forceinline__ void mul4(float2 k, const Vec16<float> &x, float *p) 
   p[3] = hi.y;
 }
 
-template <typename T>
+// Contracted row (FAST): pairs of points with the packed sm_100 f32x2
+// multiply and fused multiply-add, in the term order of diff7_point<FAST>;
+// the w and e operands of each pair are the row's own elements shifted by
+// one (wl and er at the ends), with the clamped x faces selected first.
+__device__ __forceinline__ Vec16<float> diff7_row_fast(const K7<float> &k, const Vec16<float> &c,
+                                                       float wl, float er, const Vec16<float> &n,
+                                                       const Vec16<float> &s,
+                                                       const Vec16<float> &b,
+                                                       const Vec16<float> &t, unsigned xfix) {
+  float w0 = wl, e0 = c.v[1], e1 = c.v[2], e2 = c.v[3], e3 = er;
+  if (xfix) {
+    if (xfix & 16u) w0 = c.v[0];
+    if (xfix & 1u) e0 = c.v[0];
+    if (xfix & 2u) e1 = c.v[1];
+    if (xfix & 4u) e2 = c.v[2];
+    if (xfix & 8u) e3 = c.v[3];
+  }
+  float2 lo = __fmul2_rn(k.cc, make_float2(c.v[0], c.v[1]));
+  float2 hi = __fmul2_rn(k.cc, make_float2(c.v[2], c.v[3]));
+  lo = __ffma2_rn(k.cw, make_float2(w0, c.v[0]), lo);
+  hi = __ffma2_rn(k.cw, make_float2(c.v[1], c.v[2]), hi);
+  lo = __ffma2_rn(k.ce, make_float2(e0, e1), lo);
+  hi = __ffma2_rn(k.ce, make_float2(e2, e3), hi);
+  lo = __ffma2_rn(k.cs, make_float2(s.v[0], s.v[1]), lo);
+  hi = __ffma2_rn(k.cs, make_float2(s.v[2], s.v[3]), hi);
+  lo = __ffma2_rn(k.cn, make_float2(n.v[0], n.v[1]), lo);
+  hi = __ffma2_rn(k.cn, make_float2(n.v[2], n.v[3]), hi);
+  lo = __ffma2_rn(k.cb, make_float2(b.v[0], b.v[1]), lo);
+  hi = __ffma2_rn(k.cb, make_float2(b.v[2], b.v[3]), hi);
+  lo = __ffma2_rn(k.ct, make_float2(t.v[0], t.v[1]), lo);
+  hi = __ffma2_rn(k.ct, make_float2(t.v[2], t.v[3]), hi);
+  Vec16<float> r;
+  r.v[0] = lo.x;
+  r.v[1] = lo.y;
+  r.v[2] = hi.x;
+  r.v[3] = hi.y;
+  return r;
+}
+
+template <typename T, bool FAST = false>
 __device__ __forceinline__ Vec16<T> diff7_row(const K7<T> &k, const Vec16<T> &c, T wl, T er,
                                               const Vec16<T> &n, const Vec16<T> &s,
                                               const Vec16<T> &b, const Vec16<T> &t,
                                               unsigned xfix) {
   constexpr int V = Vec16<T>::N;
+  if constexpr (FAST && sizeof(T) == 4) {
+    return diff7_row_fast(k, c, wl, er, n, s, b, t, xfix);
+  } else if constexpr (FAST) {
+    Vec16<T> r;
+#pragma unroll
+    for (int v = 0; v < V; v++) {
+      T w = v == 0 ? ((xfix & 16u) ? c.v[0] : wl) : c.v[v - 1];
+      T e = (xfix & (1u << v)) ? c.v[v] : (v == V - 1 ? er : c.v[v + 1]);
+      r.v[v] = diff7_point<T, true>(k.s, c.v[v], w, e, n.v[v], s.v[v], b.v[v], t.v[v]);
+    }
+    return r;
+  }
   T pcc[V], pcw[V], pce[V], ps[V], pn[V], pb[V], pt[V];
   if constexpr (sizeof(T) == 4) {
     mul4(k.cc, c, pcc);
@@ -163,7 +233,7 @@ struct TileAcc {
 // (depth 1, one per face it lies on), which keeps the resident halo current
 // for the next periodic read. With ACC the convergence terms are added to
 // *acc. Returns false (warp-uniformly) if a bounded wait gave up.
-template <typename T, bool PERIODIC, bool ACC>
+template <typename T, bool PERIODIC, bool ACC, bool FAST = false>
 __device__ __forceinline__ bool diff7_consume(const Ring &R, RingPos &p, const GridView out,
                                               int nx, int ny, int nz, const Dom3 d,
                                               const C7<T> k, const TmaGeom geo, int x0, int y0,
@@ -261,8 +331,8 @@ __device__ __forceinline__ bool diff7_consume(const Ring &R, RingPos &p, const G
     if (!(yedge || zedge)) {
 #pragma unroll
       for (int r = 0; r < VY; r++)
-        res[r] = diff7_row(kk, vc[r], wl[r], er[r], r == 0 ? vn : vc[r - 1],
-                           r == VY - 1 ? vs : vc[r + 1], vb[r], vt[r], xfix);
+        res[r] = diff7_row<T, FAST>(kk, vc[r], wl[r], er[r], r == 0 ? vn : vc[r - 1],
+                                    r == VY - 1 ? vs : vc[r + 1], vb[r], vt[r], xfix);
     } else {
 #pragma unroll
       for (int r = 0; r < VY; r++) {
@@ -282,7 +352,7 @@ __device__ __forceinline__ bool diff7_consume(const Ring &R, RingPos &p, const G
           if (y == ny - 1) s = c;
           if (z == 0) bb = c;
           if (z == nz - 1) t = c;
-          res[r].v[v] = diff7_point(k, c, w, e, n, s, bb, t);
+          res[r].v[v] = diff7_point<T, FAST>(k, c, w, e, n, s, bb, t);
         }
       }
     }
@@ -562,7 +632,7 @@ __device__ __forceinline__ bool diff7_tb_stage1(const Ring &R1, RingPos &p1, con
 // (tile_x, tile_y) of the domain over z chunk zc, read through tensor map
 // `tin`, written to `out`. Called by every thread of the CTA; `smem` is the
 // CTA's 128-byte aligned dynamic shared memory (barriers + ring).
-template <typename T, bool PERIODIC, bool ACC>
+template <typename T, bool PERIODIC, bool ACC, bool FAST = false>
 __device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridView out, int nx,
                                            int ny, int nz, const Dom3 d, const C7<T> k,
                                            const TmaGeom geo, int tile_x, int tile_y, int zc,
@@ -597,8 +667,8 @@ __device__ __forceinline__ void diff7_tile(const CUtensorMap *tin, const GridVie
     }
     return;
   }
-  if (!diff7_consume<T, PERIODIC, ACC>(R, pos, out, nx, ny, nz, d, k, geo, x0, y0, zb, nzl,
-                                       images, acc) &&
+  if (!diff7_consume<T, PERIODIC, ACC, FAST>(R, pos, out, nx, ny, nz, d, k, geo, x0, y0, zb, nzl,
+                                             images, acc) &&
       (tid & 31) == 0)
     atomicExch(err, 1);
 }

@@ -727,6 +727,21 @@ psb_status psb_set_impl(int impl) {
   return PSB_OK;
 }
 
+psb_status psb_set_fp_mode(int mode) {
+  if (mode != PSB_FP_EXACT && mode != PSB_FP_FMA) return set_status(PSB_ERR_INVALID);
+  PSB_CHECK(ensure_init());
+  rt().fp_mode = mode;
+  drop_graphs();
+  return PSB_OK;
+}
+
+psb_status psb_get_fp_mode(int *mode) {
+  if (!mode) return set_status(PSB_ERR_INVALID);
+  PSB_CHECK(ensure_init());
+  *mode = rt().fp_mode;
+  return PSB_OK;
+}
+
 psb_status psb_set_graph(int enable) {
   PSB_CHECK(ensure_init());
   rt().use_graph = enable != 0;

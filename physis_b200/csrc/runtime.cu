@@ -106,6 +106,8 @@ psb_status ensure_init() {
     else if (!strcmp(impl, "tma")) r.impl = PSB_IMPL_TMA;
     else if (!strcmp(impl, "generic")) r.impl = PSB_IMPL_GENERIC;
   }
+  const char *fp = getenv("PHYSIS_B200_FP_MODE");
+  if (fp && !strcmp(fp, "fma")) r.fp_mode = PSB_FP_FMA;
   const char *graph = getenv("PHYSIS_B200_GRAPH");
   if (graph) r.use_graph = atoi(graph) != 0;
   r.inited = true;
