@@ -452,6 +452,14 @@ psb_status psb_grid_copy(__PSGrid *dst, const __PSGrid *src);
 
 /* Register a generic stencil; *kernel_id is usable with PSStencilMap. */
 psb_status psb_generic_register(const psb_generic_stencil *desc, int *kernel_id);
+/* Which kernel ran the last application of a generic stencil (no
+ * counterpart in the reference): PSB_IMPL_TMA for the TMA z-streaming
+ * kernel (3-D, float or double, every grid read of the accumulation type
+ * with offsets within +-2, at most four grids read, not in place, not
+ * red-black), PSB_IMPL_GENERIC for the thread-per-point kernel, which runs
+ * every other form and every map under psb_set_impl(PSB_IMPL_PLAIN or
+ * PSB_IMPL_GENERIC). */
+psb_status psb_generic_last_impl(int *impl);
 
 /* Compiled stencils: a DSL stencil function (docs/programming.md:117-190 of
  * the reference: `const int` index parameters, grids, scalars;

@@ -200,6 +200,9 @@ psb_status himeno_launch(MapImpl &m, const psb_tune_config &cfg, cudaStream_t s,
 // launch (temporal blocking): reads in, writes out.
 psb_status diffusion7_tb2_launch(MapImpl &m, GridImpl *in, GridImpl *out, int zchunk,
                                  cudaStream_t s, int64_t *launches);
+psb_status generic_tma_launch(MapImpl &m, const GenericDesc &gd, int color, cudaStream_t s,
+                              int64_t *launches);
+void generic_note_impl(int impl);
 psb_status generic_launch(MapImpl &m, const GenericDesc &d, int color, cudaStream_t s,
                           int64_t *launches);
 psb_status reduce_view(const GridView &v, int type, int op, const Dom3 &dom, double *result,

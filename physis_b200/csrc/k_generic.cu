@@ -80,6 +80,13 @@ psb_status generic_upload(GenericDesc &d) {
 
 psb_status generic_launch(MapImpl &m, const GenericDesc &gd, int color, cudaStream_t s,
                           int64_t *launches) {
+  // The TMA z-streaming kernel takes every map it can (k_generic_tma.cu);
+  // PSB_IMPL_PLAIN and PSB_IMPL_GENERIC keep the thread-per-point kernel.
+  if (rt().impl != PSB_IMPL_PLAIN && rt().impl != PSB_IMPL_GENERIC) {
+    const psb_status st = generic_tma_launch(m, gd, color, s, launches);
+    if (st != PSB_ERR_UNSUPPORTED) return st;
+  }
+  generic_note_impl(PSB_IMPL_GENERIC);
   const psb_generic_stencil &desc = gd.host;
   GenGrids G;
   for (int i = 0; i < desc.ngrids; i++) {
