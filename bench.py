@@ -40,6 +40,9 @@ WORKLOADS = {
     "c2f64": ("diffusion7", np.float64, (256, 256, 256), 1000, 16),
     "c3": ("himeno", np.float32, (257, 257, 513), 200, 56),
     "c1": ("diffusion7", np.float32, (64, 64, 64), 100, 8),
+    # a user stencil through the generic term table: the 27-point box
+    # average (each neighbour times 1/27), interior of 512^3
+    "g27": ("generic27", np.float32, (512, 512, 512), 100, 8),
     # batched: 256 members, see c4_members(); dims/steps are per member
     "c4": ("batch", np.float32, (0, 0, 0), 0, 0),
     # served: a Poisson trace of solve requests, see c5_trace()
@@ -61,6 +64,10 @@ def describe(wl):
     if k == "himeno":
         return ("19-point Himeno Jacobi %dx%dx%d fp32, %d sweeps per solve, FP64 residual fused "
                 "per sweep" % (dims + (steps,)))
+    if k == "generic27":
+        return ("generic (user) stencil: 27-point box average sum_{d in {-1,0,1}^3} (1/27)*u(p+d) "
+                "as a psb_generic_stencil term table, %dx%dx%d fp32 interior [1,n-1)^3, %d time "
+                "steps per solve (double-buffered PSStencilRun)" % (dims + (steps,)))
     return ("7-point diffusion %dx%dx%d %s, %d time steps per solve (double-buffered "
             "PSStencilRun), clamped faces" % (dims + ("fp32" if dt == np.float32 else "fp64", steps)))
 
@@ -232,6 +239,22 @@ def cpu_baseline_sample(wl, field=None):
             secs = time.perf_counter() - t0
         pts = (nx - 2) * (ny - 2) * (nz - 2) * sweeps
         sample = "%dx%dx%d, %d sweeps" % (nx, ny, nz, sweeps)
+    elif k == "generic27":
+        f = field if field is not None else c2_field(dims, dt)
+        count = 2
+        c = float(np.float32(1.0 / 27.0))
+        if use_ref:
+            _, secs = oracle.ref_box27(f, count, c)
+        else:
+            from physis_b200.workloads import box27_struct
+            import physis_b200 as ps
+            w = [f.copy(), f.copy()]
+            t0 = time.perf_counter()
+            oracle.generic_apply(box27_struct(ps.PS_FLOAT), w, [1, 1, 1],
+                                 [nx - 1, ny - 1, nz - 1])
+            secs = (time.perf_counter() - t0) * count
+        pts = (nx - 2) * (ny - 2) * (nz - 2) * count
+        sample = "%dx%dx%d, %d time steps of the 27-point box average" % (nx, ny, nz, count)
     else:
         f = field if field is not None else c2_field(dims, dt)
         count = 12 if nx * ny * nz >= 1 << 26 else 100
@@ -356,6 +379,46 @@ def numerics_himeno(ps, dims, tsteps, grids, m1, m2, p, coef):
     return out
 
 
+def generic27_stencil(ps, accum=None):
+    from physis_b200.workloads import box27_stencil
+    return box27_stencil(accum if accum is not None else ps.PS_FLOAT)
+
+
+def numerics_generic27(ps, dt, n=96, steps=10):
+    """The generic 27-point path at n^3 for `steps` steps against the oracle
+    port (bit-exact check) and the FP64 oracle (the same term table
+    evaluated in double by the port)."""
+    from oracle import oracle
+    from physis_b200.workloads import box27_stencil, box27_struct
+    f = c2_field((n, n, n), dt)
+    st = box27_stencil(ps.PS_FLOAT)
+    g = [ps.grid_new(ps.PS_FLOAT, (n, n, n)) for _ in range(2)]
+    for x in g:
+        ps.PSGridCopyin(x, f)
+    d = ps.PSDomain3DNew(1, n - 1, 1, n - 1, 1, n - 1)
+    a = ps.PSStencilMap(st.kernel_id, d, g[0], g[1])
+    b = ps.PSStencilMap(st.kernel_id, d, g[1], g[0])
+    ps.PSStencilRun(a, b, steps // 2)
+    got = ps.PSGridCopyout(g[0])
+    for x in g:
+        ps.PSGridFree(x)
+    want = [f.copy(), f.copy()]
+    ref = [f.astype(np.float64), f.astype(np.float64)]
+    s32, s64 = box27_struct(ps.PS_FLOAT), box27_struct(ps.PS_DOUBLE)
+    for i in range(steps):
+        src, dst = (0, 1) if i % 2 == 0 else (1, 0)
+        oracle.generic_apply(s32, [want[src], want[dst]], [1, 1, 1], [n - 1] * 3)
+        oracle.generic_apply(s64, [ref[src], ref[dst]], [1, 1, 1], [n - 1] * 3)
+    out = {"vs": "FP64 oracle (the same term table evaluated in double by the oracle port); "
+                 "bit_exact_vs_reference: equality with the oracle port's float evaluation "
+                 "(the reference CPU target's arithmetic)",
+           "sample": "%d^3, %d steps of the same stencil and field formula" % (n, steps),
+           "bit_exact_vs_reference": bool(np.array_equal(got.view(np.uint8),
+                                                         want[0].view(np.uint8)))}
+    out.update(oracle.error_norms(got, ref[0]))
+    return out
+
+
 def run_ours(args):
     dist = Dist(args.gpus)
     os.environ["PHYSIS_B200_DEVICE"] = str(dist.local)
@@ -366,9 +429,12 @@ def run_ours(args):
     nx, ny, nz = dims
     ptype = ps.PS_FLOAT if dt == np.float32 else ps.PS_DOUBLE
     kernel = ps.HIMENO19 if kname == "himeno" else ps.DIFFUSION7
-    tune = ps.autotune(kernel, ptype, dims) if args.tune else ps.tune_get(kernel, ptype, dims)
+    tune = None
+    if kname != "generic27":
+        tune = ps.autotune(kernel, ptype, dims) if args.tune else ps.tune_get(kernel, ptype, dims)
     if args.plain:
-        ps.set_impl(ps.IMPL_PLAIN)
+        # the thread-per-point shape of the reference's generated kernels
+        ps.set_impl(ps.IMPL_GENERIC if kname == "generic27" else ps.IMPL_PLAIN)
     ps.set_fp_mode(ps.FP_FMA if args.fp_mode == "fma" else ps.FP_EXACT)
 
     # Inputs, pinned host buffers for the end-to-end leg.
@@ -388,6 +454,17 @@ def run_ours(args):
             ps.himeno_residual_enable(m2, tsteps)
         pts_per_step = (nx - 2) * (ny - 2) * (nz - 2) * tsteps
         g_io = grids[0]
+    elif kname == "generic27":
+        host = c2_field(dims, dt)
+        grids = [ps.grid_new(ptype, dims), ps.grid_new(ptype, dims)]
+        ps.PSGridCopyin(grids[0], host)
+        ps.PSGridCopyin(grids[1], host)  # the boundary cells stay as they are
+        g27 = generic27_stencil(ps)
+        dom = ps.PSDomain3DNew(1, nx - 1, 1, ny - 1, 1, nz - 1)
+        m1 = ps.PSStencilMap(g27.kernel_id, dom, grids[0], grids[1])
+        m2 = ps.PSStencilMap(g27.kernel_id, dom, grids[1], grids[0])
+        pts_per_step = (nx - 2) * (ny - 2) * (nz - 2) * tsteps
+        g_io = grids[0]
     else:
         host = c2_field(dims, dt)
         grids = [ps.grid_new(ptype, dims), ps.grid_new(ptype, dims)]
@@ -403,7 +480,7 @@ def run_ours(args):
         return ps.last_run_stats()
 
     # ---- device-resident timing ------------------------------------------
-    mass0 = ps.reduce64(ps.PS_SUM, g_io) if kname != "himeno" else None
+    mass0 = ps.reduce64(ps.PS_SUM, g_io) if kname == "diffusion7" else None
     for _ in range(args.warmup):
         solve()
     ps.sync()
@@ -421,7 +498,14 @@ def run_ours(args):
     wall = time.perf_counter() - t0
     clocks = sampler.stop()
     dist.barrier()
-    mass1 = ps.reduce64(ps.PS_SUM, g_io) if kname != "himeno" else None
+    mass1 = ps.reduce64(ps.PS_SUM, g_io) if kname == "diffusion7" else None
+    gimpl = None
+    if kname == "generic27":
+        import ctypes
+        v = ctypes.c_int()
+        ps.check(ps.lib.psb_generic_last_impl(ctypes.byref(v)), "psb_generic_last_impl")
+        gimpl = {ps.IMPL_TMA: "k_generic_tma (TMA z-streaming)",
+                 ps.IMPL_GENERIC: "k_generic (thread per point)"}.get(v.value, str(v.value))
     dev_s = sum(ms_list) / 1e3
     dev_s_max = dist.max(dev_s)
     total_pts = dist.sum(pts_per_step * args.steps)
@@ -430,7 +514,8 @@ def run_ours(args):
     alg_bytes = bpl * (pts_per_step / tsteps)
     hbm, peak_kind = peaks()
     achieved = alg_bytes / per_launch_s / 1e9
-    kname_traffic = "k_himeno_tma" if kname == "himeno" else (
+    kname_traffic = "k_himeno_tma" if kname == "himeno" else "k_generic_tma_f32" if \
+        kname == "generic27" else (
         "k_diff7_tma_f32" if dt == np.float32 else "k_diff7_tma_f64")
     if args.plain:
         kname_traffic = kname_traffic.replace("tma", "plain")
@@ -464,12 +549,14 @@ def run_ours(args):
     if dist.rank == 0 and not args.no_numerics:
         if kname == "himeno":
             numerics = numerics_himeno(ps, dims, tsteps, grids, m1, m2, p, coef)
+        elif kname == "generic27":
+            numerics = numerics_generic27(ps, dt)
         else:
             numerics = numerics_diffusion(ps, dt, dims, tsteps, grids, m1, m2, host, mass0, mass1,
                                           (args.warmup + args.steps) * tsteps)
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(wl, host if kname != "himeno" else None)
+        cpu = cpu_baseline_sample(wl, host if kname in ("diffusion7", "generic27") else None)
 
     line = {
         "metric": "lattice_updates_per_s_" + wl,
@@ -496,6 +583,7 @@ def run_ours(args):
                         "fma: the reference's term order with fused multiply-adds (one rounding "
                         "per term; within 4 ulp of the reference per step)"),
             "tune": tune,
+            "generic_kernel": gimpl,
             "hbm_gbs_effective": value * bpl,
             "wall_s_timed": wall,
         },
@@ -536,6 +624,11 @@ def _ref_worker(args):
     if kind == "himeno":
         p, coef = himeno_fields(dims, seed)
         _, secs = oracle.ref_himeno(p, coef, 0.8, count)
+        nx, ny, nz = dims
+        return (nx - 2) * (ny - 2) * (nz - 2) * count, secs
+    if kind == "generic27":
+        f = c2_field(dims, dt, seed)
+        _, secs = oracle.ref_box27(f, count, float(np.float32(1.0 / 27.0)))
         nx, ny, nz = dims
         return (nx - 2) * (ny - 2) * (nz - 2) * count, secs
     f = c2_field(dims, dt, seed)

@@ -91,6 +91,8 @@ def ref():
             f.argtypes = [I, I, I, P, I, P, I]
         lib.refp_himeno_f32.restype = ctypes.c_double
         lib.refp_himeno_f32.argtypes = [I, I, I, P, P, ctypes.c_float, I]
+        lib.refp_box27_f32.restype = ctypes.c_double
+        lib.refp_box27_f32.argtypes = [I, I, I, P, I, ctypes.c_float]
         lib.refp_reduce_f32.restype = None
         lib.refp_reduce_f32.argtypes = [I, P, ctypes.c_int64, P]
         lib.refp_reduce_f64.restype = None
@@ -238,6 +240,15 @@ def ref_himeno(p, coef, omega, nn):
     nz, ny, nx = a.shape
     secs = ref().refp_himeno_f32(nx, ny, nz, _ptr(a), ctypes.cast(arr, ctypes.c_void_p),
                                  ctypes.c_float(omega), nn)
+    return a, secs
+
+
+def ref_box27(field, count, c):
+    """The reference CPU target running the 27-point box average (count
+    even double-buffered steps). Returns (field, run-loop seconds)."""
+    a = np.array(field, dtype=np.float32, copy=True, order="C")
+    nz, ny, nx = a.shape
+    secs = ref().refp_box27_f32(nx, ny, nz, _ptr(a), count, ctypes.c_float(c))
     return a, secs
 
 

@@ -208,6 +208,66 @@ double refp_himeno_f32(int nx, int ny, int nz, float *p, const float *const *coe
   return t1 - t0;
 }
 
+/* ---------------- 27-point box average (a user stencil) ---------------- */
+/* The stencil of tests/system_tests/test_cases/test_27-pt.c (neighbours in
+ * its order: z = -1, 0, 1, and in each plane the centre, then x+1, x-1,
+ * y+1 with its corners, y-1 with its corners), each neighbour weighted by
+ * c, in the ref target's lowered form; domain [1, n-1) per axis. */
+typedef struct {
+  __PSDomain dom;
+  __PSGrid *g1;
+  int g1_index;
+  __PSGrid *g2;
+  int g2_index;
+  float c;
+} __PSStencil_box27;
+
+#define B27(g, i, j, k) (((float *)(g)->p0)[__PSGridGetOffset3D((g), (i), (j), (k))])
+#define B27_PLANE(g, i, j, k, c)                                                          \
+  c * B27(g, i, j, k) + c * B27(g, i + 1, j, k) + c * B27(g, i - 1, j, k) +               \
+      c * B27(g, i, j + 1, k) + c * B27(g, i + 1, j + 1, k) + c * B27(g, i - 1, j + 1, k) + \
+      c * B27(g, i, j - 1, k) + c * B27(g, i + 1, j - 1, k) + c * B27(g, i - 1, j - 1, k)
+
+static inline void box27_kernel(int i, int j, int k, __PSGrid *g1, __PSGrid *g2, float c) {
+  B27(g2, i, j, k) = B27_PLANE(g1, i, j, k - 1, c) + B27_PLANE(g1, i, j, k, c) +
+                     B27_PLANE(g1, i, j, k + 1, c);
+}
+
+static void __PSStencilRun_kernel_box27(const __PSStencil_box27 *s) {
+  int i0, i1, i2;
+  for (i2 = s->dom.local_min[2]; i2 <= s->dom.local_max[2] - 1; i2++)
+    for (i1 = s->dom.local_min[1]; i1 <= s->dom.local_max[1] - 1; i1++)
+      for (i0 = s->dom.local_min[0]; i0 <= s->dom.local_max[0] - 1; i0++)
+        box27_kernel(i0, i1, i2, s->g1, s->g2, s->c);
+}
+
+/* count (even) double-buffered steps; both grids start as `field` (the
+ * boundary cells keep it). Returns run-loop seconds. */
+double refp_box27_f32(int nx, int ny, int nz, float *field, int count, float c) {
+  PSVectorInt dims = {nx, ny, nz};
+  __PSGrid *g1 = __PSGridNew(sizeof(float), 3, dims);
+  __PSGrid *g2 = __PSGridNew(sizeof(float), 3, dims);
+  PSGridCopyin(g1, field);
+  PSGridCopyin(g2, field);
+  PSDomain3D inner = PSDomain3DNew(1, nx - 1, 1, ny - 1, 1, nz - 1);
+  __PSStencil_box27 s0 = {inner, g1, 0, g2, 0, c};
+  __PSStencil_box27 s1 = s0;
+  s1.g1 = g2;
+  s1.g2 = g1;
+  double t0 = now_s();
+  for (int it = 0; it < count / 2; ++it) {
+    __PSStencilRun_kernel_box27(&s0);
+    __PSStencilRun_kernel_box27(&s1);
+  }
+  double t1 = now_s();
+  PSGridCopyout(g1, field);
+  PSGridFree(g1);
+  PSGridFree(g2);
+  free(g1);
+  free(g2);
+  return t1 - t0;
+}
+
 /* ---------------- PSReduce through the reference runtime ---------------- */
 void refp_reduce_f32(int op, const float *data, int64_t n, float *out) {
   PSVectorInt dims = {(int)n, 1, 1};

@@ -95,3 +95,31 @@ def himeno_gpu(p, coef, omega, sweeps, impl=ps.IMPL_AUTO, layout=ps.LAYOUT_PITCH
         for g in gs:
             ps.PSGridFree(g)
     return out, gosa
+
+
+def box27_offsets():
+    """The 27 neighbour offsets in the order of the reference's
+    tests/system_tests/test_cases/test_27-pt.c: z from -1 to 1, and in each
+    plane the centre, then its ring (x+1, x-1, y+1 and its corners, y-1 and
+    its corners)."""
+    ring = [(0, 0), (1, 0), (-1, 0), (0, 1), (1, 1), (-1, 1), (0, -1), (1, -1), (-1, -1)]
+    return [(dx, dy, dz) for dz in (-1, 0, 1) for dx, dy in ring]
+
+
+def box27_terms(accum=ps.PS_FLOAT):
+    """Terms of the 27-point box average: each neighbour times 1/27 (the
+    float value for a float stencil, so that its double evaluation starts
+    from the same coefficient)."""
+    c = float(np.float32(1.0 / 27.0))
+    return [(ps.const(c), ps.get(0, o)) for o in box27_offsets()]
+
+
+def box27_struct(accum=ps.PS_FLOAT):
+    """The 27-point box average as a psb_generic_stencil struct (unregistered:
+    slot 0 read, slot 1 written)."""
+    return ps.generic_struct(3, [(accum, (0, 1, 2))] * 2, 1, accum, box27_terms(accum))
+
+
+def box27_stencil(accum=ps.PS_FLOAT):
+    """The 27-point box average registered as a generic stencil."""
+    return ps.GenericStencil(3, [(accum, (0, 1, 2))] * 2, 1, accum, box27_terms(accum))
