@@ -824,6 +824,8 @@ def run_c4(args, dist):
         members = [m for m in members if m[0] == args.c4_kind]
     grids = c4_build(ps, members)
     b = c4_batch(ps, members, grids)
+    if args.tune:
+        b.autotune(force=True)  # tile shapes and z chunks per member size bucket, cached
     lups = sum(((d[0] - 2) * (d[1] - 2) * (d[2] - 2) if k == "him" else d[0] * d[1] * d[2]) * st
                for k, d, st in members)
     alg_bytes = sum(((d[0] - 2) * (d[1] - 2) * (d[2] - 2) * 56 if k == "him"
@@ -869,6 +871,10 @@ def run_c4(args, dist):
         "ms_per_step": per_run_s * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": describe("c4"), "step": "one run of the whole batch (256 solves)",
+                   "tiles": "per member size bucket from the batch autotuner's table "
+                            "(psb_batch_autotune; shipped entries in physis_b200/tune_b200.json) "
+                            "where it has an entry, else the fewest-tiles rule",
+                   "tuned_members": sum(1 for i in range(len(members)) if b.tuned(i)),
                    "members": len(members), "lattice_updates_per_run": lups,
                    "parallelism": "replicas (one batch per GPU)",
                    "inputs_vs_l2": "all members' grids (~18 GB) resident; each run streams "

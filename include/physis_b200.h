@@ -656,14 +656,26 @@ psb_status psb_batch_member_result(psb_batch *b, int member, int *steps_done, do
  * the reference, which has no batching): the points of an item in x and y,
  * its planes in z, the items of one step, and whether consecutive steps of
  * the member overlapped as a wavefront (1: an item waited only for the 27
- * items around it in the previous step; 0: for the whole previous step).
- * PSB_ERR_INVALID before the batch has run in mode 0 or 1. */
+ * items around it in the previous step; 0: for the whole previous step),
+ * and whether its tile shape came from the autotuner's table (1) or from
+ * the fewest-tiles rule (0). PSB_ERR_INVALID before the batch has run in
+ * mode 0 or 1. */
 typedef struct {
   int tile_x, tile_y, z_chunk;
   int tiles;
   int wavefront;
+  int tuned;
 } psb_batch_layout;
 psb_status psb_batch_member_layout(psb_batch *b, int member, psb_batch_layout *layout);
+/* Autotune the batch's members (the reference tunes by trial at translation
+ * time, translator/reference_translator.cc:749-1223): for each size bucket
+ * -- member kind, element type and extents rounded up to powers of two --
+ * without a cached entry (every bucket with force != 0), a scratch member
+ * of those extents is timed alone in the persistent kernel over candidate
+ * tile widths and z chunks; the fastest is cached in the tune table and its
+ * JSON file and used by later mode-0/1 runs for every member of the bucket
+ * (the members' own grids are not touched). */
+psb_status psb_batch_autotune(psb_batch *b, int force);
 psb_status psb_batch_free(psb_batch *b);
 
 /* ------------------------------------------------------------------------ */

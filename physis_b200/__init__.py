@@ -162,7 +162,7 @@ class Result(ctypes.Structure):
 class BatchLayout(ctypes.Structure):
     """psb_batch_layout."""
     _fields_ = [("tile_x", ctypes.c_int), ("tile_y", ctypes.c_int), ("z_chunk", ctypes.c_int),
-                ("tiles", ctypes.c_int), ("wavefront", ctypes.c_int)]
+                ("tiles", ctypes.c_int), ("wavefront", ctypes.c_int), ("tuned", ctypes.c_int)]
 
 
 # ---------------------------------------------------------------------------
@@ -250,6 +250,7 @@ def _load():
         "psb_set_fp_mode": (S, [ctypes.c_int]),
         "psb_get_fp_mode": (S, [ctypes.POINTER(ctypes.c_int)]),
         "psb_batch_member_layout": (S, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchLayout)]),
+        "psb_batch_autotune": (S, [ctypes.c_void_p, ctypes.c_int]),
         "psb_server_create": (S, [ctypes.c_size_t, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]),
         "psb_server_submit": (S, [ctypes.c_void_p, ctypes.POINTER(Request), ctypes.POINTER(ctypes.c_int64)]),
         "psb_server_cancel": (S, [ctypes.c_void_p, ctypes.c_int64]),
@@ -744,6 +745,11 @@ class Batch:
                                           ctypes.byref(which)), "psb_batch_member_result")
         return st.value, res.value, self.members[member][which.value]
 
+    def autotune(self, force=False):
+        """Tune the tile shape and z chunk of every member size bucket without
+        a cached entry (psb_batch_autotune)."""
+        check(lib.psb_batch_autotune(self.ptr, 1 if force else 0), "psb_batch_autotune")
+
     def layout(self, member):
         """How the last mode-0/1 run cut the member into items (dict of
         psb_batch_layout)."""
@@ -751,6 +757,10 @@ class Batch:
         check(lib.psb_batch_member_layout(self.ptr, member, ctypes.byref(lay)),
               "psb_batch_member_layout")
         return {k: getattr(lay, k) for k, _ in lay._fields_}
+
+    def tuned(self, member):
+        """Whether the member's tile shape came from the autotuner's table."""
+        return bool(self.layout(member)["tuned"])
 
     def free(self):
         if self.ptr:

@@ -36,6 +36,7 @@
 // decides, and only then releases the member's next step, so the decision is
 // deterministic and independent of the rest of the batch.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <numeric>
@@ -648,7 +649,38 @@ static psb_status dev_reserve(T **p, size_t *cap, size_t bytes) {
 // promotion is up to 14% faster on small Himeno members).
 static const int kPromoP = PSB_PROMO_P, kPromoC = PSB_PROMO_C, kPromoD = PSB_PROMO_D;
 
-static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int *ty_threads) {
+// Tile width and z-chunk preference of a member: forced by an autotuner
+// trial, else the tuned entry of its size bucket, else none (0: the rules
+// below decide).
+struct MemberTune {
+  int tx = 0;
+  int zc = 0;
+  bool forced = false;
+};
+
+static MemberTune member_tune(const BatchMemberHost &h) {
+  MemberTune t;
+  if (h.force_tx > 0 || h.force_zc > 0) {
+    t.tx = h.force_tx;
+    t.zc = h.force_zc;
+    t.forced = true;
+    return t;
+  }
+  psb_tune_config c;
+  if (batch_tune_find(h.kind, h.grids[0]->pub.dim, &c)) {
+    t.tx = c.tile_x / 4;
+    t.zc = c.z_chunk;
+  }
+  return t;
+}
+
+static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int *ty_threads,
+                       int force_t = 0) {
+  if (force_t >= kMinTx && force_t <= kMaxTx) {
+    *tx_threads = force_t;
+    *ty_threads = kBConsumers / force_t;
+    return;
+  }
   int64_t best_tiles = -1, best_box = 0;
   for (int t = kMinTx; t <= kMaxTx; t++) {
     const int TX = t * 4, TY = (kBConsumers / t) * rows_per_thread;
@@ -680,9 +712,16 @@ static int pick_zchunk(int64_t tiles_xy, int nz, int floor) {
   return floor;
 }
 
-static TmaGeom batch_dgeom(const GridImpl *g, int zc_floor) {
+// z chunk of a member: the trial's, else the longest chunk from the floor
+// (raised to the member's tuned chunk) that reaches the items target.
+static int member_zchunk(const MemberTune &mt, int64_t tiles_xy, int nz, int zc_floor) {
+  if (mt.forced && mt.zc > 0) return mt.zc;
+  return pick_zchunk(tiles_xy, nz, std::max(zc_floor, mt.zc));
+}
+
+static TmaGeom batch_dgeom(const GridImpl *g, int zc_floor, const MemberTune &mt) {
   TmaGeom geo;
-  pick_shape(g->pub.dim[0], g->pub.dim[1], kVY, &geo.tx_threads, &geo.ty_threads);
+  pick_shape(g->pub.dim[0], g->pub.dim[1], kVY, &geo.tx_threads, &geo.ty_threads, mt.tx);
   const int TX = geo.tx_threads * 4, TY = geo.ty_threads * kVY;
   geo.bx = TX + 8;
   geo.by = TY + 2;
@@ -692,16 +731,16 @@ static TmaGeom batch_dgeom(const GridImpl *g, int zc_floor) {
   geo.x_base = 0;
   geo.tiles_x = (g->pub.dim[0] + TX - 1) / TX;
   geo.tiles_y = (g->pub.dim[1] + TY - 1) / TY;
-  geo.zchunk = pick_zchunk((int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2], zc_floor);
+  geo.zchunk = member_zchunk(mt, (int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2], zc_floor);
   geo.stages = kBStages;
   geo.stage_bytes = kind_stage_bytes(0);
   return geo;
 }
 
-static HimenoGeom batch_hgeom(const GridImpl *g, int zc_floor) {
+static HimenoGeom batch_hgeom(const GridImpl *g, int zc_floor, const MemberTune &mt) {
   HimenoGeom geo;
   // interior domain [1, n-1): tiles start at x = 0 (x_base), y = 1.
-  pick_shape(g->pub.dim[0] - 1, g->pub.dim[1] - 2, 1, &geo.tx_threads, &geo.ty_threads);
+  pick_shape(g->pub.dim[0] - 1, g->pub.dim[1] - 2, 1, &geo.tx_threads, &geo.ty_threads, mt.tx);
   const int TX = geo.tx_threads * 4, TY = geo.ty_threads;
   geo.bx = TX + 8;
   geo.by = TY + 2;
@@ -711,7 +750,7 @@ static HimenoGeom batch_hgeom(const GridImpl *g, int zc_floor) {
   geo.x_base = 0;
   geo.tiles_x = (g->pub.dim[0] - 1 + TX - 1) / TX;
   geo.tiles_y = (g->pub.dim[1] - 2 + TY - 1) / TY;
-  geo.zchunk = pick_zchunk((int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2] - 2, zc_floor);
+  geo.zchunk = member_zchunk(mt, (int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2] - 2, zc_floor);
   geo.stages = kBStages;
   geo.stage_bytes = kind_stage_bytes(1);
   geo.nx = g->pub.dim[0];
@@ -732,6 +771,8 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
   b->members.assign(n, BMember());
   std::vector<CUtensorMap> tmaps(2 * std::max(1, n));
   std::vector<int> coef_map(n, -1);  // index of a Himeno member's 12 coefficient maps
+  std::vector<MemberTune> mt(n);
+  for (int i = 0; i < n; i++) mt[i] = member_tune(b->hm[i]);
   // The longest z chunk at which each kind's members together give
   // items_target() items per step (4 if none does).
   int zc_floor[2] = {4, 4};
@@ -742,10 +783,10 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
         if (steps[i] <= 0 || (b->hm[i].kind == BK_HIMENO) != (k == 1)) continue;
         const GridImpl *g0 = b->hm[i].grids[0];
         if (k == 1) {
-          const HimenoGeom hg = batch_hgeom(g0, 64);
+          const HimenoGeom hg = batch_hgeom(g0, 64, mt[i]);
           items += (int64_t)hg.tiles_x * hg.tiles_y * ((g0->pub.dim[2] - 2 + zc - 1) / zc);
         } else {
-          const TmaGeom dg = batch_dgeom(g0, 64);
+          const TmaGeom dg = batch_dgeom(g0, 64, mt[i]);
           items += (int64_t)dg.tiles_x * dg.tiles_y * ((g0->pub.dim[2] + zc - 1) / zc);
         }
       }
@@ -773,7 +814,7 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     M.sz = g0->sz;
     const CUtensorMap *a = nullptr, *c = nullptr;
     if (h.kind == BK_HIMENO) {
-      M.hg = batch_hgeom(g0, zc_floor[1]);
+      M.hg = batch_hgeom(g0, zc_floor[1], mt[i]);
       for (int k = 0; k < 3; k++) {
         M.dom.lo[k] = 1;
         M.dom.hi[k] = g0->pub.dim[k] - 1;
@@ -792,7 +833,7 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
         tmaps.push_back(*cm);
       }
     } else {
-      M.dg = batch_dgeom(g0, zc_floor[0]);
+      M.dg = batch_dgeom(g0, zc_floor[0], mt[i]);
       for (int k = 0; k < 3; k++) {
         M.dom.lo[k] = 0;
         M.dom.hi[k] = g0->pub.dim[k];
@@ -1255,6 +1296,122 @@ psb_status psb_batch_member_result(psb_batch *b, int member, int *steps_done, do
   return PSB_OK;
 }
 
+// Autotuner for batch members. For every size bucket (kind, element type,
+// extents rounded up to powers of two) among the members that has no
+// cached entry (or all of them, with force), a scratch member of the first
+// member's extents runs alone in the persistent kernel for kTuneSteps
+// steps under each candidate tile width and z chunk; the fastest (CUDA
+// events, best of two runs after a warm-up) goes into the tune table and
+// the cache file, where batch_prepare finds it for every member of that
+// bucket. The reference's counterpart is its translation-time trial of
+// optimisation variants (translator/reference_translator.cc:749-1223).
+constexpr int kTuneSteps = 8;
+
+static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *best_cfg) {
+  Runtime &r = rt();
+  const int ng = h.ngrids;
+  std::vector<__PSGrid *> gs(ng, nullptr);
+  psb_status st = PSB_OK;
+  for (int i = 0; i < ng && st == PSB_OK; i++)
+    st = psb_grid_new(PS_FLOAT, 3, h.grids[0]->pub.dim, PSB_LAYOUT_PITCHED, &gs[i]);
+  for (int i = 0; i < ng && st == PSB_OK; i++)
+    st = psb_grid_fill(gs[i], 0, 7 + i, h.kind == BK_HIMENO && i == 5 ? 0.15 : 0.0,
+                       h.kind == BK_HIMENO && i == 5 ? 0.18 : 1.0);
+  psb_batch *tb = batch_new();
+  BatchMemberHost t = h;
+  for (int i = 0; i < ng; i++) t.grids[i] = gs[i] ? as_impl(gs[i]) : nullptr;
+  t.steps = kTuneSteps;
+  t.check_every = 0;
+  t.tol = 0;
+  if (st == PSB_OK && h.kind == BK_DIFF7P)
+    st = launch_halo_fill(t.grids[0], PSB_BOUNDARY_PERIODIC, r.stream);
+  const int rows_per_thread = h.kind == BK_HIMENO ? 1 : kVY;
+  std::vector<int> txs = {8, 11, 16, 21, 32};
+  int heur_tx = 0, heur_ty = 0;
+  if (h.kind == BK_HIMENO)
+    pick_shape(h.grids[0]->pub.dim[0] - 1, h.grids[0]->pub.dim[1] - 2, 1, &heur_tx, &heur_ty);
+  else
+    pick_shape(h.grids[0]->pub.dim[0], h.grids[0]->pub.dim[1], kVY, &heur_tx, &heur_ty);
+  if (std::find(txs.begin(), txs.end(), heur_tx) == txs.end()) txs.push_back(heur_tx);
+  const int nz = h.grids[0]->pub.dim[2] - (h.kind == BK_HIMENO ? 2 : 0);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (st == PSB_OK && cudaEventCreate(&e0) != cudaSuccess) st = PSB_ERR_CUDA;
+  if (st == PSB_OK && cudaEventCreate(&e1) != cudaSuccess) st = PSB_ERR_CUDA;
+  double best = -1;
+  for (int tx : txs) {
+    for (int zc : {4, 8, 16, 32, 64}) {
+      if (st != PSB_OK) break;
+      if (zc > 2 * std::max(nz, 2)) continue;
+      t.force_tx = tx;
+      t.force_zc = zc;
+      batch_set_members(tb, {t}, {});
+      st = batch_prepare(tb, {kTuneSteps}, {0});
+      double ms_best = -1;
+      for (int rep = 0; rep < 3 && st == PSB_OK; rep++) {
+        int64_t launches = 0;
+        cudaEventRecord(e0, r.stream);
+        st = batch_launch_persistent(tb, r.stream, &launches);
+        cudaEventRecord(e1, r.stream);
+        if (st == PSB_OK && cudaEventSynchronize(e1) != cudaSuccess) st = PSB_ERR_CUDA;
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && (ms_best < 0 || ms < ms_best)) ms_best = ms;  // rep 0 warms up
+      }
+      if (__ps_trace)
+        fprintf(__ps_trace, "physis_b200: batch tune kind=%d tile=%dx%d zc=%d: %.4f ms\n", h.kind,
+                tx * 4, (kBConsumers / tx) * rows_per_thread, zc, ms_best);
+      if (st == PSB_OK && ms_best > 0 && (best < 0 || ms_best < best)) {
+        best = ms_best;
+        best_cfg->impl = PSB_IMPL_TMA;
+        best_cfg->tile_x = tx * 4;
+        best_cfg->tile_y = (kBConsumers / tx) * rows_per_thread;
+        best_cfg->z_chunk = zc;
+        best_cfg->stages = kBStages;
+        best_cfg->t_depth = 1;
+      }
+    }
+  }
+  batch_delete(tb);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  for (auto g : gs)
+    if (g) PSGridFree(g);
+  int err = 0;
+  cudaMemcpy(&err, r.d_error, sizeof(int), cudaMemcpyDeviceToHost);
+  if (err) {
+    cudaMemset(r.d_error, 0, sizeof(int));
+    return set_status(PSB_ERR_TIMEOUT);
+  }
+  if (st == PSB_OK && best < 0) st = PSB_ERR_UNSUPPORTED;
+  return st;
+}
+
+psb_status psb_batch_autotune(psb_batch *b, int force) {
+  if (!b) return set_status(PSB_ERR_INVALID);
+  PSB_CHECK(ensure_init());
+  Runtime &r = rt();
+  std::lock_guard<std::recursive_mutex> lk(r.mu);
+  legacy_join_in();
+  PSB_TRY(cudaStreamSynchronize(r.stream));
+  std::vector<std::array<int, 4>> done;
+  bool stored = false;
+  for (auto &h : b->hm) {
+    int bucket[3];
+    batch_tune_bucket(h.grids[0]->pub.dim, bucket);
+    std::array<int, 4> key = {h.kind, bucket[0], bucket[1], bucket[2]};
+    if (std::find(done.begin(), done.end(), key) != done.end()) continue;
+    done.push_back(key);
+    psb_tune_config cfg;
+    if (!force && batch_tune_find(h.kind, h.grids[0]->pub.dim, &cfg)) continue;
+    PSB_CHECK(batch_tune_member(h, &cfg));
+    batch_tune_store(h.kind, h.grids[0]->pub.dim, cfg);
+    stored = true;
+  }
+  if (stored) tune_save();
+  batch_invalidate(b);
+  return PSB_OK;
+}
+
 psb_status psb_batch_member_layout(psb_batch *b, int member, psb_batch_layout *layout) {
   if (!b || !layout || member < 0 || member >= (int)b->hm.size() || !b->built)
     return set_status(PSB_ERR_INVALID);
@@ -1265,6 +1422,8 @@ psb_status psb_batch_member_layout(psb_batch *b, int member, psb_batch_layout *l
   layout->z_chunk = him ? M.hg.zchunk : M.dg.zchunk;
   layout->tiles = M.ntiles;
   layout->wavefront = batch_member_wavefront(b, member) ? 1 : 0;
+  const MemberTune mt = member_tune(b->hm[member]);
+  layout->tuned = !mt.forced && mt.tx > 0 ? 1 : 0;
   return PSB_OK;
 }
 

@@ -20,6 +20,8 @@ struct BatchMemberHost {
   int check_every = 0;     // residual check interval (0: none)
   double tol = 0.0;        // relative residual tolerance (0: run all steps)
   int64_t points = 0;      // lattice updates per step
+  int force_tx = 0;        // autotuner trials: consumer threads along x (0: choose)
+  int force_zc = 0;        // autotuner trials: planes per item (0: choose)
 };
 
 }  // namespace psb

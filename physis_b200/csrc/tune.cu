@@ -134,6 +134,33 @@ static void save_cache() {
   rename(tmp.c_str(), path.c_str());
 }
 
+void batch_tune_bucket(const int *n, int *bucket) {
+  for (int i = 0; i < 3; i++) {
+    int b = 8;
+    while (b < n[i] && b < (1 << 30)) b <<= 1;
+    bucket[i] = b;
+  }
+}
+
+bool batch_tune_find(int kind, const int *n, psb_tune_config *cfg) {
+  load_cache();
+  int b[3];
+  batch_tune_bucket(n, b);
+  auto it = rt().tune.find(TuneKey{kBatchTuneBase + kind, PS_FLOAT, b[0], b[1], b[2]});
+  if (it == rt().tune.end()) return false;
+  *cfg = it->second;
+  return true;
+}
+
+void batch_tune_store(int kind, const int *n, const psb_tune_config &cfg) {
+  load_cache();
+  int b[3];
+  batch_tune_bucket(n, b);
+  rt().tune[TuneKey{kBatchTuneBase + kind, PS_FLOAT, b[0], b[1], b[2]}] = cfg;
+}
+
+void tune_save() { save_cache(); }
+
 psb_status tune_lookup(int kernel, int type, const int *n, psb_tune_config *cfg) {
   load_cache();
   TuneKey k{kernel, type, n[0], n[1], n[2]};

@@ -88,3 +88,74 @@ def test_tune_set_overrides_and_every_candidate_shape_runs():
     finally:
         ps.tune_set(ps.DIFFUSION7, ps.PS_FLOAT, dims, impl=ps.IMPL_PLAIN, tile_x=32, tile_y=16,
                     z_chunk=16, stages=6, t_depth=1)
+
+
+def _pow2(n):
+    b = 8
+    while b < n:
+        b <<= 1
+    return b
+
+
+def test_batch_autotune_caches_per_bucket_and_stays_bit_exact():
+    """psb_batch_autotune times candidate tile widths and z chunks for each
+    member size bucket on scratch grids, caches the winners (kernel id 100 +
+    member kind, extents rounded up to powers of two), and later runs use
+    them: each member's item shape is its bucket's entry and every result is
+    bit-exact against the oracle (the members' own grids were not touched)."""
+    from physis_b200.workloads import himeno_inputs
+    ps.PSInit()
+    spec = [("diff", (100, 90, 70), 6), ("diffp", (64, 48, 80), 5), ("him", (90, 66, 50), 4),
+            ("diff", (120, 70, 100), 3)]  # the last shares the first one's bucket
+    kinds = {"diff": (ps.DIFFUSION7, 0), "diffp": (ps.DIFFUSION7_PERIODIC, 1),
+             "him": (ps.HIMENO19, 2)}
+    data, grids = [], []
+    for i, (kind, dims, steps) in enumerate(spec):
+        nx, ny, nz = dims
+        if kind == "him":
+            p, coef = himeno_inputs((nz, ny, nx), 30 + i)
+            gs = [ps.grid_new(ps.PS_FLOAT, dims) for _ in range(14)]
+            ps.PSGridCopyin(gs[0], p)
+            ps.PSGridCopyin(gs[1], p)
+            for k in range(12):
+                ps.PSGridCopyin(gs[2 + k], coef[k])
+            data.append((p, coef))
+        else:
+            f = np.random.default_rng(30 + i).random((nz, ny, nx), dtype=np.float32)
+            gs = [ps.grid_new(ps.PS_FLOAT, dims) for _ in range(2)]
+            ps.PSGridCopyin(gs[0], f)
+            data.append((f, None))
+        grids.append(gs)
+    b = ps.Batch()
+    try:
+        for (kind, dims, steps), gs in zip(spec, grids):
+            b.add(kinds[kind][0], gs, [0.8] if kind == "him" else COEF, steps)
+        b.autotune(force=True)
+        with open(os.environ["PHYSIS_B200_TUNE_CACHE"]) as f:
+            entries = json.load(f)
+        tuned = {}
+        for e in entries:
+            if e["kernel"] >= 100:
+                tuned[(e["kernel"] - 100, tuple(e["n"]))] = e
+        b.run(0)
+        for i, (kind, dims, steps) in enumerate(spec):
+            key = (kinds[kind][1], tuple(_pow2(v) for v in dims))
+            assert key in tuned, key
+            e = tuned[key]
+            lay = b.layout(i)
+            assert (lay["tile_x"], lay["tile_y"]) == (e["tile_x"], e["tile_y"]), (lay, e)
+            assert lay["z_chunk"] >= e["z_chunk"] and lay["tuned"] == 1
+            done, _, g = b.result(i)
+            assert done == steps
+            f, coef = data[i]
+            if kind == "him":
+                want = oracle.himeno(f, coef, 0.8, steps)[0]
+            else:
+                want = oracle.diffusion7(f, steps, np.asarray(COEF, np.float32),
+                                         periodic=kind == "diffp")
+            assert U.bits_equal(ps.PSGridCopyout(g), want), (i, kind, lay)
+    finally:
+        b.free()
+        for gs in grids:
+            for g in gs:
+                ps.PSGridFree(g)
