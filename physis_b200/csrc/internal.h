@@ -200,6 +200,9 @@ psb_status himeno_launch(MapImpl &m, const psb_tune_config &cfg, cudaStream_t s,
 // launch (temporal blocking): reads in, writes out.
 psb_status diffusion7_tb2_launch(MapImpl &m, GridImpl *in, GridImpl *out, int zchunk,
                                  cudaStream_t s, int64_t *launches);
+bool himeno_tb2_pair(MapImpl **ms, int n);
+psb_status himeno_tb2_launch(MapImpl &m1, MapImpl &m2, GridImpl *in, GridImpl *out,
+                             int zchunk, cudaStream_t s, int64_t *launches);
 psb_status generic_tma_launch(MapImpl &m, const GenericDesc &gd, int color, cudaStream_t s,
                               int64_t *launches);
 void generic_note_impl(int impl);

@@ -200,11 +200,15 @@ static double time_config(MapImpl &m, const psb_tune_config &cfg, int reps) {
     cudaEventRecord(a, r.stream);
     for (int i = 0; i < reps; i++) {
       // Two-step (temporally blocked) candidates advance two steps per launch.
-      psb_status st =
-          m.kernel_id == PSB_KERNEL_HIMENO19 ? himeno_launch(m, cfg, r.stream, &launches)
-          : cfg.t_depth == 2 ? diffusion7_tb2_launch(m, m.grids[0], m.grids[1], cfg.z_chunk,
-                                                     r.stream, &launches)
-                             : diffusion7_launch(m, cfg, r.stream, &launches);
+      psb_status st;
+      if (m.kernel_id == PSB_KERNEL_HIMENO19)
+        st = cfg.t_depth == 2 ? himeno_tb2_launch(m, m, m.grids[0], m.grids[1], cfg.z_chunk,
+                                                  r.stream, &launches)
+                              : himeno_launch(m, cfg, r.stream, &launches);
+      else
+        st = cfg.t_depth == 2 ? diffusion7_tb2_launch(m, m.grids[0], m.grids[1], cfg.z_chunk,
+                                                      r.stream, &launches)
+                              : diffusion7_launch(m, cfg, r.stream, &launches);
       if (st != PSB_OK) {
         cudaEventDestroy(a);
         cudaEventDestroy(b);
@@ -336,6 +340,20 @@ psb_status psb_autotune(int kernel_id, int type, const PSIndex *dims, int force,
       psb_tune_config c;
       c.impl = PSB_IMPL_TMA;
       c.tile_x = 128;
+      c.tile_y = 8;
+      c.z_chunk = zc;
+      c.stages = 6;
+      c.t_depth = 2;
+      cands.push_back(c);
+    }
+  // Himeno, two sweeps per pass (64 x 8 tiles; the single-sweep fields of
+  // the entry are the default shape, used for maps run alone).
+  if (kernel_id == PSB_KERNEL_HIMENO19)
+    for (int zc : {16, 32, 64}) {
+      if (zc > dims[2] * 2) continue;
+      psb_tune_config c;
+      c.impl = PSB_IMPL_TMA;
+      c.tile_x = 64;
       c.tile_y = 8;
       c.z_chunk = zc;
       c.stages = 6;
