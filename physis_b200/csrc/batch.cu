@@ -208,6 +208,74 @@ __device__ __forceinline__ ItemGeom item_geom(const BMember &M, int t) {
   return g;
 }
 
+// Dependencies of item (s, t) of member M on its step (or pass) s-1, where
+// every item completes `units` counts (one per consumer warp). After a step
+// that measures the residual: all of it and its convergence decision.
+// Otherwise the tiles this item's planes read (its own and the 26 around
+// it, wrapping for periodic members, whose edge tiles also write the
+// opposite halo), which are also every tile that read the planes it
+// overwrites: consecutive steps of one member overlap like a wavefront
+// instead of meeting at a barrier. Every dependency is an item earlier in
+// the list, so the earliest unfinished item can always run. Bounded: false
+// when the batch's error word is set or the wait gave up.
+__device__ bool wait_item_deps(const BatchDev &B, const BMember &M, int s, int t, int units,
+                               bool after_check, bool wrap) {
+  const unsigned full = (unsigned)M.ntiles * units;
+  const unsigned *cnt = M.step_cnt + (s - 1);
+  const long long t0 = clock64();
+  unsigned sleep = 32;
+  if (after_check) {
+    while (ld_acquire(cnt) < full + 1u) {
+      if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) return false;
+      __nanosleep(sleep);
+      if (sleep < 2048) sleep <<= 1;
+    }
+  } else if (M.ntiles < kWaveTiles) {
+    // Small members: their steps are short and end almost together;
+    // waiting for the whole step costs one counter.
+    while (ld_acquire(cnt) < full) {
+      if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) return false;
+      __nanosleep(sleep);
+      if (sleep < 2048) sleep <<= 1;
+    }
+  } else if (ld_acquire(cnt) < full) {
+    const int tx = M.tiles_x, ty = M.tiles_y, tz = M.nzc;
+    const int cx = t % tx, cy = (t / tx) % ty, cz = t / (tx * ty);
+    const unsigned need = (unsigned)s * units;
+    // The 27 counters are read together (independent loads in flight at
+    // once), then only the ones not yet reached are polled.
+    const unsigned *nb[27];
+#pragma unroll
+    for (int k = 0; k < 27; k++) {
+      int x = cx + k % 3 - 1, y = cy + (k / 3) % 3 - 1, z = cz + k / 9 - 1;
+      bool in = true;
+      if (x < 0 || x >= tx) { in = wrap; x = (x + tx) % tx; }
+      if (y < 0 || y >= ty) { in = in && wrap; y = (y + ty) % ty; }
+      if (z < 0 || z >= tz) { in = in && wrap; z = (z + tz) % tz; }
+      nb[k] = in ? M.tile_done + (x + tx * (y + ty * z)) : nullptr;
+    }
+    unsigned v[27];
+#pragma unroll
+    for (int k = 0; k < 27; k++) v[k] = nb[k] ? ld_relaxed(nb[k]) : need;
+    unsigned pending = 0;
+#pragma unroll
+    for (int k = 0; k < 27; k++)
+      if (v[k] < need) pending |= 1u << k;
+    while (pending) {
+      if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) return false;
+      __nanosleep(sleep);
+      if (sleep < 2048) sleep <<= 1;
+      if (ld_relaxed(cnt) >= full) break;  // the whole step is done
+#pragma unroll
+      for (int k = 0; k < 27; k++)
+        if ((pending >> k & 1u) && ld_relaxed(nb[k]) >= need) pending &= ~(1u << k);
+    }
+    // Acquire what the relaxed reads observed.
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+  }
+  return true;
+}
+
 // Producer thread: takes items (from the shared cursor, or item `blockIdx.x`
 // of `step` when step >= 0), waits until the item's member has completed
 // its previous step, hands the item to the consumers through the descriptor
@@ -235,81 +303,11 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, const 
       m = __ldg(B.order + k);
       t = (int)(local - __ldg(B.tile_prefix + k));
       M = &B.members[m];
-      // Dependencies on step s-1 of the member. After a step that measures
-      // the residual: all of it and its convergence decision. Otherwise the
-      // tiles this item's planes read (its own and the 26 around it,
-      // wrapping for periodic members, whose edge tiles also write the
-      // opposite halo), which are also every tile that read the planes it
-      // overwrites: consecutive steps of one member overlap like a
-      // wavefront instead of meeting at a barrier. Every dependency is an
-      // item earlier in the list, so the earliest unfinished item can always
-      // run.
-      if (s > 0) {
-        const unsigned full = step_full(*M);
-        const bool after_check = is_check_step<GROUP>(*M, M->step0 + s - 1);
-        const unsigned *cnt = M->step_cnt + (s - 1);
-        const long long t0 = clock64();
-        unsigned sleep = 32;
-        if (after_check) {
-          while (ld_acquire(cnt) < full + 1u) {
-            if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) {
-              ok = false;
-              break;
-            }
-            __nanosleep(sleep);
-            if (sleep < 2048) sleep <<= 1;
-          }
-        } else if (M->ntiles < kWaveTiles) {
-          // Small members: their steps are short and end almost together;
-          // waiting for the whole step costs one counter.
-          while (ld_acquire(cnt) < full) {
-            if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) {
-              ok = false;
-              break;
-            }
-            __nanosleep(sleep);
-            if (sleep < 2048) sleep <<= 1;
-          }
-        } else if (ld_acquire(cnt) < full) {
-          const int tx = M->tiles_x, ty = M->tiles_y, tz = M->nzc;
-          const int cx = t % tx, cy = (t / tx) % ty, cz = t / (tx * ty);
-          const bool wrap = GROUP == 0 && M->kind == BK_DIFF7P;
-          const unsigned need = (unsigned)s * kBWarps;
-          // The 27 counters are read together (independent loads in flight
-          // at once), then only the ones not yet reached are polled.
-          const unsigned *nb[27];
-#pragma unroll
-          for (int k = 0; k < 27; k++) {
-            int x = cx + k % 3 - 1, y = cy + (k / 3) % 3 - 1, z = cz + k / 9 - 1;
-            bool in = true;
-            if (x < 0 || x >= tx) { in = wrap; x = (x + tx) % tx; }
-            if (y < 0 || y >= ty) { in = in && wrap; y = (y + ty) % ty; }
-            if (z < 0 || z >= tz) { in = in && wrap; z = (z + tz) % tz; }
-            nb[k] = in ? M->tile_done + (x + tx * (y + ty * z)) : nullptr;
-          }
-          unsigned v[27];
-#pragma unroll
-          for (int k = 0; k < 27; k++) v[k] = nb[k] ? ld_relaxed(nb[k]) : need;
-          unsigned pending = 0;
-#pragma unroll
-          for (int k = 0; k < 27; k++)
-            if (v[k] < need) pending |= 1u << k;
-          while (pending) {
-            if (ld_acquire_int(B.err) != 0 || clock64() - t0 > 4000000000LL) {
-              ok = false;
-              break;
-            }
-            __nanosleep(sleep);
-            if (sleep < 2048) sleep <<= 1;
-            if (ld_relaxed(cnt) >= full) break;  // the whole step is done
-#pragma unroll
-            for (int k = 0; k < 27; k++)
-              if ((pending >> k & 1u) && ld_relaxed(nb[k]) >= need) pending &= ~(1u << k);
-          }
-          // Acquire what the relaxed reads observed.
-          asm volatile("fence.acq_rel.gpu;" ::: "memory");
-        }
-      }
+      // Dependencies on step s-1 of the member (wait_item_deps).
+      if (s > 0)
+        ok = wait_item_deps(B, *M, s, t, kBWarps,
+                            is_check_step<GROUP>(*M, M->step0 + s - 1),
+                            GROUP == 0 && M->kind == BK_DIFF7P);
       if (!ok) {
         flags = kItemEnd;
       } else {
