@@ -162,7 +162,8 @@ class Result(ctypes.Structure):
 class BatchLayout(ctypes.Structure):
     """psb_batch_layout."""
     _fields_ = [("tile_x", ctypes.c_int), ("tile_y", ctypes.c_int), ("z_chunk", ctypes.c_int),
-                ("tiles", ctypes.c_int), ("wavefront", ctypes.c_int), ("tuned", ctypes.c_int)]
+                ("tiles", ctypes.c_int), ("wavefront", ctypes.c_int), ("tuned", ctypes.c_int),
+                ("t_depth", ctypes.c_int), ("units", ctypes.c_int)]
 
 
 # ---------------------------------------------------------------------------

@@ -45,6 +45,7 @@
 #include "batch.h"
 #include "k_diffusion7.cuh"
 #include "k_himeno.cuh"
+#include "k_himeno_tb2.cuh"
 
 namespace psb {
 
@@ -116,6 +117,10 @@ struct BMember {
   unsigned *tile_done;  // [ntiles] warps done on the tile, over all steps
   int *stop;         // local steps completed when converged, or -1
   double *res;       // [0] a or gosa, [1] b, [2] gosa of the first check, [3] check count
+  int group;         // work list: 0 diffusion, 1 Himeno, 2 Himeno two sweeps per pass
+  int cur0;          // buf[cur0] holds the state at local step 0; each unit flips it
+  const int *pass_start;  // group 2: local step of each pass (npasses + 1 entries)
+  int npasses;
 };
 
 struct BatchDev {
@@ -330,7 +335,7 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, const 
     // The step's inputs were written by generic stores of other CTAs and
     // acquired above; order that before the async-proxy (TMA) reads.
     asm volatile("fence.proxy.async.global;" ::: "memory");
-    const int par = (M->step0 + s) & 1;
+    const int par = (M->cur0 + s) & 1;
     const ItemGeom g = item_geom<GROUP>(*M, t);
     const int bx = GROUP == 0 ? M->dg.bx : M->hg.bx;
     const int by = GROUP == 0 ? M->dg.by : M->hg.by;
@@ -455,7 +460,7 @@ __device__ void batch_consume(const BatchDev &B, const Ring &R, const Ring &RC, 
     }
     const BMember &M = B.members[dm];
     const bool skip = (dflags & kItemSkip) != 0;
-    const int par = (M.step0 + ds) & 1;
+    const int par = (M.cur0 + ds) & 1;
     __syncwarp();
     if (lane == 0) mbar_arrive(&qempty[q]);
     const bool check = is_check_step<GROUP>(M, M.step0 + ds);
@@ -532,6 +537,222 @@ __global__ void __launch_bounds__(kBThreads, GROUP == 0 ? 3 : 2) k_batch(BatchDe
   batch_consume<GROUP>(B, R, RC, qfull, qempty, desc);
 }
 
+// ---------------------------------------------------------------------------
+// Group 2: Himeno members that advance up to two sweeps per item (passes).
+//
+// A member's local steps are cut into passes of one or two sweeps
+// (pass_start); a pass never straddles a residual check (a check step is
+// always the last step of its pass), so a check sees the sweep it needs.
+// Items are (member, pass, 64 x 8 tile x z chunk); the work list is ordered
+// by pass, then member, then tile, and an item depends on pass - 1 of its
+// member exactly as a single-sweep item depends on step - 1 (wait_item_deps:
+// the two-sweep halo of 2 cells stays inside the 27 tiles around it). Each
+// pass flips which buffer holds the state (buf[(cur0 + pass) & 1] in,
+// buf[(cur0 + pass + 1) & 1] out), so a two-sweep pass never writes the
+// buffer it reads. A CTA is one producer thread, five first-sweep warps and
+// four second-sweep warps on the rings of k_himeno_tb2.cuh; a one-sweep
+// pass runs the same rings with the second stage storing the first sweep.
+// Every consumer warp completes one unit per item (nine per item).
+// ---------------------------------------------------------------------------
+constexpr int kT2Units = kHtW1 + kHtW2;
+constexpr int kT2Threads = 32 * (1 + kT2Units);
+constexpr int kT2SmemRing = 1024;
+constexpr size_t kT2Smem = 128 + kT2SmemRing + kHtRingBytes;
+
+__device__ __forceinline__ int pass_end(const BMember &M, int q) { return __ldg(M.pass_start + q + 1); }
+
+// Whether pass q of a group-2 member ends with a residual check.
+__device__ __forceinline__ bool pass_checked(const BMember &M, int q) {
+  return is_check_step<1>(M, M.step0 + pass_end(M, q) - 1);
+}
+
+// Geometry of item t of a group-2 member: 64 x 8 tiles over the interior.
+__device__ __forceinline__ void t2_geom(const BMember &M, int t, int &x0, int &y0, int &zb,
+                                        int &nzl) {
+  const int tile_x = t % M.tiles_x;
+  const int rest = t / M.tiles_x;
+  const int tile_y = rest % M.tiles_y;
+  const int zc = rest / M.tiles_y;
+  x0 = M.hg.x_base + tile_x * kHtTX;
+  y0 = M.dom.lo[1] + tile_y * kHtTY;
+  zb = M.dom.lo[2] + zc * M.hg.zchunk;
+  nzl = min(zb + M.hg.zchunk, M.dom.hi[2]) - zb;
+}
+
+__device__ void t2_produce(const BatchDev &B, int step, const HtRings &R, uint64_t *qfull,
+                           uint64_t *qempty, ItemDesc *desc) {
+  RingPos p1{0, 0}, pc{0, 0};
+  bool ok = true;
+  for (uint32_t nq = 0;; nq++) {
+    long long item;
+    if (step >= 0)
+      item = nq == 0 ? (long long)B.step_offset[step] + blockIdx.x : (long long)B.total_items;
+    else
+      item = (long long)atomicAdd(B.cursor, 1ull);
+    int m = 0, s = 0, t = 0, flags = 0;
+    const BMember *M = nullptr;
+    if (item >= B.total_items || ld_acquire_int(B.err) != 0) {
+      flags = kItemEnd;
+    } else {
+      s = upper_index(B.step_offset, B.max_steps + 1, item);
+      const int64_t local = item - __ldg(B.step_offset + s);
+      const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
+      m = __ldg(B.order + k);
+      t = (int)(local - __ldg(B.tile_prefix + k));
+      M = &B.members[m];
+      if (s > 0) ok = wait_item_deps(B, *M, s, t, kT2Units, pass_checked(*M, s - 1), false);
+      if (!ok) {
+        flags = kItemEnd;
+      } else {
+        const int st = ld_acquire_int(M->stop);
+        if (st >= 0 && __ldg(M->pass_start + s) >= st) flags = kItemSkip;
+      }
+    }
+    const int q = nq % kQ;
+    if (nq >= kQ && !mbar_wait_bounded(&qempty[q], ((nq / kQ) - 1) & 1)) {
+      ok = false;
+      break;
+    }
+    desc[q].m = m;
+    desc[q].s = s;
+    desc[q].t = t;
+    desc[q].flags = flags;
+    mbar_arrive(&qfull[q]);
+    if (flags & kItemEnd) break;
+    if (flags & kItemSkip) continue;
+    asm volatile("fence.proxy.async.global;" ::: "memory");
+    const int par = (M->cur0 + s) & 1;
+    int x0, y0, zb, nzl;
+    t2_geom(*M, t, x0, y0, zb, nzl);
+    if (!ht_produce_tile(R, p1, pc, M->tmap[par], M->tcoef, M->hg.ax0, M->hg.ay0, M->hg.az0, x0,
+                         y0, zb, nzl)) {
+      ok = false;
+      break;
+    }
+  }
+  if (!ok) {
+    atomicExch(B.err, 1);
+    ht_drain(R, p1, pc);
+  }
+}
+
+// Completion of a group-2 item by consumer warp cw (0..8): its FP64
+// residual partial when the pass ends with a check, one unit of the tile's
+// and of the pass's counter; the warp that completes the pass combines the
+// partials in index order, decides, and only then releases the pass.
+__device__ __forceinline__ void t2_item_done(const BMember &M, int q, int t, int cw, int lane,
+                                             bool check, bool contrib, double a) {
+  const int pend = pass_end(M, q);
+  const int gstep = M.step0 + pend - 1;
+  double *P = M.partials + (int64_t)(q & 1) * M.ntiles * kT2Units * 2;
+  if (contrib) {
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_down_sync(0xffffffffu, a, o);
+    if (lane == 0) {
+      P[((int64_t)t * kT2Units + cw) * 2] = a;
+      P[((int64_t)t * kT2Units + cw) * 2 + 1] = 0.0;
+    }
+  }
+  __syncwarp();
+  unsigned last = 0;
+  if (lane == 0) {
+    __threadfence();
+    atomicAdd(M.tile_done + t, 1u);
+    const unsigned old = atomicAdd(M.step_cnt + q, 1u);
+    last = old + 1 == (unsigned)M.ntiles * kT2Units;
+  }
+  last = __shfl_sync(0xffffffffu, last, 0);
+  if (!last) return;
+  if (check && contrib) {
+    __threadfence();
+    const int n = M.ntiles * kT2Units;
+    double sa = 0;
+    for (int i = lane; i < n; i += 32) sa += __ldcg(&P[2 * i]);
+    for (int o = 16; o > 0; o >>= 1) sa += __shfl_down_sync(0xffffffffu, sa, o);
+    if (lane == 0) {
+      if (gstep == 0) M.res[2] = sa;
+      const double g0 = gstep == 0 ? sa : __ldcg(&M.res[2]);
+      const bool conv = sa <= M.tol2 * g0;
+      M.res[1] = g0;
+      M.res[0] = sa;
+      M.res[3] = (double)(gstep + 1);
+      if (conv && M.tol2 > 0) atomicExch(M.stop, pend);
+    }
+  }
+  if (lane == 0) {
+    __threadfence();
+    atomicAdd(M.step_cnt + q, 1u);
+  }
+}
+
+__device__ void t2_consume(const BatchDev &B, const HtRings &R, uint64_t *qfull,
+                           uint64_t *qempty, const ItemDesc *desc) {
+  const int lane = threadIdx.x & 31, cw = (threadIdx.x >> 5) - 1;
+  const bool first = cw < kHtW1;
+  RingPos p1{0, 0}, pc{0, 0}, p2{0, 0};
+  for (uint32_t nq = 0;; nq++) {
+    const int q = nq % kQ;
+    const bool got = __all_sync(0xffffffffu, mbar_wait_bounded(&qfull[q], (nq / kQ) & 1));
+    if (!got) {
+      if (lane == 0) atomicExch(B.err, 1);
+      return;
+    }
+    const int dm = desc[q].m, ds = desc[q].s, dt = desc[q].t, dflags = desc[q].flags;
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&qempty[q]);
+    if (dflags & kItemEnd) return;
+    const BMember &M = B.members[dm];
+    const bool skip = (dflags & kItemSkip) != 0;
+    const int len = pass_end(M, ds) - __ldg(M.pass_start + ds);
+    const bool check = pass_checked(M, ds);
+    double a = 0.0;
+    if (!skip) {
+      int x0, y0, zb, nzl;
+      t2_geom(M, dt, x0, y0, zb, nzl);
+      bool ok;
+      if (first) {
+        ok = ht_stage1_tile(R, p1, pc, p2, threadIdx.x - 32, lane, M.dom, M.omega, x0, y0, zb,
+                            nzl, check && len == 1, &a);
+      } else {
+        const int par = (M.cur0 + ds) & 1;
+        ok = ht_stage2_tile(R, p2, pc, threadIdx.x - 32 - 32 * kHtW1, lane,
+                            (float *)M.buf[par ^ 1].origin, M.sy, M.sz, M.dom, M.omega, x0, y0,
+                            zb, nzl, len == 1, check && len == 2, &a);
+      }
+      if (!ok) {
+        if (lane == 0) atomicExch(B.err, 1);
+        return;
+      }
+    }
+    t2_item_done(M, ds, dt, cw, lane, check, check && !skip, a);
+  }
+}
+
+// The group-2 kernel. step < 0: persistent (mode 0); step >= 0: item
+// blockIdx.x of that pass (mode 1). One CTA per SM (its rings take 175 KB).
+__global__ void __launch_bounds__(kT2Threads, 1) k_batch_tb2(BatchDev B, int step) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  unsigned char *smem = aligned_smem(smem_raw);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+  const HtRings R = ht_rings(bars, smem + kT2SmemRing);
+  uint64_t *qfull = bars + 48, *qempty = bars + 52;
+  ItemDesc *desc = reinterpret_cast<ItemDesc *>(smem + 448);
+  if (threadIdx.x == 0) {
+    ht_init(R);
+    for (int q = 0; q < kQ; q++) {
+      mbar_init(&qfull[q], 1);
+      mbar_init(&qempty[q], kT2Units);
+    }
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    if (threadIdx.x == 0) t2_produce(B, step, R, qfull, qempty, desc);
+    return;
+  }
+  t2_consume(B, R, qfull, qempty, desc);
+}
+static_assert(448 + kQ * sizeof(ItemDesc) <= kT2SmemRing, "item descriptors overlap the rings");
+
 }  // namespace psb
 
 using namespace psb;
@@ -568,11 +789,14 @@ struct psb_batch {
   size_t cap_members = 0, cap_tmaps = 0, cap_partials = 0, cap_done = 0, cap_stop = 0,
          cap_res = 0;  // bytes allocated (device buffers are reused while they fit)
   std::vector<BMember> members;
-  BatchGroup grp[2];
+  BatchGroup grp[3];
+  std::vector<std::vector<int>> passes;  // group-2 members: local step of each pass
+  int *d_pass = nullptr;
+  size_t cap_pass = 0;
   bool built = false;
   cudaGraphExec_t graph = nullptr;
-  cudaStream_t side = nullptr;       // second stream of the per-step graph
-  cudaEvent_t fork = nullptr, join = nullptr;
+  cudaStream_t side = nullptr, side2 = nullptr;  // streams of the second and third work lists
+  cudaEvent_t fork = nullptr, join = nullptr, join2 = nullptr;
   double last_ms = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // batch timing (apart from PSStencilRun's)
   int64_t last_launches = 0;
@@ -581,7 +805,7 @@ struct psb_batch {
 
 namespace psb {
 
-static int member_group(int kind) { return kind == BK_HIMENO ? 1 : 0; }
+
 
 // The work lists and descriptors no longer match the members.
 static void batch_invalidate(psb_batch *b) {
@@ -598,6 +822,9 @@ static void batch_release_device(psb_batch *b) {
   cudaFree(b->d_done);
   cudaFree(b->d_stop);
   cudaFree(b->d_res);
+  cudaFree(b->d_pass);
+  b->d_pass = nullptr;
+  b->cap_pass = 0;
   b->d_members = nullptr;
   b->d_tmaps = nullptr;
   b->d_partials = nullptr;
@@ -653,14 +880,16 @@ static const int kPromoP = PSB_PROMO_P, kPromoC = PSB_PROMO_C, kPromoD = PSB_PRO
 struct MemberTune {
   int tx = 0;
   int zc = 0;
+  int td = 1;  // Himeno sweeps per pass
   bool forced = false;
 };
 
 static MemberTune member_tune(const BatchMemberHost &h) {
   MemberTune t;
-  if (h.force_tx > 0 || h.force_zc > 0) {
+  if (h.force_tx > 0 || h.force_zc > 0 || h.force_td > 0) {
     t.tx = h.force_tx;
     t.zc = h.force_zc;
+    t.td = h.force_td > 0 ? h.force_td : 1;
     t.forced = true;
     return t;
   }
@@ -668,8 +897,33 @@ static MemberTune member_tune(const BatchMemberHost &h) {
   if (batch_tune_find(h.kind, h.grids[0]->pub.dim, &c)) {
     t.tx = c.tile_x / 4;
     t.zc = c.z_chunk;
+    t.td = c.t_depth;
   }
   return t;
+}
+
+// Work list of a member: 0 diffusion, 1 Himeno one sweep per item, 2 Himeno
+// up to two sweeps per item (when its tune entry or trial says so and it
+// runs at least two steps).
+static int member_group(const BatchMemberHost &h, const MemberTune &mt, int steps) {
+  if (h.kind != BK_HIMENO) return 0;
+  return mt.td == 2 && steps >= 2 ? 2 : 1;
+}
+
+// Passes of a group-2 member: from each local step s (global step0 + s) two
+// sweeps unless s is a check step or the last step, so that every check
+// step ends its pass.
+static std::vector<int> member_passes(const BatchMemberHost &h, int step0, int steps) {
+  std::vector<int> st{0};
+  auto check = [&](int g) {
+    return h.check_every > 0 && ((g + 1) % h.check_every == 0 || g == 0);
+  };
+  int s = 0;
+  while (s < steps) {
+    s += (s + 1 < steps && !check(step0 + s)) ? 2 : 1;
+    st.push_back(s);
+  }
+  return st;
 }
 
 static void pick_shape(int nx, int ny, int rows_per_thread, int *tx_threads, int *ty_threads,
@@ -755,7 +1009,29 @@ static HimenoGeom batch_hgeom(const GridImpl *g, int zc_floor, const MemberTune 
   return geo;
 }
 
+// Group 2: 64 x 8 tiles over the interior [1, n-1), x from 0; the pressure
+// box (72 x 12) is the tensor-map box of the member's p grids.
+static HimenoGeom batch_t2geom(const GridImpl *g, int zc_floor, const MemberTune &mt) {
+  HimenoGeom geo;
+  geo.tx_threads = kHtTX / 4;
+  geo.ty_threads = kHtTY;
+  geo.bx = kHtBX;
+  geo.by = kHtBY1;
+  geo.ax0 = g->pad_left;
+  geo.ay0 = g->halo;
+  geo.az0 = g->halo;
+  geo.x_base = 0;
+  geo.tiles_x = (g->pub.dim[0] - 1 + kHtTX - 1) / kHtTX;
+  geo.tiles_y = (g->pub.dim[1] - 2 + kHtTY - 1) / kHtTY;
+  geo.zchunk = member_zchunk(mt, (int64_t)geo.tiles_x * geo.tiles_y, g->pub.dim[2] - 2, zc_floor);
+  geo.stages = kHtS1;
+  geo.stage_bytes = kHtStage1;
+  geo.nx = g->pub.dim[0];
+  return geo;
+}
+
 static size_t batch_smem(int group) {
+  if (group == 2) return kT2Smem;
   return 128 + kSmemRing + (size_t)kBStages * kind_stage_bytes(group) +
          (group == 1 ? (size_t)kCStages * kCoefStageBytes : 0);
 }
@@ -770,23 +1046,40 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
   std::vector<CUtensorMap> tmaps(2 * std::max(1, n));
   std::vector<int> coef_map(n, -1);  // index of a Himeno member's 12 coefficient maps
   std::vector<MemberTune> mt(n);
-  for (int i = 0; i < n; i++) mt[i] = member_tune(b->hm[i]);
-  // The longest z chunk at which each kind's members together give
+  std::vector<int> group(n), units(n);  // work list and its units (steps or passes) per member
+  b->passes.assign(n, std::vector<int>());
+  for (int i = 0; i < n; i++) {
+    mt[i] = member_tune(b->hm[i]);
+    group[i] = member_group(b->hm[i], mt[i], steps[i]);
+    units[i] = std::max(0, steps[i]);
+    if (group[i] == 2) {
+      b->passes[i] = member_passes(b->hm[i], step0[i], steps[i]);
+      units[i] = (int)b->passes[i].size() - 1;
+    }
+  }
+  // The longest z chunk at which each work list's members together give
   // items_target() items per step (4 if none does).
-  int zc_floor[2] = {4, 4};
-  for (int k = 0; k < 2; k++) {
+  auto xy_tiles = [&](int i, int k) -> int64_t {
+    const GridImpl *g0 = b->hm[i].grids[0];
+    if (k == 2) {
+      const HimenoGeom hg = batch_t2geom(g0, 64, mt[i]);
+      return (int64_t)hg.tiles_x * hg.tiles_y;
+    }
+    if (k == 1) {
+      const HimenoGeom hg = batch_hgeom(g0, 64, mt[i]);
+      return (int64_t)hg.tiles_x * hg.tiles_y;
+    }
+    const TmaGeom dg = batch_dgeom(g0, 64, mt[i]);
+    return (int64_t)dg.tiles_x * dg.tiles_y;
+  };
+  int zc_floor[3] = {4, 4, 4};
+  for (int k = 0; k < 3; k++) {
     for (int zc = 64; zc > 4; zc >>= 1) {
       int64_t items = 0;
       for (int i = 0; i < n; i++) {
-        if (steps[i] <= 0 || (b->hm[i].kind == BK_HIMENO) != (k == 1)) continue;
-        const GridImpl *g0 = b->hm[i].grids[0];
-        if (k == 1) {
-          const HimenoGeom hg = batch_hgeom(g0, 64, mt[i]);
-          items += (int64_t)hg.tiles_x * hg.tiles_y * ((g0->pub.dim[2] - 2 + zc - 1) / zc);
-        } else {
-          const TmaGeom dg = batch_dgeom(g0, 64, mt[i]);
-          items += (int64_t)dg.tiles_x * dg.tiles_y * ((g0->pub.dim[2] + zc - 1) / zc);
-        }
+        if (steps[i] <= 0 || group[i] != k) continue;
+        const int nz = b->hm[i].grids[0]->pub.dim[2] - (k == 0 ? 0 : 2);
+        items += xy_tiles(i, k) * ((nz + zc - 1) / zc);
       }
       if (items >= items_target()) {
         zc_floor[k] = zc;
@@ -794,16 +1087,18 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
       }
     }
   }
-  int64_t partial_slots = 0;
+  int64_t partial_slots = 0, pass_words = 0;
   for (int i = 0; i < n; i++) {
     const BatchMemberHost &h = b->hm[i];
     BMember &M = b->members[i];
     memset(&M, 0, sizeof(M));
     M.kind = h.kind;
+    M.group = group[i];
     GridImpl *g0 = h.grids[0], *g1 = h.grids[1];
     for (int k = 0; k < 3; k++) M.n[k] = g0->pub.dim[k];
     M.steps = steps[i];
     M.step0 = step0[i];
+    M.cur0 = h.cur0 & 1;
     M.check_every = h.check_every;
     M.tol2 = h.tol * h.tol;
     M.buf[0] = g0->view();
@@ -812,7 +1107,8 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     M.sz = g0->sz;
     const CUtensorMap *a = nullptr, *c = nullptr;
     if (h.kind == BK_HIMENO) {
-      M.hg = batch_hgeom(g0, zc_floor[1], mt[i]);
+      const bool two = group[i] == 2;
+      M.hg = two ? batch_t2geom(g0, zc_floor[2], mt[i]) : batch_hgeom(g0, zc_floor[1], mt[i]);
       for (int k = 0; k < 3; k++) {
         M.dom.lo[k] = 1;
         M.dom.hi[k] = g0->pub.dim[k] - 1;
@@ -827,8 +1123,15 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
       coef_map[i] = (int)tmaps.size();
       for (int k = 0; k < 12; k++) {
         const CUtensorMap *cm = nullptr;
-        PSB_CHECK(get_tmap(h.grids[2 + k], M.hg.tx_threads * 4, M.hg.ty_threads, &cm, kPromoC));
+        if (two)
+          PSB_CHECK(get_tmap(h.grids[2 + k], kHtBX, kHtBY2, &cm, kPromoC));
+        else
+          PSB_CHECK(get_tmap(h.grids[2 + k], M.hg.tx_threads * 4, M.hg.ty_threads, &cm, kPromoC));
         tmaps.push_back(*cm);
+      }
+      if (two) {
+        M.npasses = units[i];
+        pass_words += units[i] + 1;
       }
     } else {
       M.dg = batch_dgeom(g0, zc_floor[0], mt[i]);
@@ -852,15 +1155,22 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     tmaps[2 * i] = *a;
     tmaps[2 * i + 1] = *c;
     M.ntiles = M.tiles_x * M.tiles_y * M.nzc;
-    partial_slots += 2 * 2 * kBWarps * (int64_t)M.ntiles;
+    partial_slots += 2 * 2 * (group[i] == 2 ? kT2Units : kBWarps) * (int64_t)M.ntiles;
   }
   PSB_CHECK(dev_reserve(&b->d_tmaps, &b->cap_tmaps, sizeof(CUtensorMap) * tmaps.size()));
   PSB_TRY(cudaMemcpy(b->d_tmaps, tmaps.data(), sizeof(CUtensorMap) * tmaps.size(),
                      cudaMemcpyHostToDevice));
   PSB_CHECK(dev_reserve(&b->d_partials, &b->cap_partials,
                         sizeof(double) * std::max<int64_t>(1, partial_slots)));
+  if (pass_words) {
+    std::vector<int> flat;
+    flat.reserve(pass_words);
+    for (int i = 0; i < n; i++) flat.insert(flat.end(), b->passes[i].begin(), b->passes[i].end());
+    PSB_CHECK(dev_reserve(&b->d_pass, &b->cap_pass, sizeof(int) * flat.size()));
+    PSB_TRY(cudaMemcpy(b->d_pass, flat.data(), sizeof(int) * flat.size(), cudaMemcpyHostToDevice));
+  }
   int64_t counters = 0;
-  for (int i = 0; i < n; i++) counters += std::max(0, steps[i]) + b->members[i].ntiles;
+  for (int i = 0; i < n; i++) counters += units[i] + b->members[i].ntiles;
   b->n_counters = std::max<int64_t>(1, counters);
   PSB_CHECK(dev_reserve(&b->d_done, &b->cap_done, sizeof(unsigned) * b->n_counters));
   PSB_CHECK(dev_reserve(&b->d_stop, &b->cap_stop, sizeof(int) * std::max(1, n)));
@@ -869,47 +1179,52 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
     PSB_TRY(cudaMemcpy(b->d_res, b->res_init.data(), sizeof(double) * 4 * n, cudaMemcpyHostToDevice));
   else
     PSB_TRY(cudaMemset(b->d_res, 0, sizeof(double) * 4 * std::max(1, n)));
-  int64_t off = 0, coff = 0;
+  int64_t off = 0, coff = 0, poff = 0;
   for (int i = 0; i < n; i++) {
     BMember &M = b->members[i];
     M.tmap[0] = b->d_tmaps + 2 * i;
     M.tmap[1] = b->d_tmaps + 2 * i + 1;
     M.tcoef = coef_map[i] >= 0 ? b->d_tmaps + coef_map[i] : nullptr;
     M.partials = b->d_partials + off;
-    off += 2 * 2 * kBWarps * (int64_t)M.ntiles;
+    off += 2 * 2 * (group[i] == 2 ? kT2Units : kBWarps) * (int64_t)M.ntiles;
     M.step_cnt = b->d_done + coff;
-    coff += std::max(0, steps[i]);
+    coff += units[i];
     M.tile_done = b->d_done + coff;
     coff += M.ntiles;
     M.stop = b->d_stop + i;
     M.res = b->d_res + 4 * i;
+    if (group[i] == 2) {
+      M.pass_start = b->d_pass + poff;
+      poff += units[i] + 1;
+    }
   }
   PSB_CHECK(dev_reserve(&b->d_members, &b->cap_members, sizeof(BMember) * std::max(1, n)));
   PSB_TRY(cudaMemcpy(b->d_members, b->members.data(), sizeof(BMember) * n, cudaMemcpyHostToDevice));
-  // One work list per kernel kind. Members are ordered by steps
-  // (descending), so the members still running at step s are a prefix.
-  for (int gi = 0; gi < 2; gi++) {
+  // One work list per kernel kind, in units of steps (passes for group 2).
+  // Members are ordered by units (descending), so the members still running
+  // at unit s are a prefix.
+  for (int gi = 0; gi < 3; gi++) {
     BatchGroup &G = b->grp[gi];
     G.order.clear();
     for (int i = 0; i < n; i++)
-      if (member_group(b->hm[i].kind) == gi) G.order.push_back(i);
+      if (group[i] == gi) G.order.push_back(i);
     std::stable_sort(G.order.begin(), G.order.end(),
-                     [&](int x, int y) { return steps[x] > steps[y]; });
+                     [&](int x, int y) { return units[x] > units[y]; });
     const int gn = (int)G.order.size();
     G.tile_prefix.assign(gn + 1, 0);
     for (int i = 0; i < gn; i++)
       G.tile_prefix[i + 1] = G.tile_prefix[i] + b->members[G.order[i]].ntiles;
-    G.max_steps = gn ? steps[G.order[0]] : 0;
+    G.max_steps = gn ? units[G.order[0]] : 0;
     G.step_offset.assign(G.max_steps + 1, 0);
     int active = gn;
     for (int st = 0; st < G.max_steps; st++) {
-      while (active > 0 && steps[G.order[active - 1]] <= st) active--;
+      while (active > 0 && units[G.order[active - 1]] <= st) active--;
       G.step_offset[st + 1] = G.step_offset[st] + G.tile_prefix[active];
     }
     G.total_items = G.max_steps ? G.step_offset[G.max_steps] : 0;
     G.work = 0;
     for (int i : G.order)
-      G.work += (double)b->hm[i].points * steps[i] * (gi == 1 ? 56.0 : 8.0);
+      G.work += (double)b->hm[i].points * steps[i] * (gi == 0 ? 8.0 : gi == 1 ? 56.0 : 28.0);
     PSB_CHECK(dev_reserve(&G.d_order, &G.cap_order, sizeof(int) * std::max(1, gn)));
     if (gn) PSB_TRY(cudaMemcpy(G.d_order, G.order.data(), sizeof(int) * gn, cudaMemcpyHostToDevice));
     PSB_CHECK(dev_reserve(&G.d_tile_prefix, &G.cap_tile_prefix, sizeof(int64_t) * (gn + 1)));
@@ -926,13 +1241,18 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
                                    cudaSharedmemCarveoutMaxShared));
       PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<0>, kBThreads,
                                                             batch_smem(0)));
-    } else {
+    } else if (gi == 1) {
       PSB_TRY(cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                    cudaSharedmemCarveoutMaxShared));
       PSB_TRY(cudaFuncSetAttribute(k_batch<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)batch_smem(1)));
       PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch<1>, kBThreads,
                                                             batch_smem(1)));
+    } else {
+      PSB_TRY(cudaFuncSetAttribute(k_batch_tb2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)batch_smem(2)));
+      PSB_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_tb2, kT2Threads,
+                                                            batch_smem(2)));
     }
     G.blocks_persistent = std::max(1, per_sm) * r.sm_count;
   }
@@ -943,8 +1263,19 @@ psb_status batch_prepare(psb_batch *b, const std::vector<int> &steps, const std:
 // Whether the steps of member i overlap as a wavefront in the prepared
 // launch (the producer's per-tile dependency path).
 bool batch_member_wavefront(const psb_batch *b, int i) {
-  return b->built && i >= 0 && i < (int)b->members.size() &&
-         b->members[i].ntiles >= kWaveTiles && b->members[i].steps > 1;
+  if (!b->built || i < 0 || i >= (int)b->members.size()) return false;
+  const BMember &M = b->members[i];
+  return M.ntiles >= kWaveTiles && (M.group == 2 ? M.npasses : M.steps) > 1;
+}
+
+int batch_member_cur(const psb_batch *b, int i, int done) {
+  const BatchMemberHost &h = b->hm[i];
+  if (!b->built || i >= (int)b->members.size() || b->members[i].group != 2)
+    return (h.cur0 + done) & 1;
+  // Passes that ended at or before `done` each flipped the buffer.
+  const std::vector<int> &ps = b->passes[i];
+  const int passes = (int)(std::upper_bound(ps.begin(), ps.end(), done) - ps.begin()) - 1;
+  return (h.cur0 + passes) & 1;
 }
 
 // After a run: per member, local steps completed when it converged (-1 if
@@ -985,9 +1316,26 @@ static BatchDev batch_dev(psb_batch *b, int gi) {
 static psb_status batch_side_stream(psb_batch *b) {
   if (!b->side) {
     PSB_TRY(cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking));
+    PSB_TRY(cudaStreamCreateWithFlags(&b->side2, cudaStreamNonBlocking));
     PSB_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
     PSB_TRY(cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming));
+    PSB_TRY(cudaEventCreateWithFlags(&b->join2, cudaEventDisableTiming));
   }
+  return PSB_OK;
+}
+
+// One launch of work list gi on stream ss (step < 0: persistent).
+static psb_status batch_launch_group(psb_batch *b, int gi, cudaStream_t ss, int step,
+                                     unsigned blocks) {
+  const BatchDev B = batch_dev(b, gi);
+  if (gi == 0)
+    k_batch<0><<<blocks, kBThreads, batch_smem(0), ss>>>(B, step);
+  else if (gi == 1)
+    k_batch<1><<<blocks, kBThreads, batch_smem(1), ss>>>(B, step);
+  else
+    k_batch_tb2<<<blocks, kT2Threads, batch_smem(2), ss>>>(B, step);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_status(e, "k_batch");
   return PSB_OK;
 }
 
@@ -997,36 +1345,43 @@ static psb_status batch_side_stream(psb_batch *b) {
 // other's tail.
 psb_status batch_launch_persistent(psb_batch *b, cudaStream_t s, int64_t *launches) {
   PSB_CHECK(batch_reset_counters(b, s));
-  const bool both = b->grp[0].total_items && b->grp[1].total_items;
-  if (both) {
+  // Work lists with items, the one with most work first on s, the others on
+  // side streams forked from s: each one's CTAs take slots as the others
+  // retire, so they fill each other's tails.
+  int order[3], nl = 0;
+  for (int gi = 0; gi < 3; gi++)
+    if (b->grp[gi].total_items) order[nl++] = gi;
+  for (int i = 1; i < nl; i++)  // by work, descending (at most three lists)
+    for (int j = i; j > 0 && b->grp[order[j]].work > b->grp[order[j - 1]].work; j--)
+      std::swap(order[j], order[j - 1]);
+  if (nl > 1) {
     PSB_CHECK(batch_side_stream(b));
     PSB_TRY(cudaEventRecord(b->fork, s));
     PSB_TRY(cudaStreamWaitEvent(b->side, b->fork, 0));
+    if (nl > 2) PSB_TRY(cudaStreamWaitEvent(b->side2, b->fork, 0));
   }
-  const int first = b->grp[1].work > b->grp[0].work ? 1 : 0;
-  for (int k = 0; k < 2; k++) {
-    const int gi = k == 0 ? first : 1 - first;
+  for (int k = 0; k < nl; k++) {
+    const int gi = order[k];
     const BatchGroup &G = b->grp[gi];
-    if (!G.total_items) continue;
-    cudaStream_t ss = both && k == 1 ? b->side : s;
+    cudaStream_t ss = k == 0 ? s : (k == 1 ? b->side : b->side2);
     const int blocks = (int)std::min<int64_t>(G.blocks_persistent, G.total_items);
-    if (gi == 0)
-      k_batch<0><<<blocks, kBThreads, batch_smem(0), ss>>>(batch_dev(b, 0), -1);
-    else
-      k_batch<1><<<blocks, kBThreads, batch_smem(1), ss>>>(batch_dev(b, 1), -1);
+    PSB_CHECK(batch_launch_group(b, gi, ss, -1, (unsigned)blocks));
     (*launches)++;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_status(e, "k_batch");
   }
-  if (both) {
+  if (nl > 1) {
     PSB_TRY(cudaEventRecord(b->join, b->side));
     PSB_TRY(cudaStreamWaitEvent(s, b->join, 0));
+    if (nl > 2) {
+      PSB_TRY(cudaEventRecord(b->join2, b->side2));
+      PSB_TRY(cudaStreamWaitEvent(s, b->join2, 0));
+    }
   }
   return PSB_OK;
 }
 
-// Per-step launches (mode 1): both kinds' step sequences, on two streams
-// forked and joined inside one CUDA graph, recorded once and replayed.
+// Per-step launches (mode 1): each work list's unit sequence (steps, or
+// passes for two-sweep Himeno members) on its own stream, forked and joined
+// inside one CUDA graph, recorded once and replayed.
 psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches) {
   if (!b->graph) {
     PSB_CHECK(batch_side_stream(b));
@@ -1035,22 +1390,24 @@ psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches) {
     psb_status st = batch_reset_counters(b, s);
     cudaEventRecord(b->fork, s);
     cudaStreamWaitEvent(b->side, b->fork, 0);
-    for (int gi = 0; gi < 2 && st == PSB_OK; gi++) {
+    cudaStreamWaitEvent(b->side2, b->fork, 0);
+    for (int gi = 0; gi < 3 && st == PSB_OK; gi++) {
       const BatchGroup &G = b->grp[gi];
-      cudaStream_t ss = gi == 0 ? s : b->side;
-      const BatchDev B = batch_dev(b, gi);
+      cudaStream_t ss = gi == 0 ? s : (gi == 1 ? b->side : b->side2);
       int active = (int)G.order.size();
-      for (int step = 0; step < G.max_steps; step++) {
-        while (active > 0 && b->members[G.order[active - 1]].steps <= step) active--;
-        const unsigned blocks = (unsigned)G.tile_prefix[active];
-        if (gi == 0)
-          k_batch<0><<<blocks, kBThreads, batch_smem(0), ss>>>(B, step);
-        else
-          k_batch<1><<<blocks, kBThreads, batch_smem(1), ss>>>(B, step);
+      auto units = [&](int m) {
+        const BMember &M = b->members[m];
+        return M.group == 2 ? M.npasses : M.steps;
+      };
+      for (int step = 0; step < G.max_steps && st == PSB_OK; step++) {
+        while (active > 0 && units(G.order[active - 1]) <= step) active--;
+        st = batch_launch_group(b, gi, ss, step, (unsigned)G.tile_prefix[active]);
       }
     }
     cudaEventRecord(b->join, b->side);
     cudaStreamWaitEvent(s, b->join, 0);
+    cudaEventRecord(b->join2, b->side2);
+    cudaStreamWaitEvent(s, b->join2, 0);
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (st != PSB_OK || e != cudaSuccess) {
       if (e == cudaSuccess) cudaGraphDestroy(g);
@@ -1062,7 +1419,7 @@ psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches) {
     if (e != cudaSuccess) return cuda_status(e, "batch graph instantiate");
   }
   PSB_TRY(cudaGraphLaunch(b->graph, s));
-  *launches += b->grp[0].max_steps + b->grp[1].max_steps;
+  *launches += b->grp[0].max_steps + b->grp[1].max_steps + b->grp[2].max_steps;
   return PSB_OK;
 }
 
@@ -1093,8 +1450,10 @@ void batch_delete(psb_batch *b) {
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->side) cudaStreamDestroy(b->side);
+  if (b->side2) cudaStreamDestroy(b->side2);
   if (b->fork) cudaEventDestroy(b->fork);
   if (b->join) cudaEventDestroy(b->join);
+  if (b->join2) cudaEventDestroy(b->join2);
   delete b;
 }
 
@@ -1290,7 +1649,7 @@ psb_status psb_batch_member_result(psb_batch *b, int member, int *steps_done, do
   }
   if (steps_done) *steps_done = done;
   if (residual) *residual = res;
-  if (result_grid) *result_grid = done & 1;
+  if (result_grid) *result_grid = batch_member_cur(b, member, done);
   return PSB_OK;
 }
 
@@ -1336,12 +1695,20 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
   if (st == PSB_OK && cudaEventCreate(&e0) != cudaSuccess) st = PSB_ERR_CUDA;
   if (st == PSB_OK && cudaEventCreate(&e1) != cudaSuccess) st = PSB_ERR_CUDA;
   double best = -1;
-  for (int tx : txs) {
+  // Himeno buckets also try two sweeps per pass (64 x 8 tiles), recorded as
+  // t_depth 2 with tile_x 64.
+  std::vector<std::array<int, 2>> cands;  // (tile width in threads, t_depth)
+  for (int tx : txs) cands.push_back({tx, 1});
+  if (h.kind == BK_HIMENO) cands.push_back({kHtTX / 4, 2});
+  for (const auto &cd : cands) {
+    const int tx = cd[0], td = cd[1];
     for (int zc : {4, 8, 16, 32, 64}) {
       if (st != PSB_OK) break;
       if (zc > 2 * std::max(nz, 2)) continue;
+      if (td == 2 && zc < 8) continue;
       t.force_tx = tx;
       t.force_zc = zc;
+      t.force_td = td;
       batch_set_members(tb, {t}, {});
       st = batch_prepare(tb, {kTuneSteps}, {0});
       double ms_best = -1;
@@ -1356,16 +1723,17 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
         if (rep > 0 && (ms_best < 0 || ms < ms_best)) ms_best = ms;  // rep 0 warms up
       }
       if (__ps_trace)
-        fprintf(__ps_trace, "physis_b200: batch tune kind=%d tile=%dx%d zc=%d: %.4f ms\n", h.kind,
-                tx * 4, (kBConsumers / tx) * rows_per_thread, zc, ms_best);
+        fprintf(__ps_trace, "physis_b200: batch tune kind=%d tile=%dx%d zc=%d t=%d: %.4f ms\n",
+                h.kind, tx * 4, td == 2 ? kHtTY : (kBConsumers / tx) * rows_per_thread, zc, td,
+                ms_best);
       if (st == PSB_OK && ms_best > 0 && (best < 0 || ms_best < best)) {
         best = ms_best;
         best_cfg->impl = PSB_IMPL_TMA;
         best_cfg->tile_x = tx * 4;
-        best_cfg->tile_y = (kBConsumers / tx) * rows_per_thread;
+        best_cfg->tile_y = td == 2 ? kHtTY : (kBConsumers / tx) * rows_per_thread;
         best_cfg->z_chunk = zc;
         best_cfg->stages = kBStages;
-        best_cfg->t_depth = 1;
+        best_cfg->t_depth = td;
       }
     }
   }
@@ -1415,13 +1783,15 @@ psb_status psb_batch_member_layout(psb_batch *b, int member, psb_batch_layout *l
     return set_status(PSB_ERR_INVALID);
   const BMember &M = b->members[member];
   const bool him = M.kind == BK_HIMENO;
-  layout->tile_x = (him ? M.hg.tx_threads : M.dg.tx_threads) * 4;
-  layout->tile_y = him ? M.hg.ty_threads : M.dg.ty_threads * kVY;
+  layout->tile_x = M.group == 2 ? kHtTX : (him ? M.hg.tx_threads : M.dg.tx_threads) * 4;
+  layout->tile_y = M.group == 2 ? kHtTY : him ? M.hg.ty_threads : M.dg.ty_threads * kVY;
   layout->z_chunk = him ? M.hg.zchunk : M.dg.zchunk;
   layout->tiles = M.ntiles;
   layout->wavefront = batch_member_wavefront(b, member) ? 1 : 0;
   const MemberTune mt = member_tune(b->hm[member]);
   layout->tuned = !mt.forced && mt.tx > 0 ? 1 : 0;
+  layout->t_depth = M.group == 2 ? 2 : 1;
+  layout->units = M.group == 2 ? M.npasses : M.steps;
   return PSB_OK;
 }
 
@@ -1432,8 +1802,10 @@ psb_status psb_batch_free(psb_batch *b) {
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   if (b->side) cudaStreamDestroy(b->side);
+  if (b->side2) cudaStreamDestroy(b->side2);
   if (b->fork) cudaEventDestroy(b->fork);
   if (b->join) cudaEventDestroy(b->join);
+  if (b->join2) cudaEventDestroy(b->join2);
   delete b;
   return PSB_OK;
 }

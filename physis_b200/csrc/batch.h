@@ -22,6 +22,8 @@ struct BatchMemberHost {
   int64_t points = 0;      // lattice updates per step
   int force_tx = 0;        // autotuner trials: consumer threads along x (0: choose)
   int force_zc = 0;        // autotuner trials: planes per item (0: choose)
+  int force_td = 0;        // autotuner trials: Himeno sweeps per pass, 1 or 2 (0: choose)
+  int cur0 = 0;            // which of grids[0], grids[1] holds the state at the first step
 };
 
 }  // namespace psb
@@ -35,6 +37,9 @@ psb_status batch_launch_graph(psb_batch *b, cudaStream_t s, int64_t *launches);
 psb_status batch_add_member(psb_batch *b, const BatchMemberHost &m);
 psb_status batch_read_state(psb_batch *b, std::vector<int> &stop, std::vector<double> &res);
 bool batch_member_wavefront(const psb_batch *b, int i);
+// Which of member i's two grids holds its state after `done` local steps of
+// the last prepared launch.
+int batch_member_cur(const psb_batch *b, int i, int done);
 // Server access to a batch's member list (replaced every round).
 psb_batch *batch_new();
 void batch_set_members(psb_batch *b, const std::vector<BatchMemberHost> &m,

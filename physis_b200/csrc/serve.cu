@@ -61,6 +61,7 @@ struct SReq {
   bool complete = false;
   int skipped = 0;  // consecutive rounds this admitted request was left out of
   int wave_rounds = 0;  // rounds in which its steps overlapped as a wavefront
+  int cur = 0;          // which of its two state grids holds the current state
   BatchMemberHost h;
   double res[4] = {0, 0, 0, 0};
   cudaEvent_t copied = nullptr;
@@ -258,7 +259,7 @@ static psb_status retire_pack(psb_server *S, SReq *q) {
   Runtime &r = rt();
   q->stage = nullptr;
   if (q->status == PSB_OK && q->q.out && q->h.ngrids)
-    PSB_CHECK(pitched_stage_out(q->h.grids[q->steps_done & 1], &q->stage, r.stream));
+    PSB_CHECK(pitched_stage_out(q->h.grids[q->cur], &q->stage, r.stream));
   if (!q->copied) PSB_TRY(cudaEventCreateWithFlags(&q->copied, cudaEventDisableTiming));
   PSB_TRY(cudaEventRecord(q->copied, r.stream));
   return PSB_OK;
@@ -381,6 +382,7 @@ static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
   for (int i = 0; i < n; i++) {
     SReq *q = round_reqs[i];
     hm[i] = q->h;
+    hm[i].cur0 = q->cur;
     step0[i] = q->steps_done;
     steps[i] = q->cancel ? 0 : std::min(q->q.max_steps - q->steps_done, R);
     for (int k = 0; k < 4; k++) res_init[4 * i + k] = q->res[k];
@@ -454,7 +456,9 @@ static psb_status run_round(psb_server *S, std::vector<SReq *> &finished) {
   // Periodic writers keep the halo of their outputs current.
   for (int i = 0; i < n; i++) {
     SReq *q = round_reqs[i];
-    q->steps_done += stop[i] >= 0 ? stop[i] : steps[i];
+    const int done = stop[i] >= 0 ? stop[i] : steps[i];
+    q->cur = batch_member_cur(S->batch, i, done);
+    q->steps_done += done;
     for (int k = 0; k < 4; k++) q->res[k] = res[4 * i + k];
     q->residual = residual_of(q->res);
     if (q->kind == BK_DIFF7P)
@@ -618,6 +622,7 @@ static psb_status run_alone_plain(psb_server *S, SReq *q) {
   for (int i = 0; i < 2; i++)
     if (ms[i]) psb_stencil_free(ms[i]);
   if (q->cancel && st == PSB_OK) st = PSB_ERR_CANCELLED;
+  q->cur = q->steps_done & 1;  // this loop alternates the two maps step by step
   std::lock_guard<std::mutex> lk(S->mu);
   S->rounds++;
   S->launches += launches;

@@ -239,3 +239,97 @@ def test_batch_wavefront_with_residual_checks():
         b.free()
     finally:
         M.free()
+
+
+def _pow2(n):
+    b = 8
+    while b < n:
+        b <<= 1
+    return b
+
+
+def _two_sweep_entries(spec, zc=8):
+    """Tune entries that put every Himeno member of spec on two sweeps per pass
+    (batch bucket entries: kernel 100 + 2, extents rounded up to powers of 2)."""
+    for kind, dims, _ in spec:
+        if kind == "him":
+            ps.tune_set(102, ps.PS_FLOAT, tuple(_pow2(v) for v in dims), impl=ps.IMPL_TMA,
+                        tile_x=64, tile_y=8, z_chunk=zc, stages=6, t_depth=2)
+
+
+def _drop_entries(spec):
+    for kind, dims, _ in spec:
+        if kind == "him":
+            ps.tune_set(102, ps.PS_FLOAT, tuple(_pow2(v) for v in dims), impl=ps.IMPL_TMA,
+                        tile_x=64, tile_y=8, z_chunk=8, stages=6, t_depth=1)
+
+
+TWO_SWEEP_MEMBERS = [
+    ("him", (160, 160, 160), 20),   # wavefront path
+    ("him", (70, 40, 33), 7),       # odd steps: a one-sweep last pass
+    ("him", (33, 20, 65), 2),
+    ("diffp", (48, 20, 9), 10),
+    ("him", (130, 12, 18), 5),
+    ("diff", (64, 64, 64), 6),
+]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", [0, 1])
+def test_batch_two_sweep_himeno_bit_exact(mode):
+    """Himeno members on two sweeps per pass (the autotuner's t_depth 2) give
+    the oracle's fields bit for bit, in persistent and per-pass graph mode,
+    next to diffusion members on the single-step lists."""
+    spec = TWO_SWEEP_MEMBERS
+    M = Members(spec)
+    _two_sweep_entries(spec)
+    try:
+        b = M.batch()
+        b.run(mode)
+        for i, (kind, dims, steps) in enumerate(spec):
+            lay = b.layout(i)
+            done, _, g = b.result(i)
+            assert done == steps
+            if kind == "him":
+                assert lay["t_depth"] == 2 and lay["units"] == (steps + 1) // 2, (i, lay)
+            if i == 0:
+                assert lay["wavefront"] == 1
+            assert U.bits_equal(ps.PSGridCopyout(g), _want(kind, M.data[i], steps)), (mode, i, lay)
+        b.free()
+    finally:
+        _drop_entries(spec)
+        M.free()
+
+
+@pytest.mark.gpu
+def test_batch_two_sweep_himeno_checks_match_one_sweep():
+    """With residual checks (every 4 steps, and the first sweep) a pass never
+    straddles a check: stop steps, residuals and fields equal those of the
+    one-sweep list."""
+    spec = [("him", (96, 64, 40), 60), ("him", (40, 33, 33), 45), ("diff", (40, 40, 40), 30)]
+    stop = lambda i: ((0.05, 4), (0.08, 4), (0.0, 0))[i]
+    results = {}
+    for td in (1, 2):
+        M = Members(spec)
+        if td == 2:
+            _two_sweep_entries(spec)
+        try:
+            b = M.batch(stop)
+            b.run(0)
+            results[td] = []
+            for i in range(len(spec)):
+                done, res, g = b.result(i)
+                results[td].append((done, res, ps.PSGridCopyout(g), b.layout(i)["t_depth"]))
+            b.free()
+        finally:
+            _drop_entries(spec)
+            M.free()
+    for i, (kind, dims, steps) in enumerate(spec):
+        d1, r1, f1, t1 = results[1][i]
+        d2, r2, f2, t2 = results[2][i]
+        if kind == "him":
+            assert t1 == 1 and t2 == 2
+        assert 0 < d1 <= steps
+        assert d1 == d2 and r1 == pytest.approx(r2, rel=1e-12), (i, d1, d2, r1, r2)
+        assert U.bits_equal(f1, f2), i
+        assert U.bits_equal(f2, _want(kind, _inputs(kind, dims, 100 + i), d2)), i

@@ -249,3 +249,34 @@ def test_large_requests_take_the_wavefront_path():
         assert alone_recs[0]["steps_done"] == recs[i]["steps_done"]
         assert alone_recs[0]["wave_rounds"] >= 1
         assert bits_equal(alone_outs[0], want[i]), i
+
+
+def test_two_sweep_himeno_requests_match_one_sweep():
+    """Himeno requests served on two sweeps per pass (tune entries with
+    t_depth 2 for their size buckets) end with the same steps, residuals and
+    fields as on the one-sweep kernel (a pass flips which grid holds the
+    state; the server tracks it for the copy-out)."""
+    def bucket(dims):
+        return tuple(1 << max(3, (v - 1).bit_length()) for v in dims)
+
+    reqs = [dict(kernel=ps.HIMENO19, dims=(96, 80, 72), params=[0.8], max_steps=150, tol=0.02,
+                 check_every=10, seed=41),
+            dict(kernel=ps.HIMENO19, dims=(40, 36, 30), params=[0.8], max_steps=33, seed=42),
+            dict(kernel=ps.DIFFUSION7, dims=(50, 40, 30), params=list(COEF), max_steps=40,
+                 seed=43)]
+    base = _serve(reqs)
+    try:
+        for r in reqs:
+            if r["kernel"] == ps.HIMENO19:
+                ps.tune_set(102, ps.PS_FLOAT, bucket(r["dims"]), impl=ps.IMPL_TMA, tile_x=64,
+                            tile_y=8, z_chunk=8, stages=6, t_depth=2)
+        two = _serve(reqs)
+    finally:
+        for r in reqs:
+            if r["kernel"] == ps.HIMENO19:
+                ps.tune_set(102, ps.PS_FLOAT, bucket(r["dims"]), impl=ps.IMPL_TMA, tile_x=64,
+                            tile_y=8, z_chunk=8, stages=6, t_depth=1)
+    for a, b, oa, ob in zip(base[0], two[0], base[1], two[1]):
+        assert a["steps_done"] == b["steps_done"]
+        assert b["residual"] == pytest.approx(a["residual"], rel=1e-12)
+        assert bits_equal(oa, ob)
