@@ -1041,12 +1041,45 @@ def c5_numerics(ps, trace, served, shared, arena, max_work=5e8):
                                     "after the steps each was served" % max_work)
 
 
+def c5_tune(ps, trace):
+    """Autotune the batch size buckets the trace's requests fall in: one
+    representative member per (kind, bucket), on its own grids, through
+    psb_batch_autotune (the entries are cached for the server's rounds)."""
+    def bucket(side):
+        return 1 << max(3, (side - 1).bit_length())
+    seen, members = set(), []
+    for _, kind, side, _ in trace:
+        key = (kind, bucket(side))
+        if key not in seen:
+            seen.add(key)
+            members.append((kind, side))
+    b = ps.Batch()
+    grids = []
+    try:
+        for kind, side in members:
+            n = 14 if kind == "him" else 2
+            gs = [ps.grid_new(ps.PS_FLOAT, (side,) * 3) for _ in range(n)]
+            grids.append(gs)
+            if kind == "him":
+                b.add(ps.HIMENO19, gs, [0.8], 8)
+            else:
+                b.add(ps.DIFFUSION7, gs, COEF, 8)
+        b.autotune(force=True)
+    finally:
+        b.free()
+        for gs in grids:
+            for g in gs:
+                ps.PSGridFree(g)
+    return len(members)
+
+
 def run_c5(args, dist):
     os.environ["PHYSIS_B200_DEVICE"] = str(dist.local)
     import ctypes
     import physis_b200 as ps
     ps.PSInit()
     trace = c5_trace(count=args.c5_requests)
+    tuned_buckets = c5_tune(ps, trace) if args.tune else None
 
     def pinned(n):
         hp = ctypes.c_void_p()
@@ -1089,6 +1122,10 @@ def run_c5(args, dist):
         "config": {"workload": describe("c5"), "step": "one served solve (request)",
                    "requests": n, "trace_seed": 5005, "arrival_rate_per_s": C5_RATE,
                    "budget_bytes": C5_BUDGET,
+                   "tiles": "per member size bucket from the batch autotuner's table where it "
+                            "has an entry (tile shape, z chunk, Himeno sweeps per pass), else "
+                            "the fewest-tiles rule",
+                   "buckets_tuned_in_run": tuned_buckets,
                    "inputs": "diffusion u0 from pinned host memory (U[0,1)); Himeno p and "
                              "coefficients generated on the device from per-request seeds; "
                              "every final field copied back to pinned host memory",
