@@ -57,6 +57,13 @@ struct GtTable {
   GtFactor post;
   GtFactor a[PSB_MAX_TERMS];
   GtFactor b[PSB_MAX_TERMS];
+  // Every term one staged read times a constant (the common user stencil),
+  // no post factor: a packed form. word = (aligned offset << 8) |
+  // (coefficient is 1) << 5 | (offset mod V) << 3 | window plane; the read's
+  // V values of a row come from 16-byte-aligned loads shifted in registers.
+  int simple;
+  int word[PSB_MAX_TERMS];
+  double coef[PSB_MAX_TERMS];
 };
 
 struct GtMaps {
@@ -104,6 +111,48 @@ __device__ __forceinline__ GtBlk<T> gt_load(int kind, int k, int off, double c,
 #pragma unroll
     for (int v = 0; v < V; v++) out.v[r][v] = p[r * bx + v];
   return out;
+}
+
+// The V values at p + sh .. p + sh + V - 1 of one row (p 16-byte aligned),
+// from at most two aligned loads.
+__device__ __forceinline__ void gt_row(const float *p, int sh, float (&o)[4]) {
+  if (sh == 0) {
+    const float4 a = *reinterpret_cast<const float4 *>(p);
+    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
+  } else if (sh == 1) {
+    const float4 a = *reinterpret_cast<const float4 *>(p);
+    o[0] = a.y; o[1] = a.z; o[2] = a.w; o[3] = p[4];
+  } else if (sh == 2) {
+    const float2 a = *reinterpret_cast<const float2 *>(p + 2);
+    const float2 b = *reinterpret_cast<const float2 *>(p + 4);
+    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
+  } else {
+    const float4 b = *reinterpret_cast<const float4 *>(p + 4);
+    o[0] = p[3]; o[1] = b.x; o[2] = b.y; o[3] = b.z;
+  }
+}
+
+__device__ __forceinline__ void gt_row(const double *p, int sh, double (&o)[2]) {
+  if (sh == 0) {
+    const double2 a = *reinterpret_cast<const double2 *>(p);
+    o[0] = a.x; o[1] = a.y;
+  } else {
+    const double2 b = *reinterpret_cast<const double2 *>(p + 2);
+    o[0] = p[1]; o[1] = b.x;
+  }
+}
+
+// c times the V values of a row, each product rounded (packed for float).
+__device__ __forceinline__ void gt_scale(float c, float (&o)[4]) {
+  const float2 cc = make_float2(c, c);
+  const float2 lo = __fmul2_rn(cc, make_float2(o[0], o[1]));
+  const float2 hi = __fmul2_rn(cc, make_float2(o[2], o[3]));
+  o[0] = lo.x; o[1] = lo.y; o[2] = hi.x; o[3] = hi.y;
+}
+
+__device__ __forceinline__ void gt_scale(double c, double (&o)[2]) {
+  o[0] = xmul(c, o[0]);
+  o[1] = xmul(c, o[1]);
 }
 
 template <typename T>
@@ -191,6 +240,30 @@ __global__ void __launch_bounds__(kGtThreads) k_generic_tma(const __grid_constan
     }
     const int slot0 = i % S;
     GtBlk<T> acc;
+    if (tab.simple) {
+      for (int t = 0; t < tab.nterms; t++) {
+        const int w = tab.word[t];
+        int sl = slot0 + (w & 7);
+        if (sl >= S) sl -= S;
+        const T *p = reinterpret_cast<const T *>(ring + (size_t)sl * geo.stage_bytes) + (w >> 8) +
+                     thr_off;
+        const int sh = (w >> 3) & 3;
+        GtBlk<T> v;
+#pragma unroll
+        for (int r = 0; r < kGtVY; r++) {
+          gt_row(p + r * geo.bx, sh, v.v[r]);
+          if (!(w & 32)) gt_scale((T)tab.coef[t], v.v[r]);
+        }
+        if (t == 0) {
+          acc = v;
+        } else {
+#pragma unroll
+          for (int r = 0; r < kGtVY; r++)
+#pragma unroll
+            for (int k = 0; k < V; k++) acc.v[r][k] = xadd(acc.v[r][k], v.v[r][k]);
+        }
+      }
+    } else {
     for (int t = 0; t < tab.nterms; t++) {
       const GtFactor fa = tab.a[t], fb = tab.b[t];
       const GtBlk<T> va = gt_load<T>(fa.kind, fa.k, fa.off, fa.c, ring, geo.stage_bytes, S,
@@ -212,6 +285,7 @@ __global__ void __launch_bounds__(kGtThreads) k_generic_tma(const __grid_constan
 #pragma unroll
           for (int v = 0; v < V; v++) acc.v[r][v] = xadd(acc.v[r][v], p.v[r][v]);
       }
+    }
     }
     if (tab.has_post) {
       const GtFactor fp = tab.post;
@@ -359,6 +433,20 @@ static psb_status gt_launch(MapImpl &m, const psb_generic_stencil &desc, const G
     tab.b[t] = gt_compact(desc.terms[t].b, p, geo.plane_elems, geo.bx);
   }
   if (desc.has_post) tab.post = gt_compact(desc.post, p, geo.plane_elems, geo.bx);
+  // The packed form when every term is one read times a constant.
+  tab.simple = !desc.has_post;
+  for (int t = 0; t < desc.nterms && tab.simple; t++) {
+    const GtFactor &a = tab.a[t], &b = tab.b[t];
+    const bool ra = a.kind == 2, rb = b.kind == 2;
+    if (ra == rb) {
+      tab.simple = 0;
+      break;
+    }
+    const GtFactor &rd = ra ? a : b, &cf = ra ? b : a;
+    const int sh = rd.off & (V - 1);
+    tab.word[t] = ((rd.off - sh) << 8) | ((cf.kind == 1) << 5) | (sh << 3) | rd.k;
+    tab.coef[t] = cf.kind == 1 ? 1.0 : cf.c;
+  }
   const size_t smem = 128 + 512 + (size_t)geo.stages * geo.stage_bytes;
   if (smem > r.smem_optin) return PSB_ERR_UNSUPPORTED;
   static size_t configured[2] = {0, 0};
