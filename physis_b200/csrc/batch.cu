@@ -1664,33 +1664,54 @@ psb_status psb_batch_member_result(psb_batch *b, int member, int *steps_done, do
 // optimisation variants (translator/reference_translator.cc:749-1223).
 constexpr int kTuneSteps = 8;
 
+// Bytes of scratch grids the tuner may hold at once for one bucket.
+constexpr int64_t kTuneBytes = 4ll << 30;
+
 static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *best_cfg) {
   Runtime &r = rt();
   const int ng = h.ngrids;
-  std::vector<__PSGrid *> gs(ng, nullptr);
-  psb_status st = PSB_OK;
-  for (int i = 0; i < ng && st == PSB_OK; i++)
-    st = psb_grid_new(PS_FLOAT, 3, h.grids[0]->pub.dim, PSB_LAYOUT_PITCHED, &gs[i]);
-  for (int i = 0; i < ng && st == PSB_OK; i++)
-    st = psb_grid_fill(gs[i], 0, 7 + i, h.kind == BK_HIMENO && i == 5 ? 0.15 : 0.0,
-                       h.kind == BK_HIMENO && i == 5 ? 0.18 : 1.0);
-  psb_batch *tb = batch_new();
-  BatchMemberHost t = h;
-  for (int i = 0; i < ng; i++) t.grids[i] = gs[i] ? as_impl(gs[i]) : nullptr;
-  t.steps = kTuneSteps;
-  t.check_every = 0;
-  t.tol = 0;
-  if (st == PSB_OK && h.kind == BK_DIFF7P)
-    st = launch_halo_fill(t.grids[0], PSB_BOUNDARY_PERIODIC, r.stream);
+  const int *dim = h.grids[0]->pub.dim;
   const int rows_per_thread = h.kind == BK_HIMENO ? 1 : kVY;
   std::vector<int> txs = {8, 11, 16, 21, 32};
   int heur_tx = 0, heur_ty = 0;
   if (h.kind == BK_HIMENO)
-    pick_shape(h.grids[0]->pub.dim[0] - 1, h.grids[0]->pub.dim[1] - 2, 1, &heur_tx, &heur_ty);
+    pick_shape(dim[0] - 1, dim[1] - 2, 1, &heur_tx, &heur_ty);
   else
-    pick_shape(h.grids[0]->pub.dim[0], h.grids[0]->pub.dim[1], kVY, &heur_tx, &heur_ty);
+    pick_shape(dim[0], dim[1], kVY, &heur_tx, &heur_ty);
   if (std::find(txs.begin(), txs.end(), heur_tx) == txs.end()) txs.push_back(heur_tx);
-  const int nz = h.grids[0]->pub.dim[2] - (h.kind == BK_HIMENO ? 2 : 0);
+  const int nz = dim[2] - (h.kind == BK_HIMENO ? 2 : 0);
+  // A member is timed the way it runs inside a full batch: enough identical
+  // copies that one launch holds about two waves of items at the longest z
+  // chunk (a lone small member would favour short chunks and narrow tiles
+  // that a full batch does not need), within kTuneBytes of scratch grids.
+  int tx_h = 0, ty_h = 0;
+  pick_shape(dim[0], dim[1], rows_per_thread, &tx_h, &ty_h);
+  const int64_t tiles64 = (int64_t)((dim[0] + tx_h * 4 - 1) / (tx_h * 4)) *
+                          ((dim[1] + ty_h * rows_per_thread - 1) / (ty_h * rows_per_thread)) *
+                          ((nz + 63) / 64);
+  const int64_t grid_bytes = (int64_t)(h.grids[0]->alloc_bytes);
+  int copies = (int)std::min<int64_t>(256, (2 * items_target() + tiles64 - 1) / tiles64);
+  copies = (int)std::max<int64_t>(1, std::min<int64_t>(copies, kTuneBytes / (grid_bytes * ng)));
+  std::vector<__PSGrid *> gs((size_t)ng * copies, nullptr);
+  psb_status st = PSB_OK;
+  for (size_t i = 0; i < gs.size() && st == PSB_OK; i++)
+    st = psb_grid_new(PS_FLOAT, 3, dim, PSB_LAYOUT_PITCHED, &gs[i]);
+  for (size_t i = 0; i < gs.size() && st == PSB_OK; i++) {
+    const int f = (int)(i % ng);
+    st = psb_grid_fill(gs[i], 0, 7 + f, h.kind == BK_HIMENO && f == 5 ? 0.15 : 0.0,
+                       h.kind == BK_HIMENO && f == 5 ? 0.18 : 1.0);
+  }
+  psb_batch *tb = batch_new();
+  std::vector<BatchMemberHost> ts(copies, h);
+  for (int c = 0; c < copies; c++) {
+    BatchMemberHost &t = ts[c];
+    for (int i = 0; i < ng; i++) t.grids[i] = gs[(size_t)c * ng + i] ? as_impl(gs[(size_t)c * ng + i]) : nullptr;
+    t.steps = kTuneSteps;
+    t.check_every = 0;
+    t.tol = 0;
+    if (st == PSB_OK && h.kind == BK_DIFF7P)
+      st = launch_halo_fill(t.grids[0], PSB_BOUNDARY_PERIODIC, r.stream);
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (st == PSB_OK && cudaEventCreate(&e0) != cudaSuccess) st = PSB_ERR_CUDA;
   if (st == PSB_OK && cudaEventCreate(&e1) != cudaSuccess) st = PSB_ERR_CUDA;
@@ -1706,11 +1727,13 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
       if (st != PSB_OK) break;
       if (zc > 2 * std::max(nz, 2)) continue;
       if (td == 2 && zc < 8) continue;
-      t.force_tx = tx;
-      t.force_zc = zc;
-      t.force_td = td;
-      batch_set_members(tb, {t}, {});
-      st = batch_prepare(tb, {kTuneSteps}, {0});
+      for (auto &t : ts) {
+        t.force_tx = tx;
+        t.force_zc = zc;
+        t.force_td = td;
+      }
+      batch_set_members(tb, ts, {});
+      st = batch_prepare(tb, std::vector<int>(copies, kTuneSteps), std::vector<int>(copies, 0));
       double ms_best = -1;
       for (int rep = 0; rep < 3 && st == PSB_OK; rep++) {
         int64_t launches = 0;
