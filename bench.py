@@ -547,9 +547,10 @@ def run_ours(args):
     # step; with two steps per launch (temporal blocking) it is the effective
     # bandwidth and may exceed the copy peak.
     achieved = bpl * pts_per_step * args.steps / dev_s / 1e9
-    kname_traffic = "k_himeno_tma" if kname == "himeno" else "k_generic_tma_f32" if \
-        kname == "generic27" else (
-        "k_diff7_tma_f32" if dt == np.float32 else "k_diff7_tma_f64")
+    two_sweeps = kname == "himeno" and tune is not None and tune.get("t_depth") == 2
+    kname_traffic = ("k_himeno_tb2" if two_sweeps else "k_himeno_tma") if kname == "himeno" else \
+        "k_generic_tma_f32" if kname == "generic27" else (
+        "k_diff7_tma_f32" if dt == np.float32 else "k_diff7_tma_f64") + ("_fma" if fma else "")
     if args.plain:
         kname_traffic = kname_traffic.replace("tma", "plain")
     traffic = load_traffic("%s_%dx%dx%d" % (kname_traffic, nx, ny, nz))
