@@ -36,7 +36,7 @@ namespace psb {
 
 constexpr int kGtMaxGrids = 4;   // distinct grids read through TMA
 constexpr int kGtR = 2;          // largest |offset| per axis (the pitched halo)
-constexpr int kGtVY = 2;         // rows per consumer thread
+constexpr int kGtVY = 4;         // rows per consumer thread
 constexpr int kGtConsumers = 128;
 constexpr int kGtThreads = kGtConsumers + 32;
 
@@ -58,9 +58,13 @@ struct GtTable {
   GtFactor a[PSB_MAX_TERMS];
   GtFactor b[PSB_MAX_TERMS];
   // Every term one staged read times a constant (the common user stencil),
-  // no post factor: a packed form. word = (aligned offset << 8) |
-  // (coefficient is 1) << 5 | (offset mod V) << 3 | window plane; the read's
-  // V values of a row come from 16-byte-aligned loads shifted in registers.
+  // no post factor: a packed form. word = (row offset << 10) | (the run of
+  // terms on this row needs the previous lane's values) << 9 | (... the next
+  // lane's) << 8 | (coefficient is 1) << 7 | (first term of a run on a new
+  // row) << 6 | (dx + 2) << 3 | window plane. The row offset is the read's
+  // offset without its x part (a multiple of V): consecutive terms on the
+  // same row (same plane, grid and dy) reuse the row's values in registers,
+  // and x offsets shift them between lanes with warp shuffles.
   int simple;
   int word[PSB_MAX_TERMS];
   double coef[PSB_MAX_TERMS];
@@ -113,32 +117,66 @@ __device__ __forceinline__ GtBlk<T> gt_load(int kind, int k, int off, double c,
   return out;
 }
 
-// The V values at p + sh .. p + sh + V - 1 of one row (p 16-byte aligned),
-// from at most two aligned loads.
-__device__ __forceinline__ void gt_row(const float *p, int sh, float (&o)[4]) {
-  if (sh == 0) {
-    const float4 a = *reinterpret_cast<const float4 *>(p);
-    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
-  } else if (sh == 1) {
-    const float4 a = *reinterpret_cast<const float4 *>(p);
-    o[0] = a.y; o[1] = a.z; o[2] = a.w; o[3] = p[4];
-  } else if (sh == 2) {
-    const float2 a = *reinterpret_cast<const float2 *>(p + 2);
-    const float2 b = *reinterpret_cast<const float2 *>(p + 4);
-    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
-  } else {
-    const float4 b = *reinterpret_cast<const float4 *>(p + 4);
-    o[0] = p[3]; o[1] = b.x; o[2] = b.y; o[3] = b.z;
+// The values of one staged row around a thread's V points: its own aligned
+// vector a (x .. x+V-1), the first two values after it (the next lane's, or
+// loaded by the last lane) and the two before it (the previous lane's, or
+// loaded by lane 0): ext = [p0 p1 a0 .. aV-1 n0 n1], so the term at x offset
+// dx takes ext[2 + dx + j] for its point j.
+template <typename T>
+struct GtRow {
+  T e[16 / sizeof(T) + 4];
+};
+
+template <typename T>
+__device__ __forceinline__ void gt_row_load(const T *p, int lane, bool need_n, bool need_p,
+                                            GtRow<T> &r) {
+  constexpr int V = 16 / sizeof(T);
+  const Vec16<T> a = lds16(p);
+#pragma unroll
+  for (int j = 0; j < V; j++) r.e[2 + j] = a.v[j];
+  if (need_n) {
+    r.e[V + 2] = __shfl_down_sync(0xffffffffu, a.v[0], 1);
+    r.e[V + 3] = __shfl_down_sync(0xffffffffu, a.v[1], 1);
+    if (lane == 31) {
+      r.e[V + 2] = p[V];
+      r.e[V + 3] = p[V + 1];
+    }
+  }
+  if (need_p) {
+    r.e[0] = __shfl_up_sync(0xffffffffu, a.v[V - 2], 1);
+    r.e[1] = __shfl_up_sync(0xffffffffu, a.v[V - 1], 1);
+    if (lane == 0) {
+      r.e[0] = p[-2];
+      r.e[1] = p[-1];
+    }
   }
 }
 
-__device__ __forceinline__ void gt_row(const double *p, int sh, double (&o)[2]) {
-  if (sh == 0) {
-    const double2 a = *reinterpret_cast<const double2 *>(p);
-    o[0] = a.x; o[1] = a.y;
-  } else {
-    const double2 b = *reinterpret_cast<const double2 *>(p + 2);
-    o[0] = p[1]; o[1] = b.x;
+// The term's V values: ext[2 + dx + j] (dx uniform across the warp).
+template <typename T>
+__device__ __forceinline__ void gt_row_pick(const GtRow<T> &r, int dxp2, T (&o)[16 / sizeof(T)]) {
+  constexpr int V = 16 / sizeof(T);
+  switch (dxp2) {
+    case 0:
+#pragma unroll
+      for (int j = 0; j < V; j++) o[j] = r.e[j];
+      break;
+    case 1:
+#pragma unroll
+      for (int j = 0; j < V; j++) o[j] = r.e[j + 1];
+      break;
+    case 2:
+#pragma unroll
+      for (int j = 0; j < V; j++) o[j] = r.e[j + 2];
+      break;
+    case 3:
+#pragma unroll
+      for (int j = 0; j < V; j++) o[j] = r.e[j + 3];
+      break;
+    default:
+#pragma unroll
+      for (int j = 0; j < V; j++) o[j] = r.e[j + 4];
+      break;
   }
 }
 
@@ -156,7 +194,7 @@ __device__ __forceinline__ void gt_scale(double c, double (&o)[2]) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kGtThreads) k_generic_tma(const __grid_constant__ GtMaps maps,
+__global__ void __launch_bounds__(kGtThreads, 3) k_generic_tma(const __grid_constant__ GtMaps maps,
                                                             const __grid_constant__ GtTable tab,
                                                             GridView out, Dom3 d,
                                                             const __grid_constant__ GtGeom geo,
@@ -241,18 +279,24 @@ __global__ void __launch_bounds__(kGtThreads) k_generic_tma(const __grid_constan
     const int slot0 = i % S;
     GtBlk<T> acc;
     if (tab.simple) {
+      GtRow<T> row[kGtVY];
       for (int t = 0; t < tab.nterms; t++) {
         const int w = tab.word[t];
-        int sl = slot0 + (w & 7);
-        if (sl >= S) sl -= S;
-        const T *p = reinterpret_cast<const T *>(ring + (size_t)sl * geo.stage_bytes) + (w >> 8) +
-                     thr_off;
-        const int sh = (w >> 3) & 3;
+        if (w & 64) {  // a new row: its values into registers
+          int sl = slot0 + (w & 7);
+          if (sl >= S) sl -= S;
+          const T *p = reinterpret_cast<const T *>(ring + (size_t)sl * geo.stage_bytes) +
+                       (w >> 10) + thr_off;
+#pragma unroll
+          for (int r = 0; r < kGtVY; r++)
+            gt_row_load(p + r * geo.bx, lane, (w >> 8) & 1, (w >> 9) & 1, row[r]);
+        }
+        const int dxp2 = (w >> 3) & 7;
         GtBlk<T> v;
 #pragma unroll
         for (int r = 0; r < kGtVY; r++) {
-          gt_row(p + r * geo.bx, sh, v.v[r]);
-          if (!(w & 32)) gt_scale((T)tab.coef[t], v.v[r]);
+          gt_row_pick(row[r], dxp2, v.v[r]);
+          if (!(w & 128)) gt_scale((T)tab.coef[t], v.v[r]);
         }
         if (t == 0) {
           acc = v;
@@ -435,17 +479,25 @@ static psb_status gt_launch(MapImpl &m, const psb_generic_stencil &desc, const G
   if (desc.has_post) tab.post = gt_compact(desc.post, p, geo.plane_elems, geo.bx);
   // The packed form when every term is one read times a constant.
   tab.simple = !desc.has_post;
-  for (int t = 0; t < desc.nterms && tab.simple; t++) {
-    const GtFactor &a = tab.a[t], &b = tab.b[t];
-    const bool ra = a.kind == 2, rb = b.kind == 2;
-    if (ra == rb) {
-      tab.simple = 0;
-      break;
+  for (int t = 0; t < desc.nterms && tab.simple; t++)
+    if ((tab.a[t].kind == 2) == (tab.b[t].kind == 2)) tab.simple = 0;
+  if (tab.simple) {
+    // Runs of consecutive terms on the same row (plane, grid, dy) share one
+    // load; each run records whether it needs the neighbouring lanes.
+    int run_start = 0;
+    for (int t = 0; t < desc.nterms; t++) {
+      const GtFactor &rd = tab.a[t].kind == 2 ? tab.a[t] : tab.b[t];
+      const GtFactor &cf = tab.a[t].kind == 2 ? tab.b[t] : tab.a[t];
+      const int dx = desc.terms[t].a.grid >= 0 ? desc.terms[t].a.offset[0]
+                                               : desc.terms[t].b.offset[0];
+      const int rowoff = rd.off - dx;
+      const bool fresh = t == 0 || rowoff != (tab.word[t - 1] >> 10) || rd.k != (tab.word[t - 1] & 7);
+      if (fresh) run_start = t;
+      tab.word[t] = (rowoff << 10) | ((cf.kind == 1) << 7) | (fresh << 6) | ((dx + 2) << 3) | rd.k;
+      tab.coef[t] = cf.kind == 1 ? 1.0 : cf.c;
+      if (dx > 0) tab.word[run_start] |= 1 << 8;
+      if (dx < 0) tab.word[run_start] |= 1 << 9;
     }
-    const GtFactor &rd = ra ? a : b, &cf = ra ? b : a;
-    const int sh = rd.off & (V - 1);
-    tab.word[t] = ((rd.off - sh) << 8) | ((cf.kind == 1) << 5) | (sh << 3) | rd.k;
-    tab.coef[t] = cf.kind == 1 ? 1.0 : cf.c;
   }
   const size_t smem = 128 + 512 + (size_t)geo.stages * geo.stage_bytes;
   if (smem > r.smem_optin) return PSB_ERR_UNSUPPORTED;
