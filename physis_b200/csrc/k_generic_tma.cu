@@ -67,7 +67,8 @@ struct GtTable {
   // and x offsets shift them between lanes with warp shuffles.
   int simple;
   int word[PSB_MAX_TERMS];
-  double coef[PSB_MAX_TERMS];
+  double coef[PSB_MAX_TERMS];    // the constant factor in double grids' arithmetic
+  float coef32[PSB_MAX_TERMS];   // ... converted to float once, for float grids
 };
 
 struct GtMaps {
@@ -152,32 +153,73 @@ __device__ __forceinline__ void gt_row_load(const T *p, int lane, bool need_n, b
   }
 }
 
-// The term's V values: ext[2 + dx + j] (dx uniform across the warp).
-template <typename T>
-__device__ __forceinline__ void gt_row_pick(const GtRow<T> &r, int dxp2, T (&o)[16 / sizeof(T)]) {
-  constexpr int V = 16 / sizeof(T);
-  switch (dxp2) {
-    case 0:
+// One packed-form term on the cached rows: the window ext[DXP2 + j] (x
+// offset DXP2 - 2), times c unless ONE, added to the running sum (FIRST:
+// starts it, as the reference's sum starts from its first term). Float
+// products go in pairs through the sm_100 f32x2 multiply (each lane rounded
+// like the scalar one); the sums stay scalar.
+template <int DXP2, bool ONE, bool FIRST>
+__device__ __forceinline__ void gt_term(const GtRow<float> (&row)[kGtVY], float c,
+                                        GtBlk<float> &acc) {
+  const float2 cc = make_float2(c, c);
 #pragma unroll
-      for (int j = 0; j < V; j++) o[j] = r.e[j];
-      break;
-    case 1:
-#pragma unroll
-      for (int j = 0; j < V; j++) o[j] = r.e[j + 1];
-      break;
-    case 2:
-#pragma unroll
-      for (int j = 0; j < V; j++) o[j] = r.e[j + 2];
-      break;
-    case 3:
-#pragma unroll
-      for (int j = 0; j < V; j++) o[j] = r.e[j + 3];
-      break;
-    default:
-#pragma unroll
-      for (int j = 0; j < V; j++) o[j] = r.e[j + 4];
-      break;
+  for (int r = 0; r < kGtVY; r++) {
+    float2 lo = make_float2(row[r].e[DXP2], row[r].e[DXP2 + 1]);
+    float2 hi = make_float2(row[r].e[DXP2 + 2], row[r].e[DXP2 + 3]);
+    if (!ONE) {
+      lo = __fmul2_rn(cc, lo);
+      hi = __fmul2_rn(cc, hi);
+    }
+    if (FIRST) {
+      acc.v[r][0] = lo.x;
+      acc.v[r][1] = lo.y;
+      acc.v[r][2] = hi.x;
+      acc.v[r][3] = hi.y;
+    } else {  // scalar adds: a packed add may be fused with the packed multiply
+      acc.v[r][0] = xadd(acc.v[r][0], lo.x);
+      acc.v[r][1] = xadd(acc.v[r][1], lo.y);
+      acc.v[r][2] = xadd(acc.v[r][2], hi.x);
+      acc.v[r][3] = xadd(acc.v[r][3], hi.y);
+    }
   }
+}
+
+template <int DXP2, bool ONE, bool FIRST>
+__device__ __forceinline__ void gt_term(const GtRow<double> (&row)[kGtVY], double c,
+                                        GtBlk<double> &acc) {
+#pragma unroll
+  for (int r = 0; r < kGtVY; r++)
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+      double v = row[r].e[DXP2 + j];
+      if (!ONE) v = xmul(c, v);
+      acc.v[r][j] = FIRST ? v : xadd(acc.v[r][j], v);
+    }
+}
+
+// key = (dx + 2) | (coefficient is 1) << 3, uniform across the warp.
+template <bool FIRST, typename T>
+__device__ __forceinline__ void gt_term_key(int key, const GtRow<T> (&row)[kGtVY], T c,
+                                            GtBlk<T> &acc) {
+  switch (key) {
+    case 0: gt_term<0, false, FIRST>(row, c, acc); break;
+    case 1: gt_term<1, false, FIRST>(row, c, acc); break;
+    case 2: gt_term<2, false, FIRST>(row, c, acc); break;
+    case 3: gt_term<3, false, FIRST>(row, c, acc); break;
+    case 4: gt_term<4, false, FIRST>(row, c, acc); break;
+    case 8: gt_term<0, true, FIRST>(row, c, acc); break;
+    case 9: gt_term<1, true, FIRST>(row, c, acc); break;
+    case 10: gt_term<2, true, FIRST>(row, c, acc); break;
+    case 11: gt_term<3, true, FIRST>(row, c, acc); break;
+    default: gt_term<4, true, FIRST>(row, c, acc); break;
+  }
+}
+
+__device__ __forceinline__ float gt_coef(const GtTable &tab, int t, float) {
+  return tab.coef32[t];
+}
+__device__ __forceinline__ double gt_coef(const GtTable &tab, int t, double) {
+  return tab.coef[t];
 }
 
 // c times the V values of a row, each product rounded (packed for float).
@@ -194,7 +236,7 @@ __device__ __forceinline__ void gt_scale(double c, double (&o)[2]) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(kGtThreads, 3) k_generic_tma(const __grid_constant__ GtMaps maps,
+__global__ void __launch_bounds__(kGtThreads, sizeof(T) == 4 ? 4 : 3) k_generic_tma(const __grid_constant__ GtMaps maps,
                                                             const __grid_constant__ GtTable tab,
                                                             GridView out, Dom3 d,
                                                             const __grid_constant__ GtGeom geo,
@@ -280,32 +322,22 @@ __global__ void __launch_bounds__(kGtThreads, 3) k_generic_tma(const __grid_cons
     GtBlk<T> acc;
     if (tab.simple) {
       GtRow<T> row[kGtVY];
-      for (int t = 0; t < tab.nterms; t++) {
+      auto load_rows = [&](int w) {
+        int sl = slot0 + (w & 7);
+        if (sl >= S) sl -= S;
+        const T *p = reinterpret_cast<const T *>(ring + (size_t)sl * geo.stage_bytes) +
+                     (w >> 10) + thr_off;
+#pragma unroll
+        for (int r = 0; r < kGtVY; r++)
+          gt_row_load(p + r * geo.bx, lane, (w >> 8) & 1, (w >> 9) & 1, row[r]);
+      };
+      const int w0 = tab.word[0];
+      load_rows(w0);
+      gt_term_key<true>(((w0 >> 3) & 7) | ((w0 >> 4) & 8), row, gt_coef(tab, 0, T()), acc);
+      for (int t = 1; t < tab.nterms; t++) {
         const int w = tab.word[t];
-        if (w & 64) {  // a new row: its values into registers
-          int sl = slot0 + (w & 7);
-          if (sl >= S) sl -= S;
-          const T *p = reinterpret_cast<const T *>(ring + (size_t)sl * geo.stage_bytes) +
-                       (w >> 10) + thr_off;
-#pragma unroll
-          for (int r = 0; r < kGtVY; r++)
-            gt_row_load(p + r * geo.bx, lane, (w >> 8) & 1, (w >> 9) & 1, row[r]);
-        }
-        const int dxp2 = (w >> 3) & 7;
-        GtBlk<T> v;
-#pragma unroll
-        for (int r = 0; r < kGtVY; r++) {
-          gt_row_pick(row[r], dxp2, v.v[r]);
-          if (!(w & 128)) gt_scale((T)tab.coef[t], v.v[r]);
-        }
-        if (t == 0) {
-          acc = v;
-        } else {
-#pragma unroll
-          for (int r = 0; r < kGtVY; r++)
-#pragma unroll
-            for (int k = 0; k < V; k++) acc.v[r][k] = xadd(acc.v[r][k], v.v[r][k]);
-        }
+        if (w & 64) load_rows(w);  // a new row: its values into registers
+        gt_term_key<false>(((w >> 3) & 7) | ((w >> 4) & 8), row, gt_coef(tab, t, T()), acc);
       }
     } else {
     for (int t = 0; t < tab.nterms; t++) {
@@ -495,6 +527,7 @@ static psb_status gt_launch(MapImpl &m, const psb_generic_stencil &desc, const G
       if (fresh) run_start = t;
       tab.word[t] = (rowoff << 10) | ((cf.kind == 1) << 7) | (fresh << 6) | ((dx + 2) << 3) | rd.k;
       tab.coef[t] = cf.kind == 1 ? 1.0 : cf.c;
+      tab.coef32[t] = (float)tab.coef[t];
       if (dx > 0) tab.word[run_start] |= 1 << 8;
       if (dx < 0) tab.word[run_start] |= 1 << 9;
     }
