@@ -860,6 +860,15 @@ def run_c4(args, dist):
     members = c4_members(count=args.members)
     if args.c4_kind:
         members = [m for m in members if m[0] == args.c4_kind]
+    if args.c4_cube:
+        members = [(k, (args.c4_cube,) * 3, st) for k, _, st in members]
+    if args.c4_steps:
+        members = [(k, d, args.c4_steps) for k, d, _ in members]
+    if args.c4_him_two_sweeps:
+        for k, d, _ in members:
+            if k == "him":
+                ps.batch_tune_set(ps.HIMENO19, d, impl=ps.IMPL_TMA, tile_x=64, tile_y=8, z_chunk=0,
+                                  stages=6, t_depth=2)
     grids = c4_build(ps, members)
     b = c4_batch(ps, members, grids)
     if args.tune:
@@ -939,6 +948,13 @@ def run_c4(args, dist):
         "cpu_baseline": cpu,
         "numerics": numerics,
     }
+    overrides = {k: v for k, v in (("members", args.members if args.members != 256 else None),
+                                   ("kind", args.c4_kind), ("cube", args.c4_cube),
+                                   ("steps", args.c4_steps),
+                                   ("himeno_two_sweeps", args.c4_him_two_sweeps or None))
+                 if v is not None}
+    if overrides:
+        line["config"]["profiling_overrides"] = overrides
     b.free()
     for g in grids:
         for x in g:
@@ -1358,6 +1374,12 @@ def main():
     ap.add_argument("--members", type=int, default=256, help="c4: batch members (profiling)")
     ap.add_argument("--skip-loops", action="store_true", help="c4: skip the per-grid loops")
     ap.add_argument("--skip-graph", action="store_true", help="c4: skip the per-step graph mode")
+    ap.add_argument("--c4-cube", type=int, default=None,
+                    help="c4: every member a cube of this side (kinds and steps kept; profiling)")
+    ap.add_argument("--c4-steps", type=int, default=None,
+                    help="c4: every member this many steps (profiling)")
+    ap.add_argument("--c4-him-two-sweeps", action="store_true",
+                    help="c4: pin every Himeno bucket to two sweeps per pass (profiling)")
     ap.add_argument("--c4-kind", default=None, choices=["diffp", "him"],
                     help="c4: keep only one kind of member (profiling)")
     ap.add_argument("--c5-requests", type=int, default=128, help="c5: requests in the trace")

@@ -674,12 +674,22 @@ psb_status psb_batch_member_layout(psb_batch *b, int member, psb_batch_layout *l
 /* Autotune the batch's members (the reference tunes by trial at translation
  * time, translator/reference_translator.cc:749-1223): for each size bucket
  * -- member kind, element type and extents rounded up to powers of two --
- * without a cached entry (every bucket with force != 0), a scratch member
- * of those extents is timed alone in the persistent kernel over candidate
- * tile widths and z chunks; the fastest is cached in the tune table and its
- * JSON file and used by later mode-0/1 runs for every member of the bucket
- * (the members' own grids are not touched). */
+ * without a cached entry (every bucket with force != 0), copies of a
+ * scratch member of those extents are timed in the persistent kernel over
+ * candidate tile widths (Himeno: also two sweeps per pass), the z chunk
+ * following the batch's own rule; the fastest is cached in the tune table
+ * and its JSON file and used by later mode-0/1 runs for every member of the
+ * bucket (the members' own grids are not touched). */
 psb_status psb_batch_autotune(psb_batch *b, int force);
+/* Batch member shapes live in the tune table (psb_tune_set/psb_tune_get and
+ * its JSON cache) under kernel id PSB_BATCH_TUNE_BASE + kernel_id - 1, where
+ * kernel_id is the member's stencil (PSB_KERNEL_DIFFUSION7,
+ * _DIFFUSION7_PERIODIC or _HIMENO19), type PS_FLOAT, and the member's size
+ * bucket (each extent rounded up to a power of two, at least 8). A run
+ * uses tile_x (consumer threads along x = tile_x / 4) and, for Himeno,
+ * t_depth (2: two sweeps per pass of 64 x 8 tiles); the z chunk follows the
+ * batch's own rule. Setting an entry by hand pins the shape of a bucket. */
+#define PSB_BATCH_TUNE_BASE 100
 psb_status psb_batch_free(psb_batch *b);
 
 /* ------------------------------------------------------------------------ */

@@ -627,6 +627,27 @@ def tune_set(kernel, type_, dims, **cfg):
     check(lib.psb_tune_set(kernel, type_, d, ctypes.byref(c)), "psb_tune_set")
 
 
+PSB_BATCH_TUNE_BASE = 100
+
+
+def batch_bucket(dims):
+    """Size bucket of a batch member: each extent rounded up to a power of
+    two, at least 8."""
+    out = []
+    for n in dims:
+        b = 8
+        while b < n:
+            b <<= 1
+        out.append(b)
+    return out
+
+
+def batch_tune_set(kernel, dims, **cfg):
+    """Pin the shape of the batch members of stencil `kernel` whose size
+    bucket is that of `dims` (the PSB_BATCH_TUNE_BASE entry)."""
+    tune_set(PSB_BATCH_TUNE_BASE + kernel - 1, PS_FLOAT, batch_bucket(dims), **cfg)
+
+
 def himeno_residual_enable(m, history=1):
     check(lib.psb_himeno_residual_enable(m.handle, history), "psb_himeno_residual_enable")
 

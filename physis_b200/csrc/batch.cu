@@ -1724,15 +1724,16 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
   std::vector<std::array<int, 2>> cands;  // (tile width in threads, t_depth)
   for (int tx : txs) cands.push_back({tx, 1});
   if (h.kind == BK_HIMENO) cands.push_back({kHtTX / 4, 2});
+  // The z chunk is left to the batch's own rule (items per step over the
+  // whole work list), as in a real run: a chunk that wins for the copies
+  // alone is not the one a mixed batch would give this member.
   for (const auto &cd : cands) {
     const int tx = cd[0], td = cd[1];
-    for (int zc : {4, 8, 16, 32, 64}) {
+    {
       if (st != PSB_OK) break;
-      if (zc > 2 * std::max(nz, 2)) continue;
-      if (td == 2 && zc < 8) continue;
       for (auto &t : ts) {
         t.force_tx = tx;
-        t.force_zc = zc;
+        t.force_zc = 0;
         t.force_td = td;
       }
       batch_set_members(tb, ts, {});
@@ -1749,15 +1750,15 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
         if (rep > 0 && (ms_best < 0 || ms < ms_best)) ms_best = ms;  // rep 0 warms up
       }
       if (__ps_trace)
-        fprintf(__ps_trace, "physis_b200: batch tune kind=%d tile=%dx%d zc=%d t=%d: %.4f ms\n",
-                h.kind, tx * 4, td == 2 ? kHtTY : (kBConsumers / tx) * rows_per_thread, zc, td,
+        fprintf(__ps_trace, "physis_b200: batch tune kind=%d tile=%dx%d t=%d: %.4f ms\n",
+                h.kind, tx * 4, td == 2 ? kHtTY : (kBConsumers / tx) * rows_per_thread, td,
                 ms_best);
       if (st == PSB_OK && ms_best > 0 && (best < 0 || ms_best < best)) {
         best = ms_best;
         best_cfg->impl = PSB_IMPL_TMA;
         best_cfg->tile_x = tx * 4;
         best_cfg->tile_y = td == 2 ? kHtTY : (kBConsumers / tx) * rows_per_thread;
-        best_cfg->z_chunk = zc;
+        best_cfg->z_chunk = 0;  // the batch's rule
         best_cfg->stages = kBStages;
         best_cfg->t_depth = td;
       }

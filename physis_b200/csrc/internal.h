@@ -224,7 +224,7 @@ psb_status tune_lookup(int kernel, int type, const int *n, psb_tune_config *cfg)
 // Batched members are tuned per (kernel kind, element type, size bucket):
 // each extent rounded up to a power of two. Their entries live in the same
 // table and cache file under kernel id kBatchTuneBase + the member kind.
-constexpr int kBatchTuneBase = 100;
+constexpr int kBatchTuneBase = PSB_BATCH_TUNE_BASE;
 void batch_tune_bucket(const int *n, int *bucket);
 bool batch_tune_find(int kind, const int *n, psb_tune_config *cfg);
 void batch_tune_store(int kind, const int *n, const psb_tune_config &cfg);

@@ -36,7 +36,10 @@ namespace psb {
 
 constexpr int kGtMaxGrids = 4;   // distinct grids read through TMA
 constexpr int kGtR = 2;          // largest |offset| per axis (the pitched halo)
-constexpr int kGtVY = 4;         // rows per consumer thread
+#ifndef PSB_GT_VY
+#define PSB_GT_VY 4
+#endif
+constexpr int kGtVY = PSB_GT_VY;  // rows per consumer thread
 constexpr int kGtConsumers = 128;
 constexpr int kGtThreads = kGtConsumers + 32;
 

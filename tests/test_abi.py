@@ -135,3 +135,25 @@ def test_tune_cache_roundtrip(tmp_path, monkeypatch):
     out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
     assert "'tile_x': 128" in out.stdout
+
+
+def test_batch_tune_entries_use_the_header_base_and_buckets():
+    """ps.batch_tune_set writes the entry a batch member of that stencil and
+    size bucket reads: kernel id PSB_BATCH_TUNE_BASE + kernel_id - 1 (the
+    header's value), extents rounded up to powers of two, at least 8."""
+    import sys
+    import physis_b200 as ps
+    with open(os.path.join(ROOT, "include", "physis_b200.h")) as f:
+        base = int(re.search(r"#define PSB_BATCH_TUNE_BASE (\d+)", f.read()).group(1))
+    assert base == ps.PSB_BATCH_TUNE_BASE
+    assert ps.batch_bucket((3, 100, 257)) == [8, 128, 512]
+    assert ps.batch_bucket((8, 128, 512)) == [8, 128, 512]
+    code = (
+        "import physis_b200 as ps\n"
+        "ps.batch_tune_set(ps.HIMENO19, (100, 70, 33), impl=2, tile_x=64, tile_y=8,"
+        " z_chunk=0, stages=6, t_depth=2)\n"
+        "print(ps.tune_get(%d + ps.HIMENO19 - 1, ps.PS_FLOAT, (128, 128, 64)))\n" % base)
+    env = dict(os.environ, PHYSIS_B200_TUNE_CACHE=os.devnull, PYTHONPATH=ROOT)
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    assert "'t_depth': 2" in out.stdout and "'tile_x': 64" in out.stdout
