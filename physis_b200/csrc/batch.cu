@@ -1666,6 +1666,9 @@ psb_status psb_batch_member_result(psb_batch *b, int member, int *steps_done, do
 // bucket. The reference's counterpart is its translation-time trial of
 // optimisation variants (translator/reference_translator.cc:749-1223).
 constexpr int kTuneSteps = 8;
+// A fixed tile width or two sweeps per pass replaces the fewest-tiles rule
+// only if its trial takes at most this fraction of the rule's time.
+constexpr double kTuneMargin = 0.9;
 
 // Bytes of scratch grids the tuner may hold at once for one bucket.
 constexpr int64_t kTuneBytes = 4ll << 30;
@@ -1675,13 +1678,11 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
   const int ng = h.ngrids;
   const int *dim = h.grids[0]->pub.dim;
   const int rows_per_thread = h.kind == BK_HIMENO ? 1 : kVY;
-  std::vector<int> txs = {8, 11, 16, 21, 32};
-  int heur_tx = 0, heur_ty = 0;
-  if (h.kind == BK_HIMENO)
-    pick_shape(dim[0] - 1, dim[1] - 2, 1, &heur_tx, &heur_ty);
-  else
-    pick_shape(dim[0], dim[1], kVY, &heur_tx, &heur_ty);
-  if (std::find(txs.begin(), txs.end(), heur_tx) == txs.end()) txs.push_back(heur_tx);
+  // Candidate 0 is the fewest-tiles rule itself, which every member of the
+  // bucket applies to its own extents; a fixed width must beat it clearly,
+  // since it is timed on one member's extents and then given to the whole
+  // bucket.
+  const std::vector<int> txs = {0, 8, 11, 16, 21, 32};
   const int nz = dim[2] - (h.kind == BK_HIMENO ? 2 : 0);
   // A member is timed the way it runs inside a full batch: enough identical
   // copies that one launch holds about two waves of items at the longest z
@@ -1718,10 +1719,10 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (st == PSB_OK && cudaEventCreate(&e0) != cudaSuccess) st = PSB_ERR_CUDA;
   if (st == PSB_OK && cudaEventCreate(&e1) != cudaSuccess) st = PSB_ERR_CUDA;
-  double best = -1;
+  double best = -1, rule_ms = -1;
   // Himeno buckets also try two sweeps per pass (64 x 8 tiles), recorded as
   // t_depth 2 with tile_x 64.
-  std::vector<std::array<int, 2>> cands;  // (tile width in threads, t_depth)
+  std::vector<std::array<int, 2>> cands;  // (tile width in threads or 0, t_depth)
   for (int tx : txs) cands.push_back({tx, 1});
   if (h.kind == BK_HIMENO) cands.push_back({kHtTX / 4, 2});
   // The z chunk is left to the batch's own rule (items per step over the
@@ -1751,13 +1752,15 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
       }
       if (__ps_trace)
         fprintf(__ps_trace, "physis_b200: batch tune kind=%d tile=%dx%d t=%d: %.4f ms\n",
-                h.kind, tx * 4, td == 2 ? kHtTY : (kBConsumers / tx) * rows_per_thread, td,
-                ms_best);
-      if (st == PSB_OK && ms_best > 0 && (best < 0 || ms_best < best)) {
+                h.kind, tx * 4, td == 2 ? kHtTY : tx ? (kBConsumers / tx) * rows_per_thread : 0,
+                td, ms_best);
+      if (tx == 0 && td == 1) rule_ms = ms_best;
+      const double bar = tx == 0 && td == 1 ? best : std::min(best, kTuneMargin * rule_ms);
+      if (st == PSB_OK && ms_best > 0 && (best < 0 || ms_best < bar)) {
         best = ms_best;
         best_cfg->impl = PSB_IMPL_TMA;
-        best_cfg->tile_x = tx * 4;
-        best_cfg->tile_y = td == 2 ? kHtTY : (kBConsumers / tx) * rows_per_thread;
+        best_cfg->tile_x = tx * 4;  // 0: the fewest-tiles rule
+        best_cfg->tile_y = td == 2 ? kHtTY : tx ? (kBConsumers / tx) * rows_per_thread : 0;
         best_cfg->z_chunk = 0;  // the batch's rule
         best_cfg->stages = kBStages;
         best_cfg->t_depth = td;
