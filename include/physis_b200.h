@@ -657,8 +657,9 @@ psb_status psb_batch_member_result(psb_batch *b, int member, int *steps_done, do
  * its planes in z, the items of one step, and whether consecutive steps of
  * the member overlapped as a wavefront (1: an item waited only for the 27
  * items around it in the previous step; 0: for the whole previous step),
- * whether its tile shape came from the autotuner's table (1) or from the
- * fewest-tiles rule (0), the sweeps an item advances (t_depth: 2 for
+ * whether its bucket has an entry in the autotuner's table (1; the entry
+ * may keep the fewest-tiles rule) or not (0: the rule), the sweeps an item
+ * advances (t_depth: 2 for
  * Himeno members that run two sweeps per pass) and the member's units of
  * work in the launch (steps, or passes when t_depth is 2). PSB_ERR_INVALID
  * before the batch has run in mode 0 or 1. */

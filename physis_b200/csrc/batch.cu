@@ -882,6 +882,7 @@ struct MemberTune {
   int zc = 0;
   int td = 1;  // Himeno sweeps per pass
   bool forced = false;
+  bool tuned = false;  // from the bucket's tune entry (tx 0: the entry kept the rule)
 };
 
 static MemberTune member_tune(const BatchMemberHost &h) {
@@ -895,6 +896,7 @@ static MemberTune member_tune(const BatchMemberHost &h) {
   }
   psb_tune_config c;
   if (batch_tune_find(h.kind, h.grids[0]->pub.dim, &c)) {
+    t.tuned = true;
     t.tx = c.tile_x / 4;
     t.zc = c.z_chunk;
     t.td = c.t_depth;
@@ -1819,7 +1821,7 @@ psb_status psb_batch_member_layout(psb_batch *b, int member, psb_batch_layout *l
   layout->tiles = M.ntiles;
   layout->wavefront = batch_member_wavefront(b, member) ? 1 : 0;
   const MemberTune mt = member_tune(b->hm[member]);
-  layout->tuned = !mt.forced && mt.tx > 0 ? 1 : 0;
+  layout->tuned = mt.tuned ? 1 : 0;
   layout->t_depth = M.group == 2 ? 2 : 1;
   layout->units = M.group == 2 ? M.npasses : M.steps;
   return PSB_OK;
