@@ -39,6 +39,12 @@ constexpr int kGtR = 2;          // largest |offset| per axis (the pitched halo)
 #ifndef PSB_GT_VY
 #define PSB_GT_VY 4
 #endif
+// Products of the packed form: 2 all through the f32x2 multiply, 1 only at
+// even window offsets, 0 scalar (the results are the same; the instruction
+// counts differ).
+#ifndef PSB_GT_PACKED_MUL
+#define PSB_GT_PACKED_MUL 2
+#endif
 constexpr int kGtVY = PSB_GT_VY;  // rows per consumer thread
 constexpr int kGtConsumers = 128;
 constexpr int kGtThreads = kGtConsumers + 32;
@@ -170,8 +176,13 @@ __device__ __forceinline__ void gt_term(const GtRow<float> (&row)[kGtVY], float 
     float2 lo = make_float2(row[r].e[DXP2], row[r].e[DXP2 + 1]);
     float2 hi = make_float2(row[r].e[DXP2 + 2], row[r].e[DXP2 + 3]);
     if (!ONE) {
-      lo = __fmul2_rn(cc, lo);
-      hi = __fmul2_rn(cc, hi);
+      if (PSB_GT_PACKED_MUL == 2 || (PSB_GT_PACKED_MUL == 1 && DXP2 % 2 == 0)) {
+        lo = __fmul2_rn(cc, lo);
+        hi = __fmul2_rn(cc, hi);
+      } else {
+        lo = make_float2(xmul(c, lo.x), xmul(c, lo.y));
+        hi = make_float2(xmul(c, hi.x), xmul(c, hi.y));
+      }
     }
     if (FIRST) {
       acc.v[r][0] = lo.x;
