@@ -460,6 +460,19 @@ psb_status psb_generic_register(const psb_generic_stencil *desc, int *kernel_id)
  * every other form and every map under psb_set_impl(PSB_IMPL_PLAIN or
  * PSB_IMPL_GENERIC). */
 psb_status psb_generic_last_impl(int *impl);
+/* Whether the last TMA application of a generic stencil ran a kernel
+ * compiled at run time for its table (1) or the kernel that interprets the
+ * table (0). Tables whose every term is one grid read times a constant (no
+ * post factor) are compiled by NVRTC for sm_100a when the map first runs --
+ * the reference's translator likewise emits one kernel per stencil
+ * (translator/cuda_translator.cc:615-869) -- and cached per process for
+ * every table of the same shape (coefficients are launch arguments). Same
+ * arithmetic, same results; without NVRTC or the library's device headers
+ * (csrc/ beside lib/, or $PHYSIS_B200_CSRC) the interpreting kernel runs. */
+psb_status psb_generic_last_compiled(int *compiled);
+/* Run-time compilation of generic tables on (1, the default unless
+ * $PHYSIS_B200_GENERIC_COMPILE=0) or off (0). */
+psb_status psb_set_generic_compile(int on);
 
 /* Compiled stencils: a DSL stencil function (docs/programming.md:117-190 of
  * the reference: `const int` index parameters, grids, scalars;

@@ -249,6 +249,8 @@ def _load():
                                         ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_int)]),
         "psb_set_fp_mode": (S, [ctypes.c_int]),
+        "psb_set_generic_compile": (S, [ctypes.c_int]),
+        "psb_generic_last_compiled": (S, [ctypes.POINTER(ctypes.c_int)]),
         "psb_get_fp_mode": (S, [ctypes.POINTER(ctypes.c_int)]),
         "psb_batch_member_layout": (S, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchLayout)]),
         "psb_batch_autotune": (S, [ctypes.c_void_p, ctypes.c_int]),
@@ -597,6 +599,19 @@ def get_fp_mode():
     m = ctypes.c_int()
     check(lib.psb_get_fp_mode(ctypes.byref(m)), "psb_get_fp_mode")
     return m.value
+
+
+def set_generic_compile(on):
+    """Run-time compilation of generic tables on the TMA path (default on)."""
+    check(lib.psb_set_generic_compile(1 if on else 0), "psb_set_generic_compile")
+
+
+def generic_last_compiled():
+    """Whether the last TMA application of a generic stencil ran a kernel
+    compiled for its table."""
+    v = ctypes.c_int()
+    check(lib.psb_generic_last_compiled(ctypes.byref(v)), "psb_generic_last_compiled")
+    return bool(v.value)
 
 
 def set_graph(enable):

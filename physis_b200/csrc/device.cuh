@@ -2,11 +2,18 @@
 // bounded waits and periodic halo images.
 #pragma once
 
+#ifdef __CUDACC_RTC__
+// Compiled at run time: the library hands the compiler the fixed-width
+// integer types and the tensor-map type itself (rtc.cu).
+#include "psb_rtc_prelude.h"
+#include "views.h"
+#else
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "internal.h"
+#endif
 
 namespace psb {
 

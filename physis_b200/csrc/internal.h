@@ -12,28 +12,11 @@
 #include <vector>
 
 #include "../../include/physis_b200.h"
+#include "views.h"
 
 namespace psb {
 
-// ---------------------------------------------------------------------------
-// Device-side views
-// ---------------------------------------------------------------------------
-
-// A strided view of one grid: element (x, y, z) lives at
-// origin[x + y*sy + z*sz]. Dense grids have sy = nx, sz = nx*ny; pitched
-// grids have 128-byte rows and a resident halo around the origin.
-struct GridView {
-  void *origin;
-  int64_t sy, sz;
-  int n[3];
-  int type;      // PSPrimitiveType or -1 when unknown
-  int halo;      // cells of resident halo in every direction (0 for dense)
-};
-
-struct Dom3 {
-  int lo[3];
-  int hi[3];
-};
+// Device-side views (GridView, Dom3) are in views.h.
 
 // ---------------------------------------------------------------------------
 // Host-side objects
@@ -232,5 +215,17 @@ void tune_save();
 
 // Host monotonic seconds.
 double now_s();
+
+// Run-time compilation (rtc.cu): a kernel `name` compiled by NVRTC for
+// sm_100a from `source` (which may include the library's device headers),
+// cached per device and key; PSB_ERR_UNSUPPORTED when NVRTC, the headers or
+// the compile are unavailable (the caller keeps its own kernel).
+bool rtc_available();
+psb_status rtc_function(const std::string &key, const std::string &source, const char *name,
+                        const std::vector<std::string> &options, int smem_bytes,
+                        CUfunction *fn);
+psb_status rtc_cached(const std::string &key, CUfunction *fn);  // no compile
+psb_status rtc_launch(CUfunction fn, unsigned blocks, unsigned threads, unsigned smem,
+                      cudaStream_t s, void **args);
 
 }  // namespace psb
