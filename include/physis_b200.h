@@ -462,8 +462,8 @@ psb_status psb_generic_register(const psb_generic_stencil *desc, int *kernel_id)
 psb_status psb_generic_last_impl(int *impl);
 /* Whether the last TMA application of a generic stencil ran a kernel
  * compiled at run time for its table (1) or the kernel that interprets the
- * table (0). Tables whose every term is one grid read times a constant (no
- * post factor) are compiled by NVRTC for sm_100a when the map first runs --
+ * table (0). Tables on the TMA path are compiled by NVRTC for sm_100a when
+ * the map first runs --
  * the reference's translator likewise emits one kernel per stencil
  * (translator/cuda_translator.cc:615-869) -- and cached per process for
  * every table of the same shape (coefficients are launch arguments). Same

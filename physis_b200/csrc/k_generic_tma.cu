@@ -106,25 +106,42 @@ static bool generic_compile_on() {
   return g_generic_compile == 1;
 }
 
-// Source of a kernel for one packed-form table: the term program the
-// library's kernel interprets word by word (GtTableProg), written out with
-// every word's fields as constants: which rows to load and when, which
-// neighbouring lanes they need, each term's x offset and whether it is
-// multiplied. Coefficients stay in the launch's table (read at constant
-// offsets), so tables that differ only in coefficients share one kernel.
+// Source of a kernel for one table, the library's device headers plus its
+// term program written out with every structural field as a constant.
+// Packed tables: which rows to load and when, which neighbouring lanes each
+// run needs, each term's x offset and whether it is multiplied (the program
+// GtTableProg interprets word by word). General tables: each factor's kind,
+// window plane and offset (the loop the interpreting kernel runs).
+// Coefficients stay in the launch's table (read at constant offsets), so
+// tables that differ only in coefficients share one kernel.
+static std::string gt_factor_src(const GtFactor &f, const char *side, int t) {
+  return "GtFactor{" + std::to_string(f.kind) + ", " + std::to_string(f.k) + ", " +
+         std::to_string(f.off) + ", 0, tab." + side + "[" + std::to_string(t) + "].c}";
+}
+
 static std::string gt_jit_source(const GtTable &tab, bool dbl, std::string *key) {
   const char *T = dbl ? "double" : "float";
-  std::string body, k = std::string(T) + ":";
+  std::string body, k = std::string(T) + (tab.simple ? ":p:" : ":g:");
   for (int t = 0; t < tab.nterms; t++) {
-    const int w = tab.word[t];
-    k += std::to_string(w) + ",";
-    if (t == 0 || (w & 64))
-      body += "    gt_rows<T>(ring, sbytes, S, slot0, thr_off, bx, lane, " + std::to_string(w & 7) +
-              ", " + std::to_string(w >> 10) + ", " + ((w >> 8) & 1 ? "true" : "false") + ", " +
-              ((w >> 9) & 1 ? "true" : "false") + ", row);\n";
-    body += "    gt_term<" + std::to_string((w >> 3) & 7) + ", " + ((w >> 7) & 1 ? "true" : "false") +
-            ", " + (t == 0 ? "true" : "false") + ">(row, gt_coef(tab, " + std::to_string(t) +
-            ", T()), acc);\n";
+    if (tab.simple) {
+      const int w = tab.word[t];
+      k += std::to_string(w) + ",";
+      if (t == 0 || (w & 64))
+        body += "    gt_rows<T>(ring, sbytes, S, slot0, thr_off, bx, lane, " +
+                std::to_string(w & 7) + ", " + std::to_string(w >> 10) + ", " +
+                ((w >> 8) & 1 ? "true" : "false") + ", " + ((w >> 9) & 1 ? "true" : "false") +
+                ", row);\n";
+      body += "    gt_term<" + std::to_string((w >> 3) & 7) + ", " +
+              ((w >> 7) & 1 ? "true" : "false") + ", " + (t == 0 ? "true" : "false") +
+              ">(row, gt_coef(tab, " + std::to_string(t) + ", T()), acc);\n";
+    } else {
+      const GtFactor &a = tab.a[t], &b = tab.b[t];
+      k += std::to_string(a.kind) + "." + std::to_string(a.k) + "." + std::to_string(a.off) + "*" +
+           std::to_string(b.kind) + "." + std::to_string(b.k) + "." + std::to_string(b.off) + ",";
+      body += "    gt_general_term<T>(" + gt_factor_src(a, "a", t) + ", " +
+              gt_factor_src(b, "b", t) + ", " + (t == 0 ? "true" : "false") +
+              ", ring, sbytes, S, slot0, thr_off, bx, acc);\n";
+    }
   }
   *key = "k_generic_tma:" + k + "vy" + std::to_string(kGtVY) + "pm" +
          std::to_string(PSB_GT_PACKED_MUL) + "pa" + std::to_string(PSB_GT_PACKED_ADD);
@@ -132,7 +149,9 @@ static std::string gt_jit_source(const GtTable &tab, bool dbl, std::string *key)
                     "  static constexpr bool kCompiled = true;\n  template <typename T>\n"
                     "  static __device__ __forceinline__ void eval(const GtTable &tab, "
                     "const unsigned char *ring, int sbytes, int S, int slot0, int thr_off, "
-                    "int bx, int lane, GtBlk<T> &acc) {\n    GtRow<T> row[kGtVY];\n";
+                    "int bx, int lane, GtBlk<T> &acc) {\n";
+  if (tab.simple) src += "    GtRow<T> row[kGtVY];\n";
+  else src += "    (void)lane;\n";
   src += body;
   src += "  }\n};\n}  // namespace psb\n";
   src += std::string("extern \"C\" __global__ void __launch_bounds__(psb::kGtThreads, ") +
@@ -144,11 +163,11 @@ static std::string gt_jit_source(const GtTable &tab, bool dbl, std::string *key)
   return src;
 }
 
-// The compiled kernel of a packed-form table, or nullptr (the interpreting
-// kernel runs). Never compiles while the stream is being captured: the first
+// The compiled kernel of a table, or nullptr (the interpreting kernel
+// runs). Never compiles while the stream is being captured: the first
 // iteration of every run is eager, so a captured one finds its kernel cached.
 static CUfunction gt_jit(const GtTable &tab, bool dbl, cudaStream_t s, size_t smem_optin) {
-  if (!tab.simple || !generic_compile_on()) return nullptr;
+  if (!generic_compile_on()) return nullptr;
   std::string key;
   const std::string src = gt_jit_source(tab, dbl, &key);
   CUfunction fn = nullptr;

@@ -237,6 +237,36 @@ __device__ __forceinline__ double gt_coef(const GtTable &tab, int t, double) {
   return tab.coef[t];
 }
 
+// One term of the general form, a_t * b_t (b_t = 1: a_t alone), added to
+// the running sum (first: starts it). The interpreting kernel passes the
+// table's factors; a compiled kernel passes factors whose kind, plane and
+// offset are constants, so the loads fold to fixed shared-memory offsets.
+template <typename T>
+__device__ __forceinline__ void gt_general_term(const GtFactor &fa, const GtFactor &fb,
+                                                bool first, const unsigned char *ring,
+                                                int sbytes, int S, int slot0, int thr_off,
+                                                int bx, GtBlk<T> &acc) {
+  constexpr int V = 16 / sizeof(T);
+  const GtBlk<T> va = gt_load<T>(fa.kind, fa.k, fa.off, fa.c, ring, sbytes, S, slot0, thr_off, bx);
+  GtBlk<T> p = va;
+  if (fb.kind != 1) {
+    const GtBlk<T> vb =
+        gt_load<T>(fb.kind, fb.k, fb.off, fb.c, ring, sbytes, S, slot0, thr_off, bx);
+#pragma unroll
+    for (int r = 0; r < kGtVY; r++)
+#pragma unroll
+      for (int v = 0; v < V; v++) p.v[r][v] = xmul(va.v[r][v], vb.v[r][v]);
+  }
+  if (first) {
+    acc = p;
+  } else {
+#pragma unroll
+    for (int r = 0; r < kGtVY; r++)
+#pragma unroll
+      for (int v = 0; v < V; v++) acc.v[r][v] = xadd(acc.v[r][v], p.v[r][v]);
+  }
+}
+
 __device__ __forceinline__ int gt_key(int w) { return ((w >> 3) & 7) | ((w >> 4) & 8); }
 
 // The VY rows of the run that starts with a term word's fields (window
@@ -276,9 +306,10 @@ struct GtTableProg {
 
 // The kernel body, shared by the library's own kernel (which interprets the
 // term table) and kernels compiled at run time for one table (whose term
-// program is fixed at compile time). Prog::eval evaluates a packed-form
-// table on the rows of the window; Prog::kCompiled says the table is always
-// packed (the general form is not compiled in).
+// program is fixed at compile time). Prog::eval evaluates the sum of the
+// terms; the library's program handles packed tables only (general ones take
+// the loop below), a compiled program (Prog::kCompiled) is the whole table,
+// packed or general. The post factor is applied here in both cases.
 template <typename T, class Prog>
 __device__ __forceinline__ void gt_body(const GtMaps &maps, const GtTable &tab,
                                         const GridView &out, const Dom3 &d, const GtGeom &geo,
@@ -365,28 +396,9 @@ __device__ __forceinline__ void gt_body(const GtMaps &maps, const GtTable &tab,
     if (Prog::kCompiled || tab.simple) {
       Prog::template eval<T>(tab, ring, geo.stage_bytes, S, slot0, thr_off, geo.bx, lane, acc);
     } else {
-    for (int t = 0; t < tab.nterms; t++) {
-      const GtFactor fa = tab.a[t], fb = tab.b[t];
-      const GtBlk<T> va = gt_load<T>(fa.kind, fa.k, fa.off, fa.c, ring, geo.stage_bytes, S,
-                                     slot0, thr_off, geo.bx);
-      GtBlk<T> p = va;
-      if (fb.kind != 1) {
-        const GtBlk<T> vb = gt_load<T>(fb.kind, fb.k, fb.off, fb.c, ring, geo.stage_bytes, S,
-                                       slot0, thr_off, geo.bx);
-#pragma unroll
-        for (int r = 0; r < kGtVY; r++)
-#pragma unroll
-          for (int v = 0; v < V; v++) p.v[r][v] = xmul(va.v[r][v], vb.v[r][v]);
-      }
-      if (t == 0) {
-        acc = p;
-      } else {
-#pragma unroll
-        for (int r = 0; r < kGtVY; r++)
-#pragma unroll
-          for (int v = 0; v < V; v++) acc.v[r][v] = xadd(acc.v[r][v], p.v[r][v]);
-      }
-    }
+      for (int t = 0; t < tab.nterms; t++)
+        gt_general_term<T>(tab.a[t], tab.b[t], t == 0, ring, geo.stage_bytes, S, slot0, thr_off,
+                           geo.bx, acc);
     }
     if (tab.has_post) {
       const GtFactor fp = tab.post;

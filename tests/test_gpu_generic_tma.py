@@ -1,6 +1,6 @@
 """The generic stencil on the TMA z-streaming kernel (k_generic_tma), both as
 the kernel that interprets the term table and as the kernel compiled at run
-time for the table (tables whose terms are all one read times a constant).
+time for the table.
 
 Every map the TMA path can take must give exactly what the thread-per-point
 kernel and the oracle port give (the reference's term order and roundings):
@@ -144,7 +144,7 @@ def test_random_tables_bit_exact(seed, modes, dtype, compile_mode):
         pytest.skip("grid too thin for plain reads")
     got, plain, impl, st, compiled = _run_both(d, arrays, dims_list, dom, ps.LAYOUT_PITCHED)
     assert impl == ps.IMPL_TMA
-    assert compiled == (compile_mode and _is_packed(st))
+    assert compiled == compile_mode
     want = [a.copy() for a in arrays]
     oracle.generic_apply(st.struct, want, list(dom[0]), list(dom[1]))
     assert U.bits_equal(got, plain)

@@ -61,6 +61,35 @@ psb_generic_tma_compiled(const __grid_constant__ psb::GtMaps maps,
 """
 
 
+# A general program: products of two reads, a constant times a read, a bare
+# read.
+GENERAL = r"""
+#include "k_generic_tma.cuh"
+namespace psb {
+struct GtCompiledProg {
+  static constexpr bool kCompiled = true;
+  template <typename T>
+  static __device__ __forceinline__ void eval(const GtTable &tab, const unsigned char *ring,
+      int sbytes, int S, int slot0, int thr_off, int bx, int lane, GtBlk<T> &acc) {
+    (void)lane;
+    gt_general_term<T>(GtFactor{2, 1, -140, 0, tab.a[0].c}, GtFactor{2, 0, 2880, 0, tab.b[0].c},
+                       true, ring, sbytes, S, slot0, thr_off, bx, acc);
+    gt_general_term<T>(GtFactor{0, 0, 0, 0, tab.a[1].c}, GtFactor{2, 2, 5, 0, tab.b[1].c},
+                       false, ring, sbytes, S, slot0, thr_off, bx, acc);
+    gt_general_term<T>(GtFactor{2, 1, 0, 0, tab.a[2].c}, GtFactor{1, 0, 0, 0, tab.b[2].c},
+                       false, ring, sbytes, S, slot0, thr_off, bx, acc);
+  }
+};
+}  // namespace psb
+extern "C" __global__ void __launch_bounds__(psb::kGtThreads, MINB)
+psb_generic_tma_compiled(const __grid_constant__ psb::GtMaps maps,
+                         const __grid_constant__ psb::GtTable tab, psb::GridView out,
+                         psb::Dom3 d, const __grid_constant__ psb::GtGeom geo, int *err) {
+  psb::gt_body<TYPE, psb::GtCompiledProg>(maps, tab, out, d, geo, err);
+}
+"""
+
+
 def _compile(src, opts):
     err, prog = nvrtc.nvrtcCreateProgram(src.encode(), b"psb_stencil.cu", 1, [PRELUDE.encode()],
                                          [b"psb_rtc_prelude.h"])
@@ -83,6 +112,16 @@ def test_generated_kernel_compiles_for_sm100a(typ, minb, packed_mul, packed_add)
     opts = ["--gpu-architecture=sm_100a", "-std=c++17", "--fmad=false", "-default-device",
             "-I" + CSRC, "-DPSB_GT_VY=4", "-DPSB_GT_PACKED_MUL=%d" % packed_mul,
             "-DPSB_GT_PACKED_ADD=%d" % packed_add]
+    res, log, size = _compile(src, opts)
+    assert res == nvrtc.nvrtcResult.NVRTC_SUCCESS, log
+    assert size > 0
+
+
+@pytest.mark.parametrize("typ,minb", [("float", 4), ("double", 3)])
+def test_generated_general_kernel_compiles_for_sm100a(typ, minb):
+    src = GENERAL.replace("MINB", str(minb)).replace("TYPE", typ)
+    opts = ["--gpu-architecture=sm_100a", "-std=c++17", "--fmad=false", "-default-device",
+            "-I" + CSRC, "-DPSB_GT_VY=4"]
     res, log, size = _compile(src, opts)
     assert res == nvrtc.nvrtcResult.NVRTC_SUCCESS, log
     assert size > 0
