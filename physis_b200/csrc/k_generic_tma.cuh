@@ -22,12 +22,6 @@ constexpr int kGtR = 2;          // largest |offset| per axis (the pitched halo)
 #ifndef PSB_GT_PACKED_MUL
 #define PSB_GT_PACKED_MUL 1
 #endif
-// Sums of the packed form: 1 in pairs through add.rn.f32x2 (inline PTX with
-// an explicit rounding mode, which is never contracted with a multiply), 0
-// scalar rounded adds.
-#ifndef PSB_GT_PACKED_ADD
-#define PSB_GT_PACKED_ADD 0
-#endif
 constexpr int kGtVY = PSB_GT_VY;  // rows per consumer thread
 constexpr int kGtConsumers = 128;
 constexpr int kGtThreads = kGtConsumers + 32;
@@ -150,17 +144,6 @@ __device__ __forceinline__ void gt_row_load(const T *p, int lane, bool need_n, b
 // starts it, as the reference's sum starts from its first term). Float
 // products go in pairs through the sm_100 f32x2 multiply (each lane rounded
 // like the scalar one); the sums stay scalar.
-// a + b per lane, each rounded to nearest: one add.rn.f32x2.
-__device__ __forceinline__ float2 gt_add2(float2 a, float2 b) {
-  float2 r;
-  asm("{\n\t.reg .b64 ra, rb, rd;\n\t"
-      "mov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-      "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
-
 template <int DXP2, bool ONE, bool FIRST>
 __device__ __forceinline__ void gt_term(const GtRow<float> (&row)[kGtVY], float c,
                                         GtBlk<float> &acc) {
@@ -183,14 +166,7 @@ __device__ __forceinline__ void gt_term(const GtRow<float> (&row)[kGtVY], float 
       acc.v[r][1] = lo.y;
       acc.v[r][2] = hi.x;
       acc.v[r][3] = hi.y;
-    } else if (PSB_GT_PACKED_ADD) {
-      const float2 a = gt_add2(make_float2(acc.v[r][0], acc.v[r][1]), lo);
-      const float2 b = gt_add2(make_float2(acc.v[r][2], acc.v[r][3]), hi);
-      acc.v[r][0] = a.x;
-      acc.v[r][1] = a.y;
-      acc.v[r][2] = b.x;
-      acc.v[r][3] = b.y;
-    } else {  // scalar adds (the packed add intrinsic may be fused with the multiply)
+    } else {  // scalar adds: paired f32x2 adds gave results 1 ulp off the scalar sums
       acc.v[r][0] = xadd(acc.v[r][0], lo.x);
       acc.v[r][1] = xadd(acc.v[r][1], lo.y);
       acc.v[r][2] = xadd(acc.v[r][2], hi.x);
