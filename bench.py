@@ -535,6 +535,9 @@ def run_ours(args):
         ps.check(ps.lib.psb_generic_last_impl(ctypes.byref(v)), "psb_generic_last_impl")
         gimpl = {ps.IMPL_TMA: "k_generic_tma (TMA z-streaming)",
                  ps.IMPL_GENERIC: "k_generic (thread per point)"}.get(v.value, str(v.value))
+        if v.value == ps.IMPL_TMA:
+            gimpl += (", compiled at run time for this table (psb_generic_tma_compiled)"
+                      if ps.generic_last_compiled() else ", interpreting the table")
     dev_s = sum(ms_list) / 1e3
     dev_s_max = dist.max(dev_s)
     total_pts = dist.sum(pts_per_step * args.steps)
