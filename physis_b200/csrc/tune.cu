@@ -76,24 +76,31 @@ static std::string shipped_path() {
   return libdir.substr(0, b) + "/tune_b200.json";
 }
 
+// Entries are objects {"kernel": ..., "ms": ...} with the keys in the order
+// save_cache writes them; any layout of the file (one entry per line, or a
+// whole list on one line) is read.
 static void parse_cache_file(const std::string &path) {
   Runtime &r = rt();
   FILE *f = fopen(path.c_str(), "r");
   if (!f) return;
-  char line[512];
-  while (fgets(line, sizeof(line), f)) {
+  std::string text;
+  char buf[4096];
+  size_t n;
+  while ((n = fread(buf, 1, sizeof(buf), f)) > 0) text.append(buf, n);
+  fclose(f);
+  for (size_t pos = text.find("{\"kernel\""); pos != std::string::npos;
+       pos = text.find("{\"kernel\"", pos + 1)) {
     TuneKey k;
     psb_tune_config c;
     double ms = 0;
-    int got = sscanf(line,
-                     " {\"kernel\": %d, \"type\": %d, \"n\": [%d, %d, %d], \"impl\": %d, "
+    int got = sscanf(text.c_str() + pos,
+                     "{\"kernel\": %d, \"type\": %d, \"n\": [%d, %d, %d], \"impl\": %d, "
                      "\"tile_x\": %d, \"tile_y\": %d, \"z_chunk\": %d, \"stages\": %d, "
                      "\"t_depth\": %d, \"ms\": %lf",
                      &k.kernel, &k.type, &k.nx, &k.ny, &k.nz, &c.impl, &c.tile_x, &c.tile_y,
                      &c.z_chunk, &c.stages, &c.t_depth, &ms);
     if (got >= 11) r.tune[k] = c;
   }
-  fclose(f);
 }
 
 static void load_cache() {

@@ -157,3 +157,25 @@ def test_batch_tune_entries_use_the_header_base_and_buckets():
     out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True)
     assert out.returncode == 0, out.stderr
     assert "'t_depth': 2" in out.stdout and "'tile_x': 64" in out.stdout
+
+
+def test_tune_cache_reads_a_list_on_one_line(tmp_path):
+    """The cache reader takes entries in any layout: here json.dump's whole
+    list on one line, with two entries."""
+    import json
+    import sys
+    path = tmp_path / "tune.json"
+    ents = [{"kernel": 3, "type": 2, "n": [128, 128, 128], "impl": 2, "tile_x": 64, "tile_y": 8,
+             "z_chunk": 64, "stages": 6, "t_depth": 2, "ms": 0},
+            {"kernel": 1, "type": 2, "n": [96, 96, 96], "impl": 2, "tile_x": 64, "tile_y": 4,
+             "z_chunk": 8, "stages": 6, "t_depth": 1, "ms": 0}]
+    path.write_text(json.dumps(ents))
+    code = ("import physis_b200 as ps\n"
+            "print(ps.tune_get(ps.HIMENO19, ps.PS_FLOAT, (128, 128, 128)))\n"
+            "print(ps.tune_get(ps.DIFFUSION7, ps.PS_FLOAT, (96, 96, 96)))\n")
+    env = dict(os.environ, PHYSIS_B200_TUNE_CACHE=str(path), PYTHONPATH=ROOT)
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True)
+    assert out.returncode == 0, out.stderr
+    lines = out.stdout.strip().splitlines()
+    assert "'t_depth': 2" in lines[0] and "'z_chunk': 64" in lines[0]
+    assert "'tile_y': 4" in lines[1] and "'z_chunk': 8" in lines[1]
