@@ -36,10 +36,6 @@ constexpr int kHtStage2 = (kHtBX * kHtBY2 * 4 + 127) / 128 * 128;
 constexpr int kHtField = kHtStage2;        // one coefficient box
 constexpr int kHtStageC = 12 * kHtField;
 constexpr int kHtW1 = 5, kHtW2 = 4;        // stage-1 and stage-2 warps
-#ifndef PSB_HT_PF
-#define PSB_HT_PF 2
-#endif
-constexpr int kHtPF = PSB_HT_PF;           // planes prefetched into L2 ahead of the rings
 constexpr int kHtRingBytes = kHtS1 * kHtStage1 + kHtS2 * kHtStage2 + kHtSC * kHtStageC;
 static_assert(kHtTX / kHtV * (kHtTY + 2) == 32 * kHtW1, "stage-1 threads cover the halo rows");
 static_assert(kHtTX / kHtV * kHtTY == 32 * kHtW2, "stage-2 threads cover the tile");
@@ -128,23 +124,9 @@ __device__ __forceinline__ bool ht_produce_tile(const HtRings &R, RingPos &p1, R
     ring_next(pc, kHtSC);
     return true;
   };
-  // L2 prefetch kHtPF planes ahead of the ring: the coefficient ring's live
-  // planes leave about one 35 KB stage in flight per SM, short of what hides
-  // DRAM latency; a prefetched plane's later load is an L2 hit. Only planes
-  // of this tile are prefetched (coordinates the loads also use).
-  auto prefetch = [&](int j) {
-    if (kHtPF <= 0 || j >= nzl + 2) return;
-    const int z = zb - 1 + j;
-    for (int f = 0; f < 12; f++)
-      tma_prefetch_l2_3d(coef + f, x0 - 4 + ax0, y0 - 1 + ay0, z + az0);
-    tma_prefetch_l2_3d(tin, x0 - 4 + ax0, y0 - 2 + ay0, z + 1 + az0);
-  };
-  for (int j = 0; j < kHtPF; j++) prefetch(j);
   if (!put1(zb - 2) || !put1(zb - 1)) return false;
-  for (int j = 0; j < nzl + 2; j++) {
-    prefetch(j + kHtPF);
+  for (int j = 0; j < nzl + 2; j++)
     if (!put1(zb + j) || !putc(zb - 1 + j)) return false;
-  }
   return true;
 }
 
