@@ -142,7 +142,7 @@ __device__ __forceinline__ void ht_drain(const HtRings &R, RingPos p1, RingPos p
 // each row). With acc_on, the FP64 sum of ss*ss over the tile's own domain
 // points is added to *acc. False (warp-uniformly) if a bounded wait gave up.
 __device__ __forceinline__ bool ht_stage1_tile(const HtRings &R, RingPos &p1, RingPos &pc,
-                                               RingPos &p2, int t, int lane, const Dom3 &d,
+                                               RingPos &p2, int t, int lane, const Dom3 d,
                                                float omega, int x0, int y0, int zb, int nzl,
                                                bool acc_on, double *acc) {
   const int tx = t % (kHtTX / kHtV), row = t / (kHtTX / kHtV);
@@ -232,7 +232,7 @@ __device__ __forceinline__ bool ht_stage1_tile(const HtRings &R, RingPos &p1, Ri
 // points is added to *acc. False (warp-uniformly) if a bounded wait gave up.
 __device__ __forceinline__ bool ht_stage2_tile(const HtRings &R, RingPos &p2, RingPos &pc, int t,
                                                int lane, float *pout, int64_t sy, int64_t sz,
-                                               const Dom3 &d, float omega, int x0, int y0,
+                                               const Dom3 d, float omega, int x0, int y0,
                                                int zb, int nzl, bool copy, bool acc_on,
                                                double *acc) {
   const int tx = t % (kHtTX / kHtV), row = t / (kHtTX / kHtV);
