@@ -867,7 +867,7 @@ def run_c4(args, dist):
         members = [(k, (args.c4_cube,) * 3, st) for k, _, st in members]
     if args.c4_steps:
         members = [(k, d, args.c4_steps) for k, d, _ in members]
-    if args.c4_him_two_sweeps:
+    if args.him_two_sweeps:
         for k, d, _ in members:
             if k == "him":
                 ps.batch_tune_set(ps.HIMENO19, d, impl=ps.IMPL_TMA, tile_x=64, tile_y=8, z_chunk=0,
@@ -954,7 +954,7 @@ def run_c4(args, dist):
     overrides = {k: v for k, v in (("members", args.members if args.members != 256 else None),
                                    ("kind", args.c4_kind), ("cube", args.c4_cube),
                                    ("steps", args.c4_steps),
-                                   ("himeno_two_sweeps", args.c4_him_two_sweeps or None))
+                                   ("himeno_two_sweeps", args.him_two_sweeps or None))
                  if v is not None}
     if overrides:
         line["config"]["profiling_overrides"] = overrides
@@ -1137,6 +1137,11 @@ def run_c5(args, dist):
     ps.PSInit()
     trace = c5_trace(count=args.c5_requests)
     tuned_buckets = c5_tune(ps, trace) if args.tune else None
+    if args.him_two_sweeps:
+        for side in sorted({side for _, kind, side, _ in trace if kind == "him"} |
+                           {32 + 16 * i for i in range(6)}):
+            ps.batch_tune_set(ps.HIMENO19, (side,) * 3, impl=ps.IMPL_TMA, tile_x=64, tile_y=8,
+                              z_chunk=0, stages=6, t_depth=2)
 
     def pinned(n):
         hp = ctypes.c_void_p()
@@ -1183,6 +1188,7 @@ def run_c5(args, dist):
                             "has an entry (tile shape, z chunk, Himeno sweeps per pass), else "
                             "the fewest-tiles rule",
                    "buckets_tuned_in_run": tuned_buckets,
+                   "himeno_two_sweeps_pinned": bool(args.him_two_sweeps),
                    "inputs": "diffusion u0 from pinned host memory (U[0,1)); Himeno p and "
                              "coefficients generated on the device from per-request seeds; "
                              "every final field copied back to pinned host memory",
@@ -1381,8 +1387,8 @@ def main():
                     help="c4: every member a cube of this side (kinds and steps kept; profiling)")
     ap.add_argument("--c4-steps", type=int, default=None,
                     help="c4: every member this many steps (profiling)")
-    ap.add_argument("--c4-him-two-sweeps", action="store_true",
-                    help="c4: pin every Himeno bucket to two sweeps per pass (profiling)")
+    ap.add_argument("--him-two-sweeps", action="store_true",
+                    help="c4/c5: pin every Himeno bucket to two sweeps per pass (profiling)")
     ap.add_argument("--c4-kind", default=None, choices=["diffp", "him"],
                     help="c4: keep only one kind of member (profiling)")
     ap.add_argument("--c5-requests", type=int, default=128, help="c5: requests in the trace")
