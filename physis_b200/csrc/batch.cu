@@ -904,12 +904,28 @@ static MemberTune member_tune(const BatchMemberHost &h) {
   return t;
 }
 
+// Sweeps per pass of a Himeno member whose bucket has no tune entry: two
+// when it is at least 120 points inside on every axis and the 64-wide tiles
+// of the two-sweep pass leave at most 15% of their columns outside its x
+// extent. Measured in the persistent batch on B200 (GLUPS, one sweep -> two):
+// cubes of 128 and 256 gain 11% and 5%; cubes of 32, 48, 64 and 96 lose
+// 39%, 12%, 10% and 18% (small members get short z chunks, so each pass
+// re-reads a larger share of halo planes; 96 wastes 27% of its tile columns).
+static int default_sweeps(const BatchMemberHost &h) {
+  const int *n = h.grids[0]->pub.dim;
+  const int ix = n[0] - 2, iy = n[1] - 2, iz = n[2] - 2;
+  if (ix < 120 || iy < 120 || iz < 120) return 1;
+  const int cols = (n[0] - 1 + kHtTX - 1) / kHtTX * kHtTX;  // columns of batch_t2geom's tiles
+  return ix * 100 >= cols * 85 ? 2 : 1;
+}
+
 // Work list of a member: 0 diffusion, 1 Himeno one sweep per item, 2 Himeno
-// up to two sweeps per item (when its tune entry or trial says so and it
-// runs at least two steps).
+// up to two sweeps per item (when its tune entry or trial says so, or, with
+// neither, default_sweeps; and it runs at least two steps).
 static int member_group(const BatchMemberHost &h, const MemberTune &mt, int steps) {
   if (h.kind != BK_HIMENO) return 0;
-  return mt.td == 2 && steps >= 2 ? 2 : 1;
+  const int td = mt.tuned || mt.forced ? mt.td : default_sweeps(h);
+  return td == 2 && steps >= 2 ? 2 : 1;
 }
 
 // Passes of a group-2 member: from each local step s (global step0 + s) two
@@ -1722,11 +1738,16 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
   if (st == PSB_OK && cudaEventCreate(&e0) != cudaSuccess) st = PSB_ERR_CUDA;
   if (st == PSB_OK && cudaEventCreate(&e1) != cudaSuccess) st = PSB_ERR_CUDA;
   double best = -1, rule_ms = -1;
-  // Himeno buckets also try two sweeps per pass (64 x 8 tiles), recorded as
-  // t_depth 2 with tile_x 64.
+  // The rule is the batch's default: the fewest-tiles shape with the
+  // default sweeps per pass. Himeno buckets also try the other depth (two
+  // sweeps: 64 x 8 tiles, recorded as tile_x 64).
+  const int rule_td = h.kind == BK_HIMENO ? default_sweeps(h) : 1;
   std::vector<std::array<int, 2>> cands;  // (tile width in threads or 0, t_depth)
-  for (int tx : txs) cands.push_back({tx, 1});
-  if (h.kind == BK_HIMENO) cands.push_back({kHtTX / 4, 2});
+  cands.push_back({0, rule_td});
+  for (int tx : txs)
+    if (tx > 0) cands.push_back({tx, 1});
+  if (h.kind == BK_HIMENO) cands.push_back(rule_td == 2 ? std::array<int, 2>{0, 1}
+                                                        : std::array<int, 2>{kHtTX / 4, 2});
   // The z chunk is left to the batch's own rule (items per step over the
   // whole work list), as in a real run: a chunk that wins for the copies
   // alone is not the one a mixed batch would give this member.
@@ -1756,8 +1777,9 @@ static psb_status batch_tune_member(const BatchMemberHost &h, psb_tune_config *b
         fprintf(__ps_trace, "physis_b200: batch tune kind=%d tile=%dx%d t=%d: %.4f ms\n",
                 h.kind, tx * 4, td == 2 ? kHtTY : tx ? (kBConsumers / tx) * rows_per_thread : 0,
                 td, ms_best);
-      if (tx == 0 && td == 1) rule_ms = ms_best;
-      const double bar = tx == 0 && td == 1 ? best : std::min(best, kTuneMargin * rule_ms);
+      const bool rule = tx == 0 && td == rule_td;
+      if (rule) rule_ms = ms_best;
+      const double bar = rule ? best : std::min(best, kTuneMargin * rule_ms);
       if (st == PSB_OK && ms_best > 0 && (best < 0 || ms_best < bar)) {
         best = ms_best;
         best_cfg->impl = PSB_IMPL_TMA;

@@ -275,6 +275,30 @@ TWO_SWEEP_MEMBERS = [
 
 
 @pytest.mark.gpu
+def test_batch_default_sweeps_per_pass():
+    """Without tune entries a Himeno member runs two sweeps per pass when it
+    is at least 120 inside on every axis and 64-wide tiles cover its x
+    extent with at most 15% to spare (129^3: 127 of 128 columns), else one
+    (160^3: 158 of 192; 96^3: too small); results equal the oracle's."""
+    spec = [("him", (129, 129, 129), 6), ("him", (160, 160, 160), 3), ("him", (96, 96, 96), 4),
+            ("diff", (64, 64, 64), 5)]
+    M = Members(spec)
+    try:
+        b = M.batch()
+        b.run(0)
+        want_td = [2, 1, 1, 1]
+        for i, (kind, dims, steps) in enumerate(spec):
+            lay = b.layout(i)
+            done, _, g = b.result(i)
+            assert done == steps
+            assert lay["t_depth"] == want_td[i] and lay["tuned"] == 0, (i, lay)
+            assert U.bits_equal(ps.PSGridCopyout(g), _want(kind, M.data[i], steps)), (i, lay)
+        b.free()
+    finally:
+        M.free()
+
+
+@pytest.mark.gpu
 @pytest.mark.parametrize("mode", [0, 1])
 def test_batch_two_sweep_himeno_bit_exact(mode):
     """Himeno members on two sweeps per pass (the autotuner's t_depth 2) give
