@@ -43,6 +43,9 @@ WORKLOADS = {
     # a user stencil through the generic term table: the 27-point box
     # average (each neighbour times 1/27), interior of 512^3
     "g27": ("generic27", np.float32, (512, 512, 512), 100, 8),
+    # the C2 stencil written as a stencil function in the reference's DSL and
+    # compiled by the translator-free front end (physis_b200/dsl.py)
+    "dsl7": ("dsl7", np.float32, (512, 512, 512), 100, 8),
     # batched: 256 members, see c4_members(); dims/steps are per member
     "c4": ("batch", np.float32, (0, 0, 0), 0, 0),
     # served: a Poisson trace of solve requests, see c5_trace()
@@ -68,6 +71,12 @@ def describe(wl):
         return ("generic (user) stencil: 27-point box average sum_{d in {-1,0,1}^3} (1/27)*u(p+d) "
                 "as a psb_generic_stencil term table, %dx%dx%d fp32 interior [1,n-1)^3, %d time "
                 "steps per solve (double-buffered PSStencilRun)" % (dims + (steps,)))
+    if k == "dsl7":
+        return ("7-point diffusion %dx%dx%d fp32 written as a DSL stencil function "
+                "(physis_b200.workloads.DIFFUSION7_DSL) and compiled by the translator-free "
+                "front end into the reference's generated-kernel shape (one thread per (x, y), "
+                "z loop), %d time steps per solve (double-buffered PSStencilRun), clamped "
+                "faces" % (dims + (steps,)))
     return ("7-point diffusion %dx%dx%d %s, %d time steps per solve (double-buffered "
             "PSStencilRun), clamped faces" % (dims + ("fp32" if dt == np.float32 else "fp64", steps)))
 
@@ -284,7 +293,8 @@ def _coef_sum(dt):
     return float(sum(np.float64(np.asarray(COEF, dt))))
 
 
-def numerics_diffusion(ps, dt, dims, tsteps, grids, m1, m2, host, mass0, mass1, steps_done):
+def numerics_diffusion(ps, dt, dims, tsteps, grids, m1, m2, host, mass0, mass1, steps_done,
+                       kernel_id=None):
     """Error of the 7-point path against the oracle, outside the timed
     region: (1) the full-size grid after NUMERICS_FULL_STEPS steps from the
     workload's field, against the oracle port (the reference CPU target bit
@@ -331,8 +341,9 @@ def numerics_diffusion(ps, dt, dims, tsteps, grids, m1, m2, host, mass0, mass1, 
          for _ in range(2)]
     ps.PSGridCopyin(g[0], f)
     d = ps.PSDomain3DNew(0, n, 0, n, 0, n)
-    a = ps.PSStencilMap(ps.DIFFUSION7, d, g[0], g[1], *COEF)
-    b = ps.PSStencilMap(ps.DIFFUSION7, d, g[1], g[0], *COEF)
+    kid = ps.DIFFUSION7 if kernel_id is None else kernel_id
+    a = ps.PSStencilMap(kid, d, g[0], g[1], *COEF)
+    b = ps.PSStencilMap(kid, d, g[1], g[0], *COEF)
     ps.PSStencilRun(a, b, tsteps // 2)
     got = ps.PSGridCopyout(g[0])
     for x in g:
@@ -440,7 +451,7 @@ def run_ours(args):
     ptype = ps.PS_FLOAT if dt == np.float32 else ps.PS_DOUBLE
     kernel = ps.HIMENO19 if kname == "himeno" else ps.DIFFUSION7
     tune = None
-    if kname != "generic27":
+    if kname not in ("generic27", "dsl7"):
         tune = ps.autotune(kernel, ptype, dims) if args.tune else ps.tune_get(kernel, ptype, dims)
     if args.plain:
         # the thread-per-point shape of the reference's generated kernels
@@ -483,8 +494,13 @@ def run_ours(args):
         grids = [ps.grid_new(ptype, dims), ps.grid_new(ptype, dims)]
         ps.PSGridCopyin(grids[0], host)
         dom = ps.PSDomain3DNew(0, nx, 0, ny, 0, nz)
-        m1 = ps.PSStencilMap(ps.DIFFUSION7, dom, grids[0], grids[1], *COEF)
-        m2 = ps.PSStencilMap(ps.DIFFUSION7, dom, grids[1], grids[0], *COEF)
+        kid = ps.DIFFUSION7
+        if kname == "dsl7":
+            from physis_b200 import dsl
+            from physis_b200.workloads import DIFFUSION7_DSL
+            kid = dsl.compile_stencils(DIFFUSION7_DSL)["diffusion7"].kernel_id
+        m1 = ps.PSStencilMap(kid, dom, grids[0], grids[1], *COEF)
+        m2 = ps.PSStencilMap(kid, dom, grids[1], grids[0], *COEF)
         pts_per_step = nx * ny * nz * tsteps
         g_io = grids[0]
 
@@ -493,7 +509,7 @@ def run_ours(args):
         return ps.last_run_stats()
 
     # ---- device-resident timing ------------------------------------------
-    mass0 = ps.reduce64(ps.PS_SUM, g_io) if kname == "diffusion7" else None
+    mass0 = ps.reduce64(ps.PS_SUM, g_io) if kname in ("diffusion7", "dsl7") else None
     for _ in range(args.warmup):
         solve()
     ps.sync()
@@ -511,7 +527,7 @@ def run_ours(args):
     wall = time.perf_counter() - t0
     clocks = sampler.stop()
     dist.barrier()
-    mass1 = ps.reduce64(ps.PS_SUM, g_io) if kname == "diffusion7" else None
+    mass1 = ps.reduce64(ps.PS_SUM, g_io) if kname in ("diffusion7", "dsl7") else None
     exact_mode = None
     if fma:
         # The same solves with the exact arithmetic (outside the headline's
@@ -552,7 +568,7 @@ def run_ours(args):
     achieved = bpl * pts_per_step * args.steps / dev_s / 1e9
     two_sweeps = kname == "himeno" and tune is not None and tune.get("t_depth") == 2
     kname_traffic = ("k_himeno_tb2" if two_sweeps else "k_himeno_tma") if kname == "himeno" else \
-        "k_generic_tma_f32" if kname == "generic27" else (
+        "k_generic_tma_f32" if kname == "generic27" else "k_dsl_diffusion7_f32" if kname == "dsl7" else (
         "k_diff7_tma_f32" if dt == np.float32 else "k_diff7_tma_f64") + ("_fma" if fma else "")
     if args.plain:
         kname_traffic = kname_traffic.replace("tma", "plain")
@@ -590,10 +606,12 @@ def run_ours(args):
             numerics = numerics_generic27(ps, dt)
         else:
             numerics = numerics_diffusion(ps, dt, dims, tsteps, grids, m1, m2, host, mass0, mass1,
-                                          (args.warmup + args.steps) * tsteps)
+                                          (args.warmup + args.steps) * tsteps,
+                                          kernel_id=kid if kname == "dsl7" else None)
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(wl, host if kname in ("diffusion7", "generic27") else None)
+        cpu = cpu_baseline_sample(wl, host if kname in ("diffusion7", "generic27", "dsl7")
+                                  else None)
 
     line = {
         "metric": "lattice_updates_per_s_" + wl,
@@ -613,7 +631,8 @@ def run_ours(args):
             "step": "one solve of %d time steps (PSStencilRun of two maps x %d)" % (tsteps, tsteps // 2),
             "inputs_vs_l2": "%.0f MB per grid > 126 MB L2; no flush needed" % (host.nbytes / 1e6),
             "parallelism": "replicas (one independent solve per GPU, no exchange)",
-            "impl": "plain" if args.plain else "autotuned",
+            "impl": ("DSL stencil function compiled by physis_b200.dsl (reference generated-kernel "
+                     "shape)" if kname == "dsl7" else "plain" if args.plain else "autotuned"),
             "fp_mode": ("fma: the reference's term order with fused multiply-adds (one "
                         "rounding per term; every point within 4 ulp of the exact step per "
                         "step; errors against the FP64 oracle in `numerics`)" if fma else

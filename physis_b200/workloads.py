@@ -4,8 +4,9 @@ Used by the benchmark, the smoke test and the parity tests alike: the
 Himeno inputs of the C3-style configurations (the distributions of
 examples/himeno/himenobmtxpa_physis.c:314-329) and two helpers that run a
 double-buffered 7-point or Himeno solve through PSStencilMap/PSStencilRun
-and return the result as a host array. Everything here calls the runtime
-library; nothing computes on the host.
+and return the result as a host array, the 27-point box table, and the
+7-point stencil as DSL source for the front end. Everything here calls the
+runtime library; nothing computes on the host.
 """
 import numpy as np
 
@@ -123,3 +124,25 @@ def box27_struct(accum=ps.PS_FLOAT):
 def box27_stencil(accum=ps.PS_FLOAT):
     """The 27-point box average registered as a generic stencil."""
     return ps.GenericStencil(3, [(accum, (0, 1, 2))] * 2, 1, accum, box27_terms(accum))
+
+
+# The 7-point diffusion of the C2 workload as a stencil function in the
+# reference's DSL (the form of examples/diffusion-benchmark/diffusion3d_physis.c:
+# clamped neighbours chosen at the faces, then the coefficient-weighted sum in
+# the order cc, cw, ce, cs, cn, cb, ct), for the translator-free front end.
+# Scalars follow the built-in kernel's order (ce, cw, cn, cs, ct, cb, cc), so
+# the same PSStencilMap arguments drive either.
+DIFFUSION7_DSL = """
+void diffusion7(const int x, const int y, const int z, PSGrid3DFloat u, PSGrid3DFloat v,
+                float ce, float cw, float cn, float cs, float ct, float cb, float cc) {
+  const int nx = PSGridDim(u, 0), ny = PSGridDim(u, 1), nz = PSGridDim(u, 2);
+  float c = PSGridGet(u, x, y, z);
+  float w = x == 0 ? c : PSGridGet(u, x - 1, y, z);
+  float e = x == nx - 1 ? c : PSGridGet(u, x + 1, y, z);
+  float n = y == 0 ? c : PSGridGet(u, x, y - 1, z);
+  float s = y == ny - 1 ? c : PSGridGet(u, x, y + 1, z);
+  float b = z == 0 ? c : PSGridGet(u, x, y, z - 1);
+  float t = z == nz - 1 ? c : PSGridGet(u, x, y, z + 1);
+  PSGridEmit(v, cc * c + cw * w + ce * e + cs * s + cn * n + cb * b + ct * t);
+}
+"""
