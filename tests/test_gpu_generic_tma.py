@@ -269,3 +269,39 @@ def test_multi_step_runs_refresh_the_halo(boundary, compile_mode):
         oracle.generic_apply(st.struct, [a, b], [0, 0, 0], [nx, ny, nz])
         oracle.generic_apply(st.struct, [b, a], [0, 0, 0], [nx, ny, nz])
     assert U.bits_equal(got, a)
+
+
+def test_without_device_headers_the_interpreting_kernel_runs(tmp_path):
+    """Run-time compilation needs the library's device headers; pointed at a
+    directory without them it fails quietly and the interpreting kernel runs
+    the same table with the same results (in a fresh process, so the
+    function cache starts empty)."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = r'''
+import numpy as np
+import physis_b200 as ps
+from physis_b200.workloads import box27_stencil
+from oracle import oracle
+ps.PSInit()
+st = box27_stencil(ps.PS_FLOAT)
+n = 40
+f = np.random.default_rng(2).random((n, n, n), dtype=np.float32)
+g = [ps.grid_new(ps.PS_FLOAT, (n, n, n)) for _ in range(2)]
+ps.PSGridCopyin(g[0], f)
+ps.PSGridCopyin(g[1], f)
+m = ps.PSStencilMap(st.kernel_id, ps.PSDomain3DNew(1, n - 1, 1, n - 1, 1, n - 1), g[0], g[1])
+ps.PSStencilRun(m, 1)
+got = ps.PSGridCopyout(g[1])
+want = [f.copy(), f.copy()]
+oracle.generic_apply(st.struct, want, [1, 1, 1], [n - 1] * 3)
+print("compiled", ps.generic_last_compiled())
+print("exact", np.array_equal(got.view(np.uint32), want[1].view(np.uint32)))
+'''
+    env = dict(os.environ, PHYSIS_B200_CSRC=str(tmp_path), PYTHONPATH=root)
+    out = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True,
+                         cwd=root, timeout=600)
+    assert out.returncode == 0, out.stderr
+    assert "compiled False" in out.stdout and "exact True" in out.stdout, out.stdout
