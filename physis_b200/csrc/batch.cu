@@ -281,90 +281,38 @@ __device__ bool wait_item_deps(const BatchDev &B, const BMember &M, int s, int t
   return true;
 }
 
-// The same test as wait_item_deps without waiting: whether the item's
-// dependencies are met now (with acquire ordering when they are).
-__device__ bool item_deps_ready(const BatchDev &B, const BMember &M, int s, int t, int units,
-                                bool after_check, bool wrap) {
-  const unsigned full = (unsigned)M.ntiles * units;
-  const unsigned *cnt = M.step_cnt + (s - 1);
-  if (after_check) return ld_acquire(cnt) >= full + 1u;
-  if (ld_acquire(cnt) >= full) return true;
-  if (M.ntiles < kWaveTiles) return false;
-  const int tx = M.tiles_x, ty = M.tiles_y, tz = M.nzc;
-  const int cx = t % tx, cy = (t / tx) % ty, cz = t / (tx * ty);
-  const unsigned need = (unsigned)s * units;
-  bool ready = true;
-#pragma unroll
-  for (int k = 0; k < 27; k++) {
-    int x = cx + k % 3 - 1, y = cy + (k / 3) % 3 - 1, z = cz + k / 9 - 1;
-    bool in = true;
-    if (x < 0 || x >= tx) { in = wrap; x = (x + tx) % tx; }
-    if (y < 0 || y >= ty) { in = in && wrap; y = (y + ty) % ty; }
-    if (z < 0 || z >= tz) { in = in && wrap; z = (z + tz) % tz; }
-    if (in && ld_relaxed(M.tile_done + (x + tx * (y + ty * z))) < need) ready = false;
-  }
-  if (ready) asm volatile("fence.acq_rel.gpu;" ::: "memory");
-  return ready;
-}
-
-// An item as the producer sees it: where it is in the work list, whether
-// its dependencies were already met when it was located, and its flags.
-struct ProducerItem {
-  int m, s, t, flags;
-  bool ready;
-};
-
 // Producer thread: takes items (from the shared cursor, or item `blockIdx.x`
 // of `step` when step >= 0), waits until the item's member has completed
 // its previous step, hands the item to the consumers through the descriptor
 // queue and streams its input planes into the ring. It runs ahead of the
-// consumers by up to the ring's depth, across item boundaries. The next
-// item is claimed and located (and its dependencies tested without
-// waiting) before the current item's planes are issued, while the ring is
-// usually full, so the step from one item's last plane to the next item's
-// first one is short; a dependency not met then is waited for only after
-// the current item's planes are out (the current item may be one of them).
+// consumers by up to the ring's depth, across item boundaries.
 template <int GROUP>
 __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, const Ring &RC,
                               uint64_t *qfull, uint64_t *qempty, ItemDesc *desc) {
   RingPos pos{0, 0}, cpos{0, 0};
   bool ok = true;
-  // Claim and locate one item; dependencies are tested, not waited for.
-  auto locate = [&](long long item) -> ProducerItem {
-    ProducerItem p{0, 0, 0, 0, true};
-    if (item >= B.total_items || ld_acquire_int(B.err) != 0) {
-      p.flags = kItemEnd;
-      return p;
-    }
-    p.s = upper_index(B.step_offset, B.max_steps + 1, item);
-    const int64_t local = item - __ldg(B.step_offset + p.s);
-    const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
-    p.m = __ldg(B.order + k);
-    p.t = (int)(local - __ldg(B.tile_prefix + k));
-    const BMember &M = B.members[p.m];
-    if (p.s > 0)
-      p.ready = item_deps_ready(B, M, p.s, p.t, kBWarps, is_check_step<GROUP>(M, M.step0 + p.s - 1),
-                                GROUP == 0 && M.kind == BK_DIFF7P);
-    if (p.ready) {
-      const int st = ld_acquire_int(M.stop);
-      if (st >= 0 && p.s >= st) p.flags = kItemSkip;
-    }
-    return p;
-  };
-  auto claim = [&](uint32_t nq) -> long long {
-    if (step >= 0)
-      return nq == 0 ? (long long)B.step_offset[step] + blockIdx.x : (long long)B.total_items;
-    return (long long)atomicAdd(B.cursor, 1ull);
-  };
-  ProducerItem next = locate(claim(0));
   for (uint32_t nq = 0;; nq++) {
-    const ProducerItem cur = next;
-    int m = cur.m, s = cur.s, t = cur.t, flags = cur.flags;
-    const BMember *M = flags & kItemEnd ? nullptr : &B.members[m];
-    if (!(flags & kItemEnd) && !cur.ready) {
+    long long item;
+    if (step >= 0)
+      item = nq == 0 ? (long long)B.step_offset[step] + blockIdx.x : (long long)B.total_items;
+    else
+      item = (long long)atomicAdd(B.cursor, 1ull);
+    int m = 0, s = 0, t = 0, flags = 0;
+    const BMember *M = nullptr;
+    if (item >= B.total_items || ld_acquire_int(B.err) != 0) {
+      flags = kItemEnd;
+    } else {
+      s = upper_index(B.step_offset, B.max_steps + 1, item);
+      const int64_t local = item - __ldg(B.step_offset + s);
+      const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
+      m = __ldg(B.order + k);
+      t = (int)(local - __ldg(B.tile_prefix + k));
+      M = &B.members[m];
       // Dependencies on step s-1 of the member (wait_item_deps).
-      ok = wait_item_deps(B, *M, s, t, kBWarps, is_check_step<GROUP>(*M, M->step0 + s - 1),
-                          GROUP == 0 && M->kind == BK_DIFF7P);
+      if (s > 0)
+        ok = wait_item_deps(B, *M, s, t, kBWarps,
+                            is_check_step<GROUP>(*M, M->step0 + s - 1),
+                            GROUP == 0 && M->kind == BK_DIFF7P);
       if (!ok) {
         flags = kItemEnd;
       } else {
@@ -383,7 +331,6 @@ __device__ void batch_produce(const BatchDev &B, int step, const Ring &R, const 
     desc[q].flags = flags;
     mbar_arrive(&qfull[q]);  // release: the descriptor is visible to the consumers
     if (flags & kItemEnd) break;
-    next = locate(claim(nq + 1));
     if (flags & kItemSkip) continue;
     // The step's inputs were written by generic stores of other CTAs and
     // acquired above; order that before the async-proxy (TMA) reads.
@@ -636,40 +583,24 @@ __device__ void t2_produce(const BatchDev &B, int step, const HtRings &R, uint64
                            uint64_t *qempty, ItemDesc *desc) {
   RingPos p1{0, 0}, pc{0, 0};
   bool ok = true;
-  // As in batch_produce: the next item is located before the current one's
-  // planes are issued; a dependency not met then is waited for afterwards.
-  auto locate = [&](long long item) -> ProducerItem {
-    ProducerItem p{0, 0, 0, 0, true};
-    if (item >= B.total_items || ld_acquire_int(B.err) != 0) {
-      p.flags = kItemEnd;
-      return p;
-    }
-    p.s = upper_index(B.step_offset, B.max_steps + 1, item);
-    const int64_t local = item - __ldg(B.step_offset + p.s);
-    const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
-    p.m = __ldg(B.order + k);
-    p.t = (int)(local - __ldg(B.tile_prefix + k));
-    const BMember &M = B.members[p.m];
-    if (p.s > 0)
-      p.ready = item_deps_ready(B, M, p.s, p.t, kT2Units, pass_checked(M, p.s - 1), false);
-    if (p.ready) {
-      const int st = ld_acquire_int(M.stop);
-      if (st >= 0 && __ldg(M.pass_start + p.s) >= st) p.flags = kItemSkip;
-    }
-    return p;
-  };
-  auto claim = [&](uint32_t nq) -> long long {
-    if (step >= 0)
-      return nq == 0 ? (long long)B.step_offset[step] + blockIdx.x : (long long)B.total_items;
-    return (long long)atomicAdd(B.cursor, 1ull);
-  };
-  ProducerItem next = locate(claim(0));
   for (uint32_t nq = 0;; nq++) {
-    const ProducerItem cur = next;
-    int m = cur.m, s = cur.s, t = cur.t, flags = cur.flags;
-    const BMember *M = flags & kItemEnd ? nullptr : &B.members[m];
-    if (!(flags & kItemEnd) && !cur.ready) {
-      ok = wait_item_deps(B, *M, s, t, kT2Units, pass_checked(*M, s - 1), false);
+    long long item;
+    if (step >= 0)
+      item = nq == 0 ? (long long)B.step_offset[step] + blockIdx.x : (long long)B.total_items;
+    else
+      item = (long long)atomicAdd(B.cursor, 1ull);
+    int m = 0, s = 0, t = 0, flags = 0;
+    const BMember *M = nullptr;
+    if (item >= B.total_items || ld_acquire_int(B.err) != 0) {
+      flags = kItemEnd;
+    } else {
+      s = upper_index(B.step_offset, B.max_steps + 1, item);
+      const int64_t local = item - __ldg(B.step_offset + s);
+      const int k = upper_index(B.tile_prefix, B.nmembers + 1, local);
+      m = __ldg(B.order + k);
+      t = (int)(local - __ldg(B.tile_prefix + k));
+      M = &B.members[m];
+      if (s > 0) ok = wait_item_deps(B, *M, s, t, kT2Units, pass_checked(*M, s - 1), false);
       if (!ok) {
         flags = kItemEnd;
       } else {
@@ -688,7 +619,6 @@ __device__ void t2_produce(const BatchDev &B, int step, const HtRings &R, uint64
     desc[q].flags = flags;
     mbar_arrive(&qfull[q]);
     if (flags & kItemEnd) break;
-    next = locate(claim(nq + 1));
     if (flags & kItemSkip) continue;
     asm volatile("fence.proxy.async.global;" ::: "memory");
     const int par = (M->cur0 + s) & 1;
