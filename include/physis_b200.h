@@ -557,15 +557,17 @@ typedef enum {
   PSB_IMPL_GENERIC = 3        /* the generic term-table kernel */
 } psb_impl;
 psb_status psb_set_impl(int impl);
-/* Arithmetic of the 7-point TMA kernels (no counterpart in the reference,
- * whose CUDA target compiles with nvcc's default contraction).
+/* Arithmetic of the 7-point TMA kernels and of generic tables compiled at
+ * run time whose terms are one read times a constant (no counterpart in the
+ * reference, whose CUDA target compiles with nvcc's default contraction).
  * PSB_FP_EXACT (default): every product and sum rounded in the reference's
  * term order -- bit-identical to the reference CPU target built without FMA
  * contraction. PSB_FP_FMA: the same term order with each term after the
  * first added by a fused multiply-add (one rounding per term instead of
- * two); within 4 ulp of the exact form per step. Also set by the
- * environment variable PHYSIS_B200_FP_MODE=fma. The plain, Himeno, generic
- * and batched kernels always use the exact form. */
+ * two); for the 7-point kernels within 4 ulp of the exact form per step.
+ * Also set by the environment variable PHYSIS_B200_FP_MODE=fma. The plain,
+ * Himeno, batched and interpreting generic kernels always use the exact
+ * form. */
 enum { PSB_FP_EXACT = 0, PSB_FP_FMA = 1 };
 psb_status psb_set_fp_mode(int mode);
 psb_status psb_get_fp_mode(int *mode);

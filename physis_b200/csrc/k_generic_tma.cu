@@ -119,9 +119,10 @@ static std::string gt_factor_src(const GtFactor &f, const char *side, int t) {
          std::to_string(f.off) + ", 0, tab." + side + "[" + std::to_string(t) + "].c}";
 }
 
-static std::string gt_jit_source(const GtTable &tab, bool dbl, std::string *key) {
+static std::string gt_jit_source(const GtTable &tab, bool dbl, bool fma, std::string *key) {
   const char *T = dbl ? "double" : "float";
-  std::string body, k = std::string(T) + (tab.simple ? ":p:" : ":g:");
+  fma = fma && tab.simple;  // the contracted form exists for packed tables
+  std::string body, k = std::string(T) + (tab.simple ? (fma ? ":pf:" : ":p:") : ":g:");
   for (int t = 0; t < tab.nterms; t++) {
     if (tab.simple) {
       const int w = tab.word[t];
@@ -132,8 +133,9 @@ static std::string gt_jit_source(const GtTable &tab, bool dbl, std::string *key)
                 ((w >> 8) & 1 ? "true" : "false") + ", " + ((w >> 9) & 1 ? "true" : "false") +
                 ", row);\n";
       body += "    gt_term<" + std::to_string((w >> 3) & 7) + ", " +
-              ((w >> 7) & 1 ? "true" : "false") + ", " + (t == 0 ? "true" : "false") +
-              ">(row, gt_coef(tab, " + std::to_string(t) + ", T()), acc);\n";
+              ((w >> 7) & 1 ? "true" : "false") + ", " + (t == 0 ? "true" : "false") + ", " +
+              (fma ? "true" : "false") + ">(row, gt_coef(tab, " + std::to_string(t) +
+              ", T()), acc);\n";
     } else {
       const GtFactor &a = tab.a[t], &b = tab.b[t];
       k += std::to_string(a.kind) + "." + std::to_string(a.k) + "." + std::to_string(a.off) + "*" +
@@ -166,10 +168,11 @@ static std::string gt_jit_source(const GtTable &tab, bool dbl, std::string *key)
 // The compiled kernel of a table, or nullptr (the interpreting kernel
 // runs). Never compiles while the stream is being captured: the first
 // iteration of every run is eager, so a captured one finds its kernel cached.
-static CUfunction gt_jit(const GtTable &tab, bool dbl, cudaStream_t s, size_t smem_optin) {
+static CUfunction gt_jit(const GtTable &tab, bool dbl, bool fma, cudaStream_t s,
+                         size_t smem_optin) {
   if (!generic_compile_on()) return nullptr;
   std::string key;
-  const std::string src = gt_jit_source(tab, dbl, &key);
+  const std::string src = gt_jit_source(tab, dbl, fma, &key);
   CUfunction fn = nullptr;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
@@ -279,7 +282,7 @@ static psb_status gt_launch(MapImpl &m, const psb_generic_stencil &desc, const G
     if (p.mode[i] != PSB_BOUNDARY_NONE && g->ghost_valid != p.mode[i])
       PSB_CHECK(launch_halo_fill(g, p.mode[i], s));
   }
-  CUfunction fn = gt_jit(tab, sizeof(T) == 8, s, r.smem_optin);
+  CUfunction fn = gt_jit(tab, sizeof(T) == 8, r.fp_mode == PSB_FP_FMA, s, r.smem_optin);
   GridView ov = og->view();
   if (fn) {
     void *args[] = {&maps, &tab, &ov, &d, &geo, &r.d_error};

@@ -143,8 +143,11 @@ __device__ __forceinline__ void gt_row_load(const T *p, int lane, bool need_n, b
 // offset DXP2 - 2), times c unless ONE, added to the running sum (FIRST:
 // starts it, as the reference's sum starts from its first term). Float
 // products go in pairs through the sm_100 f32x2 multiply (each lane rounded
-// like the scalar one); the sums stay scalar.
-template <int DXP2, bool ONE, bool FIRST>
+// like the scalar one); the sums stay scalar. FMA (the contracted arithmetic
+// mode, compiled kernels only): a term after the first is added with one
+// rounding, c * x + sum fused (paired for float); the first product and
+// unmultiplied terms round as in the exact form.
+template <int DXP2, bool ONE, bool FIRST, bool FMA = false>
 __device__ __forceinline__ void gt_term(const GtRow<float> (&row)[kGtVY], float c,
                                         GtBlk<float> &acc) {
   const float2 cc = make_float2(c, c);
@@ -152,6 +155,16 @@ __device__ __forceinline__ void gt_term(const GtRow<float> (&row)[kGtVY], float 
   for (int r = 0; r < kGtVY; r++) {
     float2 lo = make_float2(row[r].e[DXP2], row[r].e[DXP2 + 1]);
     float2 hi = make_float2(row[r].e[DXP2 + 2], row[r].e[DXP2 + 3]);
+    if (FMA && !FIRST && !ONE) {
+      // The contracted form: acc + c * x with one rounding (paired).
+      const float2 a = __ffma2_rn(cc, lo, make_float2(acc.v[r][0], acc.v[r][1]));
+      const float2 b = __ffma2_rn(cc, hi, make_float2(acc.v[r][2], acc.v[r][3]));
+      acc.v[r][0] = a.x;
+      acc.v[r][1] = a.y;
+      acc.v[r][2] = b.x;
+      acc.v[r][3] = b.y;
+      continue;
+    }
     if (!ONE) {
       if (PSB_GT_PACKED_MUL == 2 || (PSB_GT_PACKED_MUL == 1 && DXP2 % 2 == 0)) {
         lo = __fmul2_rn(cc, lo);
@@ -175,7 +188,7 @@ __device__ __forceinline__ void gt_term(const GtRow<float> (&row)[kGtVY], float 
   }
 }
 
-template <int DXP2, bool ONE, bool FIRST>
+template <int DXP2, bool ONE, bool FIRST, bool FMA = false>
 __device__ __forceinline__ void gt_term(const GtRow<double> (&row)[kGtVY], double c,
                                         GtBlk<double> &acc) {
 #pragma unroll
@@ -183,6 +196,10 @@ __device__ __forceinline__ void gt_term(const GtRow<double> (&row)[kGtVY], doubl
 #pragma unroll
     for (int j = 0; j < 2; j++) {
       double v = row[r].e[DXP2 + j];
+      if (FMA && !FIRST && !ONE) {
+        acc.v[r][j] = __fma_rn(c, v, acc.v[r][j]);
+        continue;
+      }
       if (!ONE) v = xmul(c, v);
       acc.v[r][j] = FIRST ? v : xadd(acc.v[r][j], v);
     }

@@ -1,4 +1,5 @@
-"""The contracted (FMA) arithmetic of the 7-point TMA kernels (PSB_FP_FMA).
+"""The contracted (FMA) arithmetic (PSB_FP_FMA) of the 7-point TMA kernels
+and of generic tables compiled at run time (bound stated at the end).
 
 Not bit-identical to the reference by design: the reference's term order
 with one rounding per term instead of two. The stated tolerance is 4 ulp
@@ -125,3 +126,75 @@ def test_mode_switch_and_exact_default():
     want = oracle.diffusion7(f, 4, np.asarray(COEF, np.float32))
     _run(f, 4)  # FMA run, then back to exact: the exact run is bit-exact again
     assert U.bits_equal(U.diffusion_gpu(f, 4, COEF, impl=ps.IMPL_TMA), want)
+
+
+# ---------------------------------------------------------------------------
+# Generic tables compiled at run time (psb_generic_tma_compiled)
+# ---------------------------------------------------------------------------
+def _positive_table(rng, nterms, typ):
+    """A read-times-constant table over one grid with positive coefficients
+    (so partial sums grow and every rounding is at most half an ulp of the
+    result), offsets within +-2, some terms unmultiplied."""
+    terms = []
+    for i in range(nterms):
+        off = tuple(int(v) for v in rng.integers(-2, 3, size=3))
+        if i % 5 == 3:
+            terms.append(ps.get(0, off))
+        else:
+            terms.append((ps.const(float(np.float32(0.01 + 0.2 * rng.random()))), ps.get(0, off)))
+    return ps.GenericStencil(3, [(typ, (0, 1, 2))] * 2, 1, typ, terms), terms
+
+
+def _exact_generic(f, terms, lo, hi):
+    """The table's value at every domain point in extended precision from the
+    same inputs (coefficients rounded to the field's type)."""
+    e = np.zeros(f.shape, dtype=np.longdouble)
+    fx = f.astype(np.longdouble)
+    (x0, y0, z0), (x1, y1, z1) = lo, hi
+    for t in terms:
+        if t[0] == "g":
+            c, g = np.longdouble(1), t
+        else:
+            c, g = np.longdouble(np.asarray(t[0][1], dtype=f.dtype)), t[1]
+        dx, dy, dz = g[2]
+        e[z0:z1, y0:y1, x0:x1] += c * fx[z0 + dz:z1 + dz, y0 + dy:y1 + dy, x0 + dx:x1 + dx]
+    return e[z0:z1, y0:y1, x0:x1]
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+@pytest.mark.parametrize("nterms", [5, 13, 27])
+def test_generic_compiled_fma_within_the_rounding_bound(nterms, dtype):
+    """FMA mode on a compiled packed table: one step from the same input lies
+    within nterms/2 + 1 ulp of the extended-precision value (each of the
+    nterms roundings is at most half an ulp of the growing positive sum),
+    and the exact mode, switched back, equals the oracle port bit for bit."""
+    ps.PSInit()
+    rng = np.random.default_rng(40 + nterms)
+    typ = ps.PS_FLOAT if dtype == np.float32 else ps.PS_DOUBLE
+    st, terms = _positive_table(rng, nterms, typ)
+    n = (52, 36, 30)
+    f = (0.5 + 0.5 * rng.random(n[::-1])).astype(dtype)
+    lo, hi = (2, 2, 2), (n[0] - 2, n[1] - 2, n[2] - 2)
+    outs = {}
+    try:
+        for mode in (ps.FP_FMA, ps.FP_EXACT):
+            ps.set_fp_mode(mode)
+            g = [ps.grid_new(typ, n) for _ in range(2)]
+            ps.PSGridCopyin(g[0], f)
+            ps.PSGridCopyin(g[1], f)
+            m = ps.PSStencilMap(st.kernel_id, ps.PSDomain3DNew(lo[0], hi[0], lo[1], hi[1], lo[2],
+                                                               hi[2]), g[0], g[1])
+            ps.PSStencilRun(m, 1)
+            assert ps.generic_last_compiled()
+            outs[mode] = ps.PSGridCopyout(g[1])
+            for x in g:
+                ps.PSGridFree(x)
+    finally:
+        ps.set_fp_mode(ps.FP_EXACT)
+    exact = _exact_generic(f, terms, lo, hi)
+    sl = (slice(lo[2], hi[2]), slice(lo[1], hi[1]), slice(lo[0], hi[0]))
+    assert _ulp_err(outs[ps.FP_FMA][sl], exact) <= nterms / 2 + 1
+    want = [f.copy(), f.copy()]
+    oracle.generic_apply(st.struct, want, list(lo), list(hi))
+    assert U.bits_equal(outs[ps.FP_EXACT], want[1])
+    assert not U.bits_equal(outs[ps.FP_FMA], outs[ps.FP_EXACT])  # the modes differ
