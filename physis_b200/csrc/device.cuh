@@ -26,25 +26,6 @@ __device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b)
 __device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
 __device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
 __device__ __forceinline__ double xsub(double a, double b) { return __dsub_rn(a, b); }
-// Paired float forms (sm_100 f32x2): per lane a * b and a + b, each rounded
-// to nearest, as inline PTX with an explicit rounding mode, which the
-// compiler never contracts into a fused multiply-add.
-__device__ __forceinline__ float2 xmul2(float2 a, float2 b) {
-  float2 r;
-  asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-      "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
-__device__ __forceinline__ float2 xadd2(float2 a, float2 b) {
-  float2 r;
-  asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-      "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-      : "=f"(r.x), "=f"(r.y)
-      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-  return r;
-}
 __device__ __forceinline__ int32_t xmul(int32_t a, int32_t b) { return a * b; }
 __device__ __forceinline__ int64_t xmul(int64_t a, int64_t b) { return a * b; }
 __device__ __forceinline__ int32_t xadd(int32_t a, int32_t b) { return a + b; }

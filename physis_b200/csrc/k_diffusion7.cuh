@@ -82,17 +82,9 @@ __device__ __forceinline__ K7<T> make_k7(const C7<T> &c) {
   return k;
 }
 
-#ifndef PSB_D7_PAIRED_EXACT
-#define PSB_D7_PAIRED_EXACT 0
-#endif
 __device__ __forceinline__ void mul4(float2 k, const Vec16<float> &x, float *p) {
-#if PSB_D7_PAIRED_EXACT
-  const float2 lo = xmul2(k, make_float2(x.v[0], x.v[1]));
-  const float2 hi = xmul2(k, make_float2(x.v[2], x.v[3]));
-#else
   const float2 lo = __fmul2_rn(k, make_float2(x.v[0], x.v[1]));
   const float2 hi = __fmul2_rn(k, make_float2(x.v[2], x.v[3]));
-#endif
   p[0] = lo.x;
   p[1] = lo.y;
   p[2] = hi.x;
@@ -191,19 +183,6 @@ __device__ __forceinline__ Vec16<T> diff7_row(const K7<T> &k, const Vec16<T> &c,
       if (xfix & (1u << v)) pe[v] = pce[v];
   }
   Vec16<T> r;
-#if PSB_D7_PAIRED_EXACT
-  if constexpr (sizeof(T) == 4) {
-#pragma unroll
-    for (int v = 0; v < V; v += 2) {
-      auto f2 = [&](const T *a) { return make_float2(a[v], a[v + 1]); };
-      const float2 q = xadd2(xadd2(xadd2(xadd2(xadd2(xadd2(f2(pcc), f2(pw)), f2(pe)), f2(ps)),
-                                           f2(pn)), f2(pb)), f2(pt));
-      r.v[v] = q.x;
-      r.v[v + 1] = q.y;
-    }
-    return r;
-  }
-#endif
 #pragma unroll
   for (int v = 0; v < V; v++)
     r.v[v] = xadd(xadd(xadd(xadd(xadd(xadd(pcc[v], pw[v]), pe[v]), ps[v]), pn[v]), pb[v]), pt[v]);

@@ -146,7 +146,7 @@ static std::string gt_jit_source(const GtTable &tab, bool dbl, bool fma, std::st
     }
   }
   *key = "k_generic_tma:" + k + "vy" + std::to_string(kGtVY) + "pm" +
-         std::to_string(PSB_GT_PACKED_MUL) + "pa" + std::to_string(PSB_GT_PAIRED_ADD);
+         std::to_string(PSB_GT_PACKED_MUL);
   std::string src = "#include \"k_generic_tma.cuh\"\nnamespace psb {\nstruct GtCompiledProg {\n"
                     "  static constexpr bool kCompiled = true;\n  template <typename T>\n"
                     "  static __device__ __forceinline__ void eval(const GtTable &tab, "
@@ -178,8 +178,7 @@ static CUfunction gt_jit(const GtTable &tab, bool dbl, bool fma, cudaStream_t s,
   if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
     return rtc_cached(key, &fn) == PSB_OK ? fn : nullptr;  // no compile or module load here
   const std::vector<std::string> opts = {"-DPSB_GT_VY=" + std::to_string(kGtVY),
-                                         "-DPSB_GT_PACKED_MUL=" + std::to_string(PSB_GT_PACKED_MUL),
-                                         "-DPSB_GT_PAIRED_ADD=" + std::to_string(PSB_GT_PAIRED_ADD)};
+                                         "-DPSB_GT_PACKED_MUL=" + std::to_string(PSB_GT_PACKED_MUL)};
   if (rtc_function(key, src, "psb_generic_tma_compiled", opts, (int)smem_optin, &fn) != PSB_OK)
     return nullptr;
   return fn;

@@ -22,11 +22,6 @@ constexpr int kGtR = 2;          // largest |offset| per axis (the pitched halo)
 #ifndef PSB_GT_PACKED_MUL
 #define PSB_GT_PACKED_MUL 1
 #endif
-// 3: every product through xmul2 (explicitly rounded inline PTX). Paired
-// sums (PSB_GT_PAIRED_ADD) go through xadd2.
-#ifndef PSB_GT_PAIRED_ADD
-#define PSB_GT_PAIRED_ADD 0
-#endif
 constexpr int kGtVY = PSB_GT_VY;  // rows per consumer thread
 constexpr int kGtConsumers = 128;
 constexpr int kGtThreads = kGtConsumers + 32;
@@ -171,10 +166,7 @@ __device__ __forceinline__ void gt_term(const GtRow<float> (&row)[kGtVY], float 
       continue;
     }
     if (!ONE) {
-      if (PSB_GT_PACKED_MUL == 3) {
-        lo = xmul2(cc, lo);
-        hi = xmul2(cc, hi);
-      } else if (PSB_GT_PACKED_MUL == 2 || (PSB_GT_PACKED_MUL == 1 && DXP2 % 2 == 0)) {
+      if (PSB_GT_PACKED_MUL == 2 || (PSB_GT_PACKED_MUL == 1 && DXP2 % 2 == 0)) {
         lo = __fmul2_rn(cc, lo);
         hi = __fmul2_rn(cc, hi);
       } else {
@@ -187,14 +179,7 @@ __device__ __forceinline__ void gt_term(const GtRow<float> (&row)[kGtVY], float 
       acc.v[r][1] = lo.y;
       acc.v[r][2] = hi.x;
       acc.v[r][3] = hi.y;
-    } else if (PSB_GT_PAIRED_ADD) {
-      const float2 a = xadd2(make_float2(acc.v[r][0], acc.v[r][1]), lo);
-      const float2 b = xadd2(make_float2(acc.v[r][2], acc.v[r][3]), hi);
-      acc.v[r][0] = a.x;
-      acc.v[r][1] = a.y;
-      acc.v[r][2] = b.x;
-      acc.v[r][3] = b.y;
-    } else {  // scalar adds
+    } else {  // scalar adds: paired f32x2 adds gave results 1 ulp off the scalar sums
       acc.v[r][0] = xadd(acc.v[r][0], lo.x);
       acc.v[r][1] = xadd(acc.v[r][1], lo.y);
       acc.v[r][2] = xadd(acc.v[r][2], hi.x);
