@@ -505,6 +505,14 @@ typedef struct {
 } psb_launch_args;
 
 typedef psb_status (*psb_compiled_launch)(const psb_launch_args *args, void *cuda_stream);
+/* The staged form of a compiled stencil: its body run over the library's TMA
+ * plane ring (the kernel body of the generic TMA path, csrc/k_generic_tma.cuh).
+ * The library prepares the tensor maps, table, output view, domain and ring
+ * geometry (opaque here; layouts of that header) and the launch shape. */
+typedef psb_status (*psb_compiled_staged)(const void *maps, const void *table, const void *out,
+                                          const void *domain, const void *geometry, int *error,
+                                          unsigned blocks, unsigned shared_bytes,
+                                          void *cuda_stream);
 
 typedef struct {
   int ndims;                          /* index parameters of the function */
@@ -521,9 +529,26 @@ typedef struct {
   int param_type[PSB_MAX_PARAMS];     /* PS_FLOAT / PS_DOUBLE / PS_INT / PS_LONG
                                          (how PSStencilMap's varargs read them) */
   psb_compiled_launch launch;
+  /* Optional staged form (staged != NULL): a 3-D function of one element
+   * type (staged_type, PS_FLOAT or PS_DOUBLE) over primitive grids that
+   * emits, once and unconditionally, into grid staged_emit (which it does
+   * not read) and reads every other grid only at constant offsets within
+   * +-2 of the point, between read_lo and read_hi per axis (read_lo > read_hi
+   * on axis 0: the grid is not read). The library runs it when the map fits
+   * (whole domain reads inside every grid, TMA-ready layouts, no red-black
+   * colour, at most four grids read) and otherwise calls `launch`. */
+  int staged_type;
+  int staged_emit;
+  int read_lo[PSB_MAX_GRIDS][3];
+  int read_hi[PSB_MAX_GRIDS][3];
+  psb_compiled_staged staged;
 } psb_compiled_stencil;
 
 psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_id);
+/* Whether the last application of a compiled stencil ran its staged form
+ * (1) or its own thread-per-point launch (0). psb_set_impl(PSB_IMPL_PLAIN or
+ * PSB_IMPL_GENERIC) keeps compiled stencils on their own launch. */
+psb_status psb_compiled_last_staged(int *staged);
 
 /* Register stencil function `name` of a kernel library made by the front end
  * (which exports psb_dsl_describe_<name>); *status_out gets the status. */

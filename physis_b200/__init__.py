@@ -119,7 +119,10 @@ class CompiledStencilStruct(ctypes.Structure):
                 ("view_type", ctypes.c_int * PSB_MAX_VIEWS),
                 ("view_emits", ctypes.c_int * PSB_MAX_VIEWS),
                 ("view_reads_offset", ctypes.c_int * PSB_MAX_VIEWS), ("nparams", ctypes.c_int),
-                ("param_type", ctypes.c_int * PSB_MAX_PARAMS), ("launch", ctypes.c_void_p)]
+                ("param_type", ctypes.c_int * PSB_MAX_PARAMS), ("launch", ctypes.c_void_p),
+                ("staged_type", ctypes.c_int), ("staged_emit", ctypes.c_int),
+                ("read_lo", (ctypes.c_int * 3) * PSB_MAX_GRIDS),
+                ("read_hi", (ctypes.c_int * 3) * PSB_MAX_GRIDS), ("staged", ctypes.c_void_p)]
 
 
 class TuneConfig(ctypes.Structure):
@@ -251,6 +254,7 @@ def _load():
         "psb_set_fp_mode": (S, [ctypes.c_int]),
         "psb_set_generic_compile": (S, [ctypes.c_int]),
         "psb_generic_last_compiled": (S, [ctypes.POINTER(ctypes.c_int)]),
+        "psb_compiled_last_staged": (S, [ctypes.POINTER(ctypes.c_int)]),
         "psb_get_fp_mode": (S, [ctypes.POINTER(ctypes.c_int)]),
         "psb_batch_member_layout": (S, [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(BatchLayout)]),
         "psb_batch_autotune": (S, [ctypes.c_void_p, ctypes.c_int]),
@@ -604,6 +608,14 @@ def get_fp_mode():
 def set_generic_compile(on):
     """Run-time compilation of generic tables on the TMA path (default on)."""
     check(lib.psb_set_generic_compile(1 if on else 0), "psb_set_generic_compile")
+
+
+def compiled_last_staged():
+    """Whether the last application of a compiled (DSL) stencil ran its staged
+    (TMA plane ring) form."""
+    v = ctypes.c_int()
+    check(lib.psb_compiled_last_staged(ctypes.byref(v)), "psb_compiled_last_staged")
+    return bool(v.value)
 
 
 def generic_last_compiled():

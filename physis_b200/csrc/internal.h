@@ -220,6 +220,12 @@ double now_s();
 // sm_100a from `source` (which may include the library's device headers),
 // cached per device and key; PSB_ERR_UNSUPPORTED when NVRTC, the headers or
 // the compile are unavailable (the caller keeps its own kernel).
+// The staged form of a compiled stencil (k_generic_tma.cu):
+// PSB_ERR_UNSUPPORTED when the map does not fit it (the caller then runs the
+// stencil's own launch).
+psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, GridImpl **views,
+                                  int color, cudaStream_t s);
+
 bool rtc_available();
 psb_status rtc_function(const std::string &key, const std::string &source, const char *name,
                         const std::vector<std::string> &options, int smem_bytes,

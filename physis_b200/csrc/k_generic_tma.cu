@@ -148,7 +148,8 @@ static std::string gt_jit_source(const GtTable &tab, bool dbl, bool fma, std::st
   *key = "k_generic_tma:" + k + "vy" + std::to_string(kGtVY) + "pm" +
          std::to_string(PSB_GT_PACKED_MUL);
   std::string src = "#include \"k_generic_tma.cuh\"\nnamespace psb {\nstruct GtCompiledProg {\n"
-                    "  static constexpr bool kCompiled = true;\n  template <typename T>\n"
+                    "  static constexpr bool kCompiled = true;\n"
+                    "  static constexpr bool kPoints = false;\n  template <typename T>\n"
                     "  static __device__ __forceinline__ void eval(const GtTable &tab, "
                     "const unsigned char *ring, int sbytes, int S, int slot0, int thr_off, "
                     "int bx, int lane, GtBlk<T> &acc) {\n";
@@ -184,18 +185,13 @@ static CUfunction gt_jit(const GtTable &tab, bool dbl, bool fma, cudaStream_t s,
   return fn;
 }
 
+// Geometry, tensor maps and grid size of a TMA launch over the staged grids
+// of plan p (the map's grids at p.slots), writing `og` over domain d.
 template <typename T>
-static psb_status gt_launch(MapImpl &m, const psb_generic_stencil &desc, const GtPlan &p,
-                            cudaStream_t s, int64_t *launches) {
+static psb_status gt_geometry(MapImpl &m, const GtPlan &p, GridImpl *og, const Dom3 &d,
+                              GtGeom &geo, GtMaps &maps, int64_t *nblocks_out) {
   constexpr int V = 16 / sizeof(T);
   Runtime &r = rt();
-  GridImpl *og = m.grids[desc.out_grid];
-  Dom3 d;
-  for (int i = 0; i < 3; i++) {
-    d.lo[i] = m.dom.local_min[i];
-    d.hi[i] = m.dom.local_max[i];
-  }
-  GtGeom geo;
   memset(&geo, 0, sizeof(geo));
   geo.tx_threads = 32;
   const int TX = geo.tx_threads * V, TY = (kGtConsumers / geo.tx_threads) * kGtVY;
@@ -220,8 +216,7 @@ static psb_status gt_launch(MapImpl &m, const psb_generic_stencil &desc, const G
     geo.zchunk /= 2;
   const int nzc = (d.hi[2] - d.lo[2] + geo.zchunk - 1) / geo.zchunk;
   const int64_t nblocks = tiles * nzc;
-  if (nblocks > 0x7fffffff) return set_status(PSB_ERR_UNSUPPORTED);
-  GtMaps maps;
+  if (nblocks > 0x7fffffff) return PSB_ERR_UNSUPPORTED;
   memset(&maps, 0, sizeof(maps));
   for (int i = 0; i < p.ngrids; i++) {
     GridImpl *g = m.grids[p.slots[i]];
@@ -233,6 +228,24 @@ static psb_status gt_launch(MapImpl &m, const psb_generic_stencil &desc, const G
     geo.ay0[i] = pitched ? g->halo : 0;
     geo.az0[i] = pitched ? g->halo : 0;
   }
+  *nblocks_out = nblocks;
+  return PSB_OK;
+}
+
+template <typename T>
+static psb_status gt_launch(MapImpl &m, const psb_generic_stencil &desc, const GtPlan &p,
+                            cudaStream_t s, int64_t *launches) {
+  Runtime &r = rt();
+  GridImpl *og = m.grids[desc.out_grid];
+  Dom3 d;
+  for (int i = 0; i < 3; i++) {
+    d.lo[i] = m.dom.local_min[i];
+    d.hi[i] = m.dom.local_max[i];
+  }
+  GtGeom geo;
+  GtMaps maps;
+  int64_t nblocks = 0;
+  if (gt_geometry<T>(m, p, og, d, geo, maps, &nblocks) != PSB_OK) return PSB_ERR_UNSUPPORTED;
   GtTable tab;
   memset(&tab, 0, sizeof(tab));
   tab.nterms = desc.nterms;
@@ -326,6 +339,80 @@ psb_status generic_tma_launch(MapImpl &m, const GenericDesc &gd, int color, cuda
 
 void generic_note_impl(int impl) { g_last_generic_impl = impl; }
 
+static int g_last_compiled_staged = 0;
+
+template <typename T>
+static psb_status staged_run(MapImpl &m, const psb_compiled_stencil &cd, const GtPlan &p,
+                             GridImpl *og, const Dom3 &d, GtTable &tab, cudaStream_t s) {
+  Runtime &r = rt();
+  GtGeom geo;
+  GtMaps maps;
+  int64_t nblocks = 0;
+  if (gt_geometry<T>(m, p, og, d, geo, maps, &nblocks) != PSB_OK) return PSB_ERR_UNSUPPORTED;
+  const size_t smem = 128 + 512 + (size_t)geo.stages * geo.stage_bytes;
+  if (smem > r.smem_optin) return PSB_ERR_UNSUPPORTED;
+  for (int k = 0; k < PSB_MAX_TERMS && k < m.nparams; k++) {
+    tab.coef[k] = m.params[k];
+    tab.coef32[k] = (float)m.params[k];
+  }
+  GridView ov = og->view();
+  return cd.staged(&maps, &tab, &ov, &d, &geo, r.d_error, (unsigned)nblocks, (unsigned)smem,
+                   (void *)s);
+}
+
+// A compiled stencil's staged form: the map must read only grids of the
+// stencil's type that TMA can stage (at most four distinct ones), never the
+// grid it emits into, and stay inside every grid it reads over the whole
+// domain (so no read needs the bounds check of the thread-per-point form).
+psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, GridImpl **views,
+                                  int color, cudaStream_t s) {
+  g_last_compiled_staged = 0;
+  const Runtime &r = rt();
+  if (!cd.staged || r.impl == PSB_IMPL_PLAIN || r.impl == PSB_IMPL_GENERIC)
+    return PSB_ERR_UNSUPPORTED;
+  if (color >= 0 || cd.ndims != 3 || cd.nviews != cd.ngrids || m.nparams > PSB_MAX_TERMS)
+    return PSB_ERR_UNSUPPORTED;
+  GridImpl *og = views[cd.staged_emit];
+  if (og->type != cd.staged_type || og->pub.num_dims != 3) return PSB_ERR_UNSUPPORTED;
+  Dom3 d;
+  for (int i = 0; i < 3; i++) {
+    d.lo[i] = m.dom.local_min[i];
+    d.hi[i] = m.dom.local_max[i];
+    if (d.hi[i] <= d.lo[i]) return PSB_ERR_UNSUPPORTED;
+  }
+  GtPlan p;
+  GtTable tab;
+  memset(&tab, 0, sizeof(tab));
+  for (int i = 0; i < cd.ngrids; i++) {
+    GridImpl *g = views[i];
+    tab.slot_grid[i] = -1;
+    for (int k = 0; k < 3; k++) tab.slot_dims[i][k] = g->pub.dim[k];
+    if (cd.read_lo[i][0] > cd.read_hi[i][0]) continue;  // not read
+    if (g == og || g->type != cd.staged_type || g->pub.num_dims != 3 || !tma_eligible(g))
+      return PSB_ERR_UNSUPPORTED;
+    for (int k = 0; k < 3; k++)
+      if (d.lo[k] + cd.read_lo[i][k] < 0 || d.hi[k] - 1 + cd.read_hi[i][k] > g->pub.dim[k] - 1)
+        return PSB_ERR_UNSUPPORTED;
+    int gi = -1;
+    for (int j = 0; j < p.ngrids; j++)
+      if (views[p.slots[j]] == g) gi = j;
+    if (gi < 0) {
+      if (p.ngrids == kGtMaxGrids) return PSB_ERR_UNSUPPORTED;
+      gi = p.ngrids++;
+      p.slots[gi] = i;
+      p.mode[gi] = PSB_BOUNDARY_NONE;
+    }
+    tab.slot_grid[i] = gi;
+    p.zmin = std::min(p.zmin, cd.read_lo[i][2]);
+    p.zmax = std::max(p.zmax, cd.read_hi[i][2]);
+  }
+  if (p.ngrids == 0) return PSB_ERR_UNSUPPORTED;
+  const psb_status st = cd.staged_type == PS_FLOAT ? staged_run<float>(m, cd, p, og, d, tab, s)
+                                                   : staged_run<double>(m, cd, p, og, d, tab, s);
+  if (st == PSB_OK) g_last_compiled_staged = 1;
+  return st;
+}
+
 }  // namespace psb
 
 extern "C" psb_status psb_generic_last_impl(int *impl) {
@@ -337,6 +424,12 @@ extern "C" psb_status psb_generic_last_impl(int *impl) {
 extern "C" psb_status psb_generic_last_compiled(int *compiled) {
   if (!compiled) return psb::set_status(PSB_ERR_INVALID);
   *compiled = psb::g_last_generic_impl == PSB_IMPL_TMA ? psb::g_last_generic_compiled : 0;
+  return PSB_OK;
+}
+
+extern "C" psb_status psb_compiled_last_staged(int *staged) {
+  if (!staged) return psb::set_status(PSB_ERR_INVALID);
+  *staged = psb::g_last_compiled_staged;
   return PSB_OK;
 }
 

@@ -55,6 +55,11 @@ struct GtTable {
   int word[PSB_MAX_TERMS];
   double coef[PSB_MAX_TERMS];    // the constant factor in double grids' arithmetic
   float coef32[PSB_MAX_TERMS];   // ... converted to float once, for float grids
+  // Point-wise programs (stencil functions compiled by the DSL front end):
+  // the staged grid of each of the function's grid parameters (-1: not
+  // read) and the parameters' extents; `coef` holds the scalar arguments.
+  int slot_grid[PSB_MAX_GRIDS];
+  int slot_dims[PSB_MAX_GRIDS][3];
 };
 
 struct GtMaps {
@@ -275,9 +280,31 @@ __device__ __forceinline__ void gt_rows(const unsigned char *ring, int sbytes, i
   for (int r = 0; r < kGtVY; r++) gt_row_load(p + r * bx, lane, need_n, need_p, row[r]);
 }
 
+// Where a consumer thread's block of points sits in the window of staged
+// planes, for point-wise programs: the thread's first point (x, y, z), its
+// offset in a stage (thr_off) and the ring's geometry.
+struct GtAt {
+  const unsigned char *ring;
+  int sbytes, S, slot0, thr_off, bx, plane_elems, zmin;
+  int x, y, z;
+};
+
+// The staged value of grid slot `slot` at (x + dx, y + dy, z + dz) from the
+// point in row r, column v of the thread's block (offsets within the halo
+// the window holds).
+template <typename T>
+__device__ __forceinline__ T gt_staged(const GtTable &tab, const GtAt &at, int slot, int r, int v,
+                                       int dx, int dy, int dz) {
+  int sl = at.slot0 + dz - at.zmin;
+  if (sl >= at.S) sl -= at.S;
+  const T *p = reinterpret_cast<const T *>(at.ring + (size_t)sl * at.sbytes);
+  return p[tab.slot_grid[slot] * at.plane_elems + at.thr_off + (r + dy) * at.bx + v + dx];
+}
+
 // The library's term program: reads the packed table word by word.
 struct GtTableProg {
   static constexpr bool kCompiled = false;
+  static constexpr bool kPoints = false;
   template <typename T>
   static __device__ __forceinline__ void eval(const GtTable &tab, const unsigned char *ring,
                                               int sbytes, int S, int slot0, int thr_off, int bx,
@@ -302,7 +329,10 @@ struct GtTableProg {
 // program is fixed at compile time). Prog::eval evaluates the sum of the
 // terms; the library's program handles packed tables only (general ones take
 // the loop below), a compiled program (Prog::kCompiled) is the whole table,
-// packed or general. The post factor is applied here in both cases.
+// packed or general. The post factor is applied here in both cases. A
+// point-wise program (Prog::kPoints: a compiled stencil function) computes
+// each point of the thread's block itself from the staged window
+// (gt_staged) and emits into acc.
 template <typename T, class Prog>
 __device__ __forceinline__ void gt_body(const GtMaps &maps, const GtTable &tab,
                                         const GridView &out, const Dom3 &d, const GtGeom &geo,
@@ -386,7 +416,11 @@ __device__ __forceinline__ void gt_body(const GtMaps &maps, const GtTable &tab,
     }
     const int slot0 = i % S;
     GtBlk<T> acc;
-    if (Prog::kCompiled || tab.simple) {
+    if constexpr (Prog::kPoints) {
+      const GtAt at{ring, geo.stage_bytes, S, slot0, thr_off, geo.bx, geo.plane_elems, geo.zmin,
+                    xg0, yg0, zb + i};
+      Prog::template eval_points<T>(tab, at, acc);
+    } else if (Prog::kCompiled || tab.simple) {
       Prog::template eval<T>(tab, ring, geo.stage_bytes, S, slot0, thr_off, geo.bx, lane, acc);
     } else {
       for (int t = 0; t < tab.nterms; t++)

@@ -245,7 +245,8 @@ psb_status launch_map(MapImpl &m, int color, int64_t *launches) {
     for (int i = 0; i < m.nparams; i++) a.params[i] = m.params[i];
     a.error = r.d_error + 1;
     a.device = r.device;
-    st = cd->launch(&a, (void *)s);
+    st = compiled_staged_launch(m, *cd, views, color, s);
+    if (st == PSB_ERR_UNSUPPORTED) st = cd->launch(&a, (void *)s);
     if (launches) (*launches)++;
     for (int v = 0; v < cd->nviews; v++)
       if (cd->view_emits[v] && views[v]->layout == PSB_LAYOUT_PITCHED)
@@ -702,6 +703,20 @@ psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_i
     if (type_size(d.view_type[v]) == 0) return set_status(PSB_ERR_INVALID);
   for (int i = 0; i < d.nparams; i++)
     if (type_size(d.param_type[i]) == 0) return set_status(PSB_ERR_INVALID);
+  if (d.staged) {
+    if ((d.staged_type != PS_FLOAT && d.staged_type != PS_DOUBLE) || d.ndims != 3 ||
+        d.staged_emit < 0 || d.staged_emit >= d.ngrids)
+      return set_status(PSB_ERR_INVALID);
+    for (int i = 0; i < d.ngrids; i++) {
+      if (d.grid_type[i] != d.staged_type || d.grid_ndims[i] != 3)
+        return set_status(PSB_ERR_INVALID);
+      if (d.read_lo[i][0] > d.read_hi[i][0]) continue;  // not read
+      if (i == d.staged_emit) return set_status(PSB_ERR_INVALID);
+      for (int k = 0; k < 3; k++)
+        if (d.read_lo[i][k] < -2 || d.read_hi[i][k] > 2 || d.read_lo[i][k] > d.read_hi[i][k])
+          return set_status(PSB_ERR_INVALID);
+    }
+  }
   Runtime &r = rt();
   std::lock_guard<std::recursive_mutex> lk(r.mu);
   r.compiled.push_back(d);
