@@ -199,6 +199,14 @@ class StencilInfo:
         self.view_emits = [0] * len(self.view_type)
         self.view_reads_offset = [0] * len(self.view_type)
         self.axes = [None] * len(gparams)
+        # What the staged (TMA plane ring) form needs: every read at
+        # (x + a, y + b, z + c) with constants |a|, |b|, |c| <= 2, read offset
+        # ranges per grid, and a single emit (see _staged_eligible).
+        self.staged_ok = ndims == 3
+        self.staged_reads = {}      # grid slot -> [lo[3], hi[3]]
+        self.emit_count = 0
+        self.emit_slot = None
+        self.staged = False
 
     @property
     def grid_types(self):
@@ -371,6 +379,19 @@ class _Rewriter:
     def _point(self):
         return [c_ast.ID(n) for n in self.index_names] + [_int(0)] * (3 - len(self.index_names))
 
+    def _staged_read(self, slot, p, forms, periodic):
+        """Record a plain read for the staged form, or rule the form out."""
+        if self.info is None:
+            return
+        if periodic or p.struct is not None or p.nd != 3 or len(forms) != 3 or \
+                any(f is None or f[0] != k or abs(f[1]) > 2 for k, f in enumerate(forms)):
+            self.info.staged_ok = False
+            return
+        lo, hi = self.info.staged_reads.setdefault(slot, [[2, 2, 2], [-2, -2, -2]])
+        for k, f in enumerate(forms):
+            lo[k] = min(lo[k], f[1])
+            hi[k] = max(hi[k], f[1])
+
     def visit(self, node):
         ch = _member_chain(node)
         if ch is not None:
@@ -407,6 +428,8 @@ class _Rewriter:
         forms, at_point = self._indices(call, p, idx)
         self._record_axes(slot, forms)
         var, sub, first, n = self._component(call, p, fname, subs)
+        if self.info is not None:
+            self.info.staged_ok = False
         if not at_point:
             self._mark(slot, first, n, "read")
         helper = "__psb_getp" if call.name.name == "PSGridGetPeriodic" else "__psb_get"
@@ -433,6 +456,8 @@ class _Rewriter:
         subs = [self.visit(e) for e in ch[2]]
         value = self.visit(args[1])
         var, sub, first, n = self._component(node, p, ch[1], subs)
+        if self.info is not None:
+            self.info.staged_ok = False
         self._mark(slot, first, n, "emit")
         if n == 1:
             return c_ast.FuncCall(c_ast.ID("__psb_emit"), c_ast.ExprList(
@@ -454,6 +479,7 @@ class _Rewriter:
             if not at_point:
                 self._mark(slot, 0, p.nviews, "read")
             per = fn == "PSGridGetPeriodic"
+            self._staged_read(slot, p, forms, per)
             if p.struct is not None:   # the whole record
                 helper = "__psb_load%s_%s" % ("p" if per else "", p.struct.name)
                 return c_ast.FuncCall(c_ast.ID(helper), c_ast.ExprList(
@@ -469,6 +495,11 @@ class _Rewriter:
                 self.fail(node, "PSGridEmit into a %d-D grid from a %d-D stencil" %
                           (p.nd, len(self.index_names)))
             self._mark(slot, 0, p.nviews, "emit")
+            if self.info is not None:
+                self.info.emit_count += 1
+                self.info.emit_slot = slot
+                if p.struct is not None:
+                    self.info.staged_ok = False
             if p.struct is not None:
                 return c_ast.FuncCall(c_ast.ID("__psb_store_" + p.struct.name), c_ast.ExprList(
                     self._field_args(p) + self._point() + [args[1]]), node.coord)
@@ -507,6 +538,7 @@ _HELPERS = r"""
 #include <math.h>
 #include <stdint.h>
 #include "physis_b200.h"
+#include "k_generic_tma.cuh"
 
 template <typename T>
 struct __psb_grid {
@@ -584,6 +616,52 @@ __device__ __forceinline__ void __psb_emit_c(const __psb_grid<T> *f, int n, int 
 
 template <typename T>
 __device__ __forceinline__ int __psb_dim(const __psb_grid<T> &g, int d) {
+  return d == 0 ? g.n0 : (d == 1 ? g.n1 : g.n2);
+}
+
+// Staged form (a stencil function run over the library's TMA plane ring):
+// a grid read from the staged window at an offset from the point in row r,
+// column v of the thread's block, and the grid emitted into, whose value
+// goes to that point's result.
+template <typename T>
+struct __psb_sgrid {
+  const psb::GtTable *tab;
+  const psb::GtAt *at;
+  int slot, r, v, x, y, z;
+  int n0, n1, n2;
+};
+
+// A read outside the grid gives 0 and sets PSB_ERR_BOUNDS, as in the
+// thread-per-point form (the window holds 2 cells beyond the tile on every
+// side, so the staged address itself is always inside the ring).
+template <typename T>
+__device__ __forceinline__ T __psb_get(const __psb_sgrid<T> &g, int i, int j = 0, int k = 0) {
+  if ((unsigned)i >= (unsigned)g.n0 || (unsigned)j >= (unsigned)g.n1 ||
+      (unsigned)k >= (unsigned)g.n2) {
+    atomicExch(g.at->err + 1, (int)PSB_ERR_BOUNDS);
+    return T(0);
+  }
+  return psb::gt_staged<T>(*g.tab, *g.at, g.slot, g.r, g.v, i - g.x, j - g.y, k - g.z);
+}
+
+template <typename T>
+__device__ __forceinline__ int __psb_dim(const __psb_sgrid<T> &g, int d) {
+  return d == 0 ? g.n0 : (d == 1 ? g.n1 : g.n2);
+}
+
+template <typename T>
+struct __psb_ogrid {
+  T *out;
+  int n0, n1, n2;
+};
+
+template <typename T, typename V>
+__device__ __forceinline__ void __psb_emit(const __psb_ogrid<T> &g, int, int, int, V v) {
+  *g.out = (T)v;
+}
+
+template <typename T>
+__device__ __forceinline__ int __psb_dim(const __psb_ogrid<T> &g, int d) {
   return d == 0 ? g.n0 : (d == 1 ? g.n1 : g.n2);
 }
 """
@@ -727,6 +805,7 @@ def translate(source):
             for slot, p in enumerate(gparams):
                 if info.axes[slot] is None:
                     info.axes[slot] = list(range(p.nd))
+            info.staged = _staged_eligible(info, fd.body)
             infos[fname] = info
             sig = _signature(fname, params)
         else:
@@ -736,14 +815,146 @@ def translate(source):
             _Rewriter(fname, params, None, names).visit(fd.body)
             sig = "__device__ " + gen.visit(fd.decl).rstrip(";")
         decls.append(sig + ";")
-        bodies.append(sig + "\n" + gen.visit(fd.body))
+        body = gen.visit(fd.body)
+        bodies.append(sig + "\n" + body)
+        if fname in infos and infos[fname].staged:
+            bodies.append(_staged_function(infos[fname], params, body))
     if not infos:
         raise DSLError("no stencil function (`void f(const int x, ..., grids, ...)`) found")
     parts.append("\n".join(decls))
     parts.append("\n\n".join(bodies))
     for info in infos.values():
+        if info.staged:
+            parts.append(_staged_entry(info))
         parts.append(_entry(info))
     return "\n\n".join(parts) + "\n", infos
+
+
+def _staged_eligible(info, body):
+    """Whether the function has a staged form: 3-D, one element type (float
+    or double) over primitive 3-D grids, every read at constant offsets
+    within +-2 of the point, one emit, as a statement of the body's top
+    level with no return before it, into a grid it does not read."""
+    if not info.staged_ok or info.emit_count != 1 or info.emit_slot is None:
+        return False
+    if any(p.struct is not None or p.nd != 3 for p in info.gparams):
+        return False
+    types = {p.ctype for p in info.gparams}
+    if len(types) != 1 or types.pop() not in (ps.PS_FLOAT, ps.PS_DOUBLE):
+        return False
+    if not info.staged_reads or info.emit_slot in info.staged_reads or len(info.scalars) > 32:
+        return False
+    items = body.block_items or []
+    at = [i for i, it in enumerate(items) if isinstance(it, c_ast.FuncCall) and
+          isinstance(it.name, c_ast.ID) and it.name.name == "__psb_emit"]
+    if len(at) != 1:
+        return False
+
+    class _Returns(c_ast.NodeVisitor):
+        found = False
+
+        def visit_Return(self, node):
+            self.found = True
+
+    r = _Returns()
+    for it in items[:at[0]]:
+        r.visit(it)
+    return not r.found
+
+
+def _staged_function(info, params, body):
+    """The function again, its grids as template parameters: staged handles
+    (reads from the plane ring, the emit into the point's result)."""
+    tpl, args, g = [], [], 0
+    for p in params:
+        if p.kind == "index":
+            args.append("const int %s" % p.name)
+        elif p.kind == "grid":
+            tpl.append("class __G%d" % g)
+            args.append("const __G%d &%s" % (g, p.name))
+            g += 1
+        elif p.kind == "scalar":
+            args.append("%s %s" % (_CTYPE[p.ctype], p.name))
+    return "template <%s>\n__device__ __forceinline__ void %s__staged(%s)\n%s" % (
+        ", ".join(tpl), info.name, ", ".join(args), body)
+
+
+def _staged_entry(info):
+    """The point-wise program, kernel and launcher of the staged form."""
+    n = info.name
+    t = _CTYPE[info.gparams[0].ctype]
+    handles, args = [], []
+    for slot in range(len(info.gparams)):
+        dims = ", ".join("tab.slot_dims[%d][%d]" % (slot, k) for k in range(3))
+        if slot == info.emit_slot:
+            handles.append("const __psb_ogrid<T> g%d{&acc.v[r][v], %s};" % (slot, dims))
+        else:
+            handles.append("const __psb_sgrid<T> g%d{&tab, &at, %d, r, v, x, y, at.z, %s};" %
+                           (slot, slot, dims))
+        args.append("g%d" % slot)
+    for k, (_, st) in enumerate(info.scalars):
+        args.append("(%s)tab.coef[%d]" % (_CTYPE[st], k))
+    return """
+struct __psb_prog_{n} {{
+  static constexpr bool kCompiled = true;
+  static constexpr bool kPoints = true;
+  template <typename T>
+  static __device__ __forceinline__ void eval(const psb::GtTable &, const unsigned char *, int,
+                                              int, int, int, int, int, psb::GtBlk<T> &) {{}}
+  template <typename T>
+  static __device__ __forceinline__ void eval_points(const psb::GtTable &tab,
+                                                     const psb::GtAt &at, psb::GtBlk<T> &acc) {{
+#pragma unroll
+    for (int r = 0; r < psb::kGtVY; r++) {{
+      const int y = at.y + r;
+      if (y < at.lo1 || y >= at.hi1) continue;
+#pragma unroll
+      for (int v = 0; v < 16 / (int)sizeof(T); v++) {{
+        const int x = at.x + v;
+        if (x < at.lo0 || x >= at.hi0) continue;
+        {handles}
+        {n}__staged(x, y, at.z, {args});
+      }}
+    }}
+  }}
+}};
+
+extern "C" __global__ void __launch_bounds__(psb::kGtThreads, 2) __psb_staged_kernel_{n}(
+    const __grid_constant__ psb::GtMaps maps, const __grid_constant__ psb::GtTable tab,
+    psb::GridView out, psb::Dom3 d, const __grid_constant__ psb::GtGeom geo, int *err) {{
+  psb::gt_body<{t}, __psb_prog_{n}>(maps, tab, out, d, geo, err);
+}}
+
+extern "C" psb_status psb_dsl_staged_{n}(const void *maps, const void *table, const void *out,
+                                         const void *dom, const void *geo, int *err,
+                                         unsigned blocks, unsigned smem, void *stream) {{
+  static unsigned configured = 0;
+  if (smem > configured) {{
+    if (cudaFuncSetAttribute(__psb_staged_kernel_{n}, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaFuncSetAttribute(__psb_staged_kernel_{n},
+                             cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+      return PSB_ERR_CUDA;
+    configured = smem;
+  }}
+  __psb_staged_kernel_{n}<<<blocks, psb::kGtThreads, smem, (cudaStream_t)stream>>>(
+      *(const psb::GtMaps *)maps, *(const psb::GtTable *)table, *(const psb::GridView *)out,
+      *(const psb::Dom3 *)dom, *(const psb::GtGeom *)geo, err);
+  return cudaGetLastError() == cudaSuccess ? PSB_OK : PSB_ERR_CUDA;
+}}
+""".format(n=n, t=t, handles="\n        ".join(handles), args=", ".join(args))
+
+
+def _read_ranges(info):
+    """Flat lo and hi read offsets per grid parameter for the descriptor
+    (lo 1 > hi 0 on every axis: not read by the staged form)."""
+    lo, hi = [], []
+    for slot in range(len(info.gparams)):
+        r = info.staged_reads.get(slot) if info.staged else None
+        lo += r[0] if r else [1, 1, 1]
+        hi += r[1] if r else [0, 0, 0]
+    return lo, hi
 
 
 def _entry(info):
@@ -817,8 +1028,21 @@ extern "C" void psb_dsl_describe_{n}(psb_compiled_stencil *d) {{
   d->nparams = {np};
   for (int i = 0; i < {np}; i++) d->param_type[i] = pt[i];
   d->launch = psb_dsl_launch_{n};
+  const int rlo[] = {{{rlo}}}, rhi[] = {{{rhi}}};
+  for (int i = 0; i < PSB_MAX_GRIDS; i++)
+    for (int k = 0; k < 3; k++) {{
+      d->read_lo[i][k] = i < {ng} ? rlo[3 * i + k] : 1;
+      d->read_hi[i][k] = i < {ng} ? rhi[3 * i + k] : 0;
+    }}
+  d->staged_type = {stype};
+  d->staged_emit = {semit};
+  d->staged = {sfn};
 }}
-""".format(n=n, binds="\n".join(binds), args=", ".join(args), gt=arr(info.grid_types),
+""".format(rlo=arr(_read_ranges(info)[0]), rhi=arr(_read_ranges(info)[1]),
+           stype=info.gparams[0].ctype if info.staged else 0,
+           semit=info.emit_slot if info.staged else 0,
+           sfn=("psb_dsl_staged_%s" % n) if info.staged else "nullptr",
+           n=n, binds="\n".join(binds), args=", ".join(args), gt=arr(info.grid_types),
            gn=arr(nd for _, _, nd in info.grids), gc=arr(comps), vt=arr(info.view_type),
            ve=arr(info.view_emits), vr=arr(info.view_reads_offset),
            pt=arr(t for _, t in info.scalars), nd=info.ndims, ng=len(info.grids),
@@ -826,7 +1050,10 @@ extern "C" void psb_dsl_describe_{n}(psb_compiled_stencil *d) {{
 
 
 _NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-               "-fmad=false", "-Xcompiler", "-fPIC", "-shared"]
+               "-fmad=false", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC", "-shared"]
+CSRC = os.path.join(HERE, "csrc")
+# Device headers the staged form compiles against (part of the cache key).
+_STAGED_HEADERS = ["k_generic_tma.cuh", "device.cuh", "views.h", "internal.h"]
 
 
 def build_library(cuda_source, cache_dir=None):
@@ -838,6 +1065,9 @@ def build_library(cuda_source, cache_dir=None):
     h = hashlib.sha256(cuda_source.encode())
     with open(os.path.join(INCLUDE, "physis_b200.h"), "rb") as f:
         h.update(f.read())
+    for name in _STAGED_HEADERS:
+        with open(os.path.join(CSRC, name), "rb") as f:
+            h.update(f.read())
     h.update(" ".join(_NVCC_FLAGS).encode())
     key = h.hexdigest()[:20]
     so = os.path.join(cache_dir, "libpsb_dsl_%s.so" % key)
@@ -850,7 +1080,7 @@ def build_library(cuda_source, cache_dir=None):
     with open(cu, "w") as f:
         f.write(cuda_source)
     tmp = so + ".tmp" + tag
-    cmd = [NVCC] + _NVCC_FLAGS + ["-I" + INCLUDE, cu, "-o", tmp]
+    cmd = [NVCC] + _NVCC_FLAGS + ["-I" + INCLUDE, "-I" + CSRC, cu, "-o", tmp]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise DSLError("nvcc failed on the generated kernel:\n" + r.stdout + r.stderr)

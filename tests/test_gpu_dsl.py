@@ -28,14 +28,27 @@ def kernels(tmp_path_factory):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("form", ["staged", "own"])
 @pytest.mark.parametrize("layout", sorted(U.LAYOUTS))
 @pytest.mark.parametrize("name", sorted(DSL))
-def test_compiled_stencil_matches_golden(name, layout, kernels):
+def test_compiled_stencil_matches_golden(name, layout, form, kernels):
+    """Both forms of a compiled stencil print the reference's answer: the
+    staged form (the function over the TMA plane ring) where the front end
+    emitted one, and the stencil's own thread-per-point launch (forced with
+    psb_set_impl(PSB_IMPL_GENERIC))."""
     src, fn, scalars = DSL[name]
     case = CASES[name]
-    out = U.run_case_gpu(case, U.LAYOUTS[layout], kernel_id=kernels[fn].kernel_id, params=scalars)
-    ps.sync()
+    if form == "own":
+        ps.set_impl(ps.IMPL_GENERIC)
+    try:
+        out = U.run_case_gpu(case, U.LAYOUTS[layout], kernel_id=kernels[fn].kernel_id,
+                             params=scalars)
+        ps.sync()
+        staged = ps.compiled_last_staged()
+    finally:
+        ps.set_impl(ps.IMPL_AUTO)
     assert C.dump_text(out, case["fmt"]) == C.golden_text(name)
+    assert staged == (form == "staged" and kernels[fn].info.staged), (name, layout, form)
 
 
 USER = D.user_cases()

@@ -37,6 +37,7 @@ PROGRAM = r"""
 namespace psb {
 struct GtCompiledProg {
   static constexpr bool kCompiled = true;
+  static constexpr bool kPoints = false;
   template <typename T>
   static __device__ __forceinline__ void eval(const GtTable &tab, const unsigned char *ring,
       int sbytes, int S, int slot0, int thr_off, int bx, int lane, GtBlk<T> &acc) {
@@ -68,6 +69,7 @@ GENERAL = r"""
 namespace psb {
 struct GtCompiledProg {
   static constexpr bool kCompiled = true;
+  static constexpr bool kPoints = false;
   template <typename T>
   static __device__ __forceinline__ void eval(const GtTable &tab, const unsigned char *ring,
       int sbytes, int S, int slot0, int thr_off, int bx, int lane, GtBlk<T> &acc) {
