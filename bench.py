@@ -46,6 +46,9 @@ WORKLOADS = {
     # the C2 stencil written as a stencil function in the reference's DSL and
     # compiled by the translator-free front end (physis_b200/dsl.py)
     "dsl7": ("dsl7", np.float32, (512, 512, 512), 100, 8),
+    # the g27 stencil written as a DSL stencil function (interior domain: the
+    # front end's staged form runs it)
+    "dsl27": ("dsl27", np.float32, (512, 512, 512), 100, 8),
     # batched: 256 members, see c4_members(); dims/steps are per member
     "c4": ("batch", np.float32, (0, 0, 0), 0, 0),
     # served: a Poisson trace of solve requests, see c5_trace()
@@ -71,12 +74,18 @@ def describe(wl):
         return ("generic (user) stencil: 27-point box average sum_{d in {-1,0,1}^3} (1/27)*u(p+d) "
                 "as a psb_generic_stencil term table, %dx%dx%d fp32 interior [1,n-1)^3, %d time "
                 "steps per solve (double-buffered PSStencilRun)" % (dims + (steps,)))
+    if k == "dsl27":
+        return ("27-point box average %dx%dx%d fp32 written as a DSL stencil function "
+                "(physis_b200.workloads.BOX27_DSL: the g27 table's terms, order and "
+                "coefficient) and compiled by the translator-free front end, interior "
+                "[1,n-1)^3, %d time steps per solve (double-buffered PSStencilRun)"
+                % (dims + (steps,)))
     if k == "dsl7":
         return ("7-point diffusion %dx%dx%d fp32 written as a DSL stencil function "
                 "(physis_b200.workloads.DIFFUSION7_DSL) and compiled by the translator-free "
-                "front end into the reference's generated-kernel shape (one thread per (x, y), "
-                "z loop), %d time steps per solve (double-buffered PSStencilRun), clamped "
-                "faces" % (dims + (steps,)))
+                "front end (the kernel form that ran is in config.generic_kernel), %d time "
+                "steps per solve (double-buffered PSStencilRun), clamped faces"
+                % (dims + (steps,)))
     return ("7-point diffusion %dx%dx%d %s, %d time steps per solve (double-buffered "
             "PSStencilRun), clamped faces" % (dims + ("fp32" if dt == np.float32 else "fp64", steps)))
 
@@ -405,20 +414,20 @@ def generic27_stencil(ps, accum=None):
     return box27_stencil(accum if accum is not None else ps.PS_FLOAT)
 
 
-def numerics_generic27(ps, dt, n=96, steps=10):
+def numerics_generic27(ps, dt, n=96, steps=10, kernel_id=None, params=()):
     """The generic 27-point path at n^3 for `steps` steps against the oracle
     port (bit-exact check) and the FP64 oracle (the same term table
     evaluated in double by the port)."""
     from oracle import oracle
     from physis_b200.workloads import box27_stencil, box27_struct
     f = c2_field((n, n, n), dt)
-    st = box27_stencil(ps.PS_FLOAT)
+    kid = box27_stencil(ps.PS_FLOAT).kernel_id if kernel_id is None else kernel_id
     g = [ps.grid_new(ps.PS_FLOAT, (n, n, n)) for _ in range(2)]
     for x in g:
         ps.PSGridCopyin(x, f)
     d = ps.PSDomain3DNew(1, n - 1, 1, n - 1, 1, n - 1)
-    a = ps.PSStencilMap(st.kernel_id, d, g[0], g[1])
-    b = ps.PSStencilMap(st.kernel_id, d, g[1], g[0])
+    a = ps.PSStencilMap(kid, d, g[0], g[1], *params)
+    b = ps.PSStencilMap(kid, d, g[1], g[0], *params)
     ps.PSStencilRun(a, b, steps // 2)
     got = ps.PSGridCopyout(g[0])
     exact = None
@@ -464,7 +473,7 @@ def run_ours(args):
     ptype = ps.PS_FLOAT if dt == np.float32 else ps.PS_DOUBLE
     kernel = ps.HIMENO19 if kname == "himeno" else ps.DIFFUSION7
     tune = None
-    if kname not in ("generic27", "dsl7"):
+    if kname not in ("generic27", "dsl7", "dsl27"):
         tune = ps.autotune(kernel, ptype, dims) if args.tune else ps.tune_get(kernel, ptype, dims)
     if args.plain:
         # the thread-per-point shape of the reference's generated kernels
@@ -492,15 +501,20 @@ def run_ours(args):
             ps.himeno_residual_enable(m2, tsteps)
         pts_per_step = (nx - 2) * (ny - 2) * (nz - 2) * tsteps
         g_io = grids[0]
-    elif kname == "generic27":
+    elif kname in ("generic27", "dsl27"):
         host = c2_field(dims, dt)
         grids = [ps.grid_new(ptype, dims), ps.grid_new(ptype, dims)]
         ps.PSGridCopyin(grids[0], host)
         ps.PSGridCopyin(grids[1], host)  # the boundary cells stay as they are
-        g27 = generic27_stencil(ps)
+        kid, kparams = generic27_stencil(ps).kernel_id, ()
+        if kname == "dsl27":
+            from physis_b200 import dsl
+            from physis_b200.workloads import BOX27_DSL
+            kid = dsl.compile_stencils(BOX27_DSL)["box27"].kernel_id
+            kparams = (float(np.float32(1.0 / 27.0)),)
         dom = ps.PSDomain3DNew(1, nx - 1, 1, ny - 1, 1, nz - 1)
-        m1 = ps.PSStencilMap(g27.kernel_id, dom, grids[0], grids[1])
-        m2 = ps.PSStencilMap(g27.kernel_id, dom, grids[1], grids[0])
+        m1 = ps.PSStencilMap(kid, dom, grids[0], grids[1], *kparams)
+        m2 = ps.PSStencilMap(kid, dom, grids[1], grids[0], *kparams)
         pts_per_step = (nx - 2) * (ny - 2) * (nz - 2) * tsteps
         g_io = grids[0]
     else:
@@ -559,6 +573,10 @@ def run_ours(args):
                       "what": "the same solves with every product and sum rounded in the "
                               "reference's order (bit-identical to the reference CPU target)"}
     gimpl = None
+    if kname in ("dsl7", "dsl27"):
+        gimpl = ("staged form: the function body over the TMA plane ring (k_generic_tma's "
+                 "kernel body)" if ps.compiled_last_staged() else
+                 "thread per (x, y) point with a z loop (the reference's generated-kernel shape)")
     if kname == "generic27":
         import ctypes
         v = ctypes.c_int()
@@ -582,7 +600,8 @@ def run_ours(args):
     achieved = bpl * pts_per_step * args.steps / dev_s / 1e9
     two_sweeps = kname == "himeno" and tune is not None and tune.get("t_depth") == 2
     kname_traffic = ("k_himeno_tb2" if two_sweeps else "k_himeno_tma") if kname == "himeno" else \
-        "k_generic_tma_f32" if kname == "generic27" else "k_dsl_diffusion7_f32" if kname == "dsl7" else (
+        "k_generic_tma_f32" if kname == "generic27" else "k_dsl_diffusion7_f32" if kname == "dsl7" \
+        else "k_dsl_box27_f32" if kname == "dsl27" else (
         "k_diff7_tma_f32" if dt == np.float32 else "k_diff7_tma_f64") + ("_fma" if fma else "")
     if args.plain:
         kname_traffic = kname_traffic.replace("tma", "plain")
@@ -618,13 +637,16 @@ def run_ours(args):
             numerics = numerics_himeno(ps, dims, tsteps, grids, m1, m2, p, coef)
         elif kname == "generic27":
             numerics = numerics_generic27(ps, dt)
+        elif kname == "dsl27":
+            numerics = numerics_generic27(ps, dt, kernel_id=kid, params=kparams)
         else:
             numerics = numerics_diffusion(ps, dt, dims, tsteps, grids, m1, m2, host, mass0, mass1,
                                           (args.warmup + args.steps) * tsteps,
                                           kernel_id=kid if kname == "dsl7" else None)
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_sample(wl, host if kname in ("diffusion7", "generic27", "dsl7")
+        cpu = cpu_baseline_sample(wl if kname != "dsl27" else "g27",
+                                  host if kname in ("diffusion7", "generic27", "dsl7", "dsl27")
                                   else None)
 
     line = {
@@ -645,8 +667,9 @@ def run_ours(args):
             "step": "one solve of %d time steps (PSStencilRun of two maps x %d)" % (tsteps, tsteps // 2),
             "inputs_vs_l2": "%.0f MB per grid > 126 MB L2; no flush needed" % (host.nbytes / 1e6),
             "parallelism": "replicas (one independent solve per GPU, no exchange)",
-            "impl": ("DSL stencil function compiled by physis_b200.dsl (reference generated-kernel "
-                     "shape)" if kname == "dsl7" else "plain" if args.plain else "autotuned"),
+            "impl": ("DSL stencil function compiled by physis_b200.dsl" if kname in ("dsl7", "dsl27")
+                     else
+                     "plain" if args.plain else "autotuned"),
             "fp_mode": (("fma: the reference's term order with fused multiply-adds (one "
                          "rounding per term; every point within 4 ulp of the exact step per "
                          "step; errors against the FP64 oracle in `numerics`)")

@@ -536,8 +536,8 @@ typedef struct {
    * +-2 of the point, between read_lo and read_hi per axis (read_lo > read_hi
    * on axis 0: the grid is not read). The library runs it when the map fits
    * (TMA-ready layouts, no red-black colour, at most four grids read, the
-   * emitted grid not bound to a read parameter) and otherwise calls
-   * `launch`; reads outside their grid still give 0 and PSB_ERR_BOUNDS. */
+   * emitted grid not bound to a read parameter, and every read range inside
+   * its grid over the whole domain) and otherwise calls `launch`. */
   int staged_type;
   int staged_emit;
   int read_lo[PSB_MAX_GRIDS][3];

@@ -361,9 +361,11 @@ static psb_status staged_run(MapImpl &m, const psb_compiled_stencil &cd, const G
 }
 
 // A compiled stencil's staged form: the map must read only grids of the
-// stencil's type that TMA can stage (at most four distinct ones) and never
-// the grid it emits into. Reads keep the thread-per-point form's bounds
-// check (a read outside its grid gives 0 and sets PSB_ERR_BOUNDS).
+// stencil's type that TMA can stage (at most four distinct ones), never the
+// grid it emits into, and stay inside every grid it reads over the whole
+// domain: the staged reads have no bounds check (a function whose reads
+// may leave the grid, even under a condition, keeps its own form, which
+// checks every read).
 psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, GridImpl **views,
                                   int color, cudaStream_t s) {
   g_last_compiled_staged = 0;
@@ -390,6 +392,9 @@ psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, Gr
     if (cd.read_lo[i][0] > cd.read_hi[i][0]) continue;  // not read
     if (g == og || g->type != cd.staged_type || g->pub.num_dims != 3 || !tma_eligible(g))
       return PSB_ERR_UNSUPPORTED;
+    for (int k = 0; k < 3; k++)
+      if (d.lo[k] + cd.read_lo[i][k] < 0 || d.hi[k] - 1 + cd.read_hi[i][k] > g->pub.dim[k] - 1)
+        return PSB_ERR_UNSUPPORTED;
     int gi = -1;
     for (int j = 0; j < p.ngrids; j++)
       if (views[p.slots[j]] == g) gi = j;

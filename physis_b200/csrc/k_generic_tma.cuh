@@ -288,7 +288,6 @@ struct GtAt {
   int sbytes, S, slot0, thr_off, bx, plane_elems, zmin;
   int x, y, z;
   int lo0, hi0, lo1, hi1;  // the domain in x and y (z is always inside)
-  int *err;                // error words: [1] takes PSB_ERR_BOUNDS
 };
 
 // The staged value of grid slot `slot` at (x + dx, y + dy, z + dz) from the
@@ -420,7 +419,7 @@ __device__ __forceinline__ void gt_body(const GtMaps &maps, const GtTable &tab,
     GtBlk<T> acc;
     if constexpr (Prog::kPoints) {
       const GtAt at{ring, geo.stage_bytes, S, slot0, thr_off, geo.bx, geo.plane_elems, geo.zmin,
-                    xg0, yg0, zb + i, d.lo[0], d.hi[0], d.lo[1], d.hi[1], err};
+                    xg0, yg0, zb + i, d.lo[0], d.hi[0], d.lo[1], d.hi[1]};
       Prog::template eval_points<T>(tab, at, acc);
     } else if (Prog::kCompiled || tab.simple) {
       Prog::template eval<T>(tab, ring, geo.stage_bytes, S, slot0, thr_off, geo.bx, lane, acc);

@@ -204,6 +204,7 @@ class StencilInfo:
         # ranges per grid, and a single emit (see _staged_eligible).
         self.staged_ok = ndims == 3
         self.staged_reads = {}      # grid slot -> [lo[3], hi[3]]
+        self.staged_rows = {}       # (slot, dy, dz) -> [dx min, dx max], in first-read order
         self.emit_count = 0
         self.emit_slot = None
         self.staged = False
@@ -391,6 +392,9 @@ class _Rewriter:
         for k, f in enumerate(forms):
             lo[k] = min(lo[k], f[1])
             hi[k] = max(hi[k], f[1])
+        row = self.info.staged_rows.setdefault((slot, forms[1][1], forms[2][1]), [2, -2])
+        row[0] = min(row[0], forms[0][1])
+        row[1] = max(row[1], forms[0][1])
 
     def visit(self, node):
         ch = _member_chain(node)
@@ -623,29 +627,25 @@ __device__ __forceinline__ int __psb_dim(const __psb_grid<T> &g, int d) {
 // a grid read from the staged window at an offset from the point in row r,
 // column v of the thread's block, and the grid emitted into, whose value
 // goes to that point's result.
-template <typename T>
-struct __psb_sgrid {
-  const psb::GtTable *tab;
-  const psb::GtAt *at;
-  int slot, r, v, x, y, z;
+// A read grid of the staged form: the rows the function reads around the
+// current row of the thread's block, in registers (L::id maps a row's grid,
+// dy and dz to its index), and the point's column v in that row. The library
+// runs the staged form only when every read the function can make over the
+// map's domain lies inside its grid, so reads need no bounds check here.
+template <typename T, class L>
+struct __psb_rgrid {
+  const psb::GtRow<T> *rows;
+  int slot, v, x, y, z;
   int n0, n1, n2;
 };
 
-// A read outside the grid gives 0 and sets PSB_ERR_BOUNDS, as in the
-// thread-per-point form (the window holds 2 cells beyond the tile on every
-// side, so the staged address itself is always inside the ring).
-template <typename T>
-__device__ __forceinline__ T __psb_get(const __psb_sgrid<T> &g, int i, int j = 0, int k = 0) {
-  if ((unsigned)i >= (unsigned)g.n0 || (unsigned)j >= (unsigned)g.n1 ||
-      (unsigned)k >= (unsigned)g.n2) {
-    atomicExch(g.at->err + 1, (int)PSB_ERR_BOUNDS);
-    return T(0);
-  }
-  return psb::gt_staged<T>(*g.tab, *g.at, g.slot, g.r, g.v, i - g.x, j - g.y, k - g.z);
+template <typename T, class L>
+__device__ __forceinline__ T __psb_get(const __psb_rgrid<T, L> &g, int i, int j = 0, int k = 0) {
+  return g.rows[L::id(g.slot, j - g.y, k - g.z)].e[2 + (i - g.x) + g.v];
 }
 
-template <typename T>
-__device__ __forceinline__ int __psb_dim(const __psb_sgrid<T> &g, int d) {
+template <typename T, class L>
+__device__ __forceinline__ int __psb_dim(const __psb_rgrid<T, L> &g, int d) {
   return d == 0 ? g.n0 : (d == 1 ? g.n1 : g.n2);
 }
 
@@ -880,21 +880,44 @@ def _staged_function(info, params, body):
 
 
 def _staged_entry(info):
-    """The point-wise program, kernel and launcher of the staged form."""
+    """The point-wise program, kernel and launcher of the staged form.
+
+    For each row of the thread's block the rows the function reads -- one
+    per (grid, dy, dz) -- are loaded into registers as the generic packed
+    form does (a 16-byte load per thread, x neighbours from the adjacent
+    lanes); every read of the function then resolves, at compile time, to a
+    register of one of those rows."""
     n = info.name
     t = _CTYPE[info.gparams[0].ctype]
+    rows = list(info.staged_rows.items())
+    ids = " : ".join("(slot == %d && dy == %d && dz == %d) ? %d" % (sl, dy, dz, k)
+                     for k, ((sl, dy, dz), _) in enumerate(rows)) + " : 0"
+    loads = []
+    for k, ((sl, dy, dz), (dxlo, dxhi)) in enumerate(rows):
+        loads.append(
+            "{ int sl = at.slot0 + %d - at.zmin; if (sl >= at.S) sl -= at.S;\n"
+            "          psb::gt_row_load(reinterpret_cast<const T *>(at.ring + (size_t)sl * at.sbytes) + "
+            "tab.slot_grid[%d] * at.plane_elems + at.thr_off + (r + %d) * at.bx, lane, %s, %s, "
+            "rows[%d]); }" % (dz, sl, dy, "true" if dxhi > 0 else "false",
+                              "true" if dxlo < 0 else "false", k))
     handles, args = [], []
     for slot in range(len(info.gparams)):
         dims = ", ".join("tab.slot_dims[%d][%d]" % (slot, k) for k in range(3))
         if slot == info.emit_slot:
             handles.append("const __psb_ogrid<T> g%d{&acc.v[r][v], %s};" % (slot, dims))
         else:
-            handles.append("const __psb_sgrid<T> g%d{&tab, &at, %d, r, v, x, y, at.z, %s};" %
-                           (slot, slot, dims))
+            handles.append("const __psb_rgrid<T, __psb_rows_%s> g%d{rows, %d, v, x, y, at.z, %s};"
+                           % (n, slot, slot, dims))
         args.append("g%d" % slot)
     for k, (_, st) in enumerate(info.scalars):
         args.append("(%s)tab.coef[%d]" % (_CTYPE[st], k))
     return """
+struct __psb_rows_{n} {{
+  static __device__ __forceinline__ constexpr int id(int slot, int dy, int dz) {{
+    return {ids};
+  }}
+}};
+
 struct __psb_prog_{n} {{
   static constexpr bool kCompiled = true;
   static constexpr bool kPoints = true;
@@ -904,8 +927,11 @@ struct __psb_prog_{n} {{
   template <typename T>
   static __device__ __forceinline__ void eval_points(const psb::GtTable &tab,
                                                      const psb::GtAt &at, psb::GtBlk<T> &acc) {{
+    const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int r = 0; r < psb::kGtVY; r++) {{
+      psb::GtRow<T> rows[{nrows}];  // every lane loads: the rows share values by shuffles
+      {loads}
       const int y = at.y + r;
       if (y < at.lo1 || y >= at.hi1) continue;
 #pragma unroll
@@ -943,7 +969,8 @@ extern "C" psb_status psb_dsl_staged_{n}(const void *maps, const void *table, co
       *(const psb::Dom3 *)dom, *(const psb::GtGeom *)geo, err);
   return cudaGetLastError() == cudaSuccess ? PSB_OK : PSB_ERR_CUDA;
 }}
-""".format(n=n, t=t, handles="\n        ".join(handles), args=", ".join(args))
+""".format(n=n, t=t, ids=ids, nrows=len(rows), loads="\n      ".join(loads),
+           handles="\n        ".join(handles), args=", ".join(args))
 
 
 def _read_ranges(info):

@@ -146,3 +146,19 @@ void diffusion7(const int x, const int y, const int z, PSGrid3DFloat u, PSGrid3D
   PSGridEmit(v, cc * c + cw * w + ce * e + cs * s + cn * n + cb * b + ct * t);
 }
 """
+
+
+def _box27_dsl():
+    def idx(v, d):
+        return v if d == 0 else "%s %s %d" % (v, "+" if d > 0 else "-", abs(d))
+    terms = " + ".join("c * PSGridGet(u, %s, %s, %s)" % (idx("x", dx), idx("y", dy), idx("z", dz))
+                       for dx, dy, dz in box27_offsets())
+    return ("void box27(const int x, const int y, const int z, PSGrid3DFloat u, PSGrid3DFloat v,\n"
+            "           float c) {\n  PSGridEmit(v, %s);\n}\n" % terms)
+
+
+# The 27-point box average as a DSL stencil function: the same terms, order
+# and coefficient (passed as the scalar c = float(1/27)) as box27_terms, so
+# over the interior [1, n-1)^3 it reads inside the grid everywhere and the
+# front end's staged form runs it.
+BOX27_DSL = _box27_dsl()

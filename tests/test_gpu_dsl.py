@@ -48,7 +48,29 @@ def test_compiled_stencil_matches_golden(name, layout, form, kernels):
     finally:
         ps.set_impl(ps.IMPL_AUTO)
     assert C.dump_text(out, case["fmt"]) == C.golden_text(name)
-    assert staged == (form == "staged" and kernels[fn].info.staged), (name, layout, form)
+    assert staged == (form == "staged" and _staged_fits(kernels[fn].info, case)), \
+        (name, layout, form)
+
+
+def _staged_fits(info, case):
+    """Whether the library may run the last map of the case in its staged
+    form: the function has one, the map is not red-black, does not read the
+    grid it emits into, and every read range stays inside its grid over the
+    domain."""
+    if not info.staged:
+        return False
+    slots, color = case["run"][-1]
+    if color == 2:
+        return False
+    lo, hi = case["dom"]
+    out = slots[info.emit_slot]
+    for param, (rlo, rhi) in info.staged_reads.items():
+        if slots[param] == out:
+            return False
+        dims = case["grids"][slots[param]][1]
+        if any(lo[k] + rlo[k] < 0 or hi[k] - 1 + rhi[k] > dims[k] - 1 for k in range(3)):
+            return False
+    return True
 
 
 USER = D.user_cases()
