@@ -574,8 +574,10 @@ def run_ours(args):
                               "reference's order (bit-identical to the reference CPU target)"}
     gimpl = None
     if kname in ("dsl7", "dsl27"):
+        form = ps.compiled_last_staged()
         gimpl = ("staged form: the function body over the TMA plane ring (k_generic_tma's "
-                 "kernel body)" if ps.compiled_last_staged() else
+                 "kernel body)%s" % (", reads that leave the point checked against the grid"
+                                      if form == 2 else "") if form else
                  "thread per (x, y) point with a z loop (the reference's generated-kernel shape)")
     if kname == "generic27":
         import ctypes

@@ -537,17 +537,24 @@ typedef struct {
    * on axis 0: the grid is not read). The library runs it when the map fits
    * (TMA-ready layouts, no red-black colour, at most four grids read, the
    * emitted grid not bound to a read parameter, and every read range inside
-   * its grid over the whole domain) and otherwise calls `launch`. */
+   * its grid over the whole domain) and otherwise calls `launch`.
+   * staged_checked (optional, with staged): the same staged form with every
+   * read that leaves the point checked against its grid (a read outside
+   * reads 0 and sets PSB_ERR_BOUNDS, as `launch` does). The library runs it
+   * when a read range may leave its grid over the domain (reads under face
+   * tests, e.g. `x == 0 ? c : PSGridGet(g, x-1, y, z)`) and the domain lies
+   * inside every grid read. */
   int staged_type;
   int staged_emit;
   int read_lo[PSB_MAX_GRIDS][3];
   int read_hi[PSB_MAX_GRIDS][3];
   psb_compiled_staged staged;
+  psb_compiled_staged staged_checked;
 } psb_compiled_stencil;
 
 psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_id);
 /* Whether the last application of a compiled stencil ran its staged form
- * (1) or its own thread-per-point launch (0). psb_set_impl(PSB_IMPL_PLAIN or
+ * (1), the checked staged form (2) or its own thread-per-point launch (0). psb_set_impl(PSB_IMPL_PLAIN or
  * PSB_IMPL_GENERIC) keeps compiled stencils on their own launch. */
 psb_status psb_compiled_last_staged(int *staged);
 

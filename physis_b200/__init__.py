@@ -122,7 +122,8 @@ class CompiledStencilStruct(ctypes.Structure):
                 ("param_type", ctypes.c_int * PSB_MAX_PARAMS), ("launch", ctypes.c_void_p),
                 ("staged_type", ctypes.c_int), ("staged_emit", ctypes.c_int),
                 ("read_lo", (ctypes.c_int * 3) * PSB_MAX_GRIDS),
-                ("read_hi", (ctypes.c_int * 3) * PSB_MAX_GRIDS), ("staged", ctypes.c_void_p)]
+                ("read_hi", (ctypes.c_int * 3) * PSB_MAX_GRIDS), ("staged", ctypes.c_void_p),
+                ("staged_checked", ctypes.c_void_p)]
 
 
 class TuneConfig(ctypes.Structure):
@@ -611,11 +612,12 @@ def set_generic_compile(on):
 
 
 def compiled_last_staged():
-    """Whether the last application of a compiled (DSL) stencil ran its staged
-    (TMA plane ring) form."""
+    """Which form the last application of a compiled (DSL) stencil ran: 0 its
+    own thread-per-point launch, 1 the staged (TMA plane ring) form, 2 the
+    staged form with its reads checked against their grids."""
     v = ctypes.c_int()
     check(lib.psb_compiled_last_staged(ctypes.byref(v)), "psb_compiled_last_staged")
-    return bool(v.value)
+    return v.value
 
 
 def generic_last_compiled():

@@ -342,8 +342,8 @@ void generic_note_impl(int impl) { g_last_generic_impl = impl; }
 static int g_last_compiled_staged = 0;
 
 template <typename T>
-static psb_status staged_run(MapImpl &m, const psb_compiled_stencil &cd, const GtPlan &p,
-                             GridImpl *og, const Dom3 &d, GtTable &tab, cudaStream_t s) {
+static psb_status staged_run(MapImpl &m, psb_compiled_staged fn, const GtPlan &p, GridImpl *og,
+                             const Dom3 &d, GtTable &tab, cudaStream_t s) {
   Runtime &r = rt();
   GtGeom geo;
   GtMaps maps;
@@ -356,16 +356,17 @@ static psb_status staged_run(MapImpl &m, const psb_compiled_stencil &cd, const G
     tab.coef32[k] = (float)m.params[k];
   }
   GridView ov = og->view();
-  return cd.staged(&maps, &tab, &ov, &d, &geo, r.d_error, (unsigned)nblocks, (unsigned)smem,
-                   (void *)s);
+  return fn(&maps, &tab, &ov, &d, &geo, r.d_error, (unsigned)nblocks, (unsigned)smem, (void *)s);
 }
 
 // A compiled stencil's staged form: the map must read only grids of the
 // stencil's type that TMA can stage (at most four distinct ones), never the
-// grid it emits into, and stay inside every grid it reads over the whole
-// domain: the staged reads have no bounds check (a function whose reads
-// may leave the grid, even under a condition, keeps its own form, which
-// checks every read).
+// grid it emits into. When every read range stays inside its grid over the
+// whole domain the unchecked form runs; when one may leave its grid (reads
+// under face tests) the checked form runs, which needs the domain inside
+// every grid read (a read at the point's own coordinate on an axis is then
+// inside, so only the axes a read leaves the point on are checked).
+// Otherwise the function keeps its own form, which checks every read.
 psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, GridImpl **views,
                                   int color, cudaStream_t s) {
   g_last_compiled_staged = 0;
@@ -385,6 +386,7 @@ psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, Gr
   GtPlan p;
   GtTable tab;
   memset(&tab, 0, sizeof(tab));
+  bool inside = true, dom_inside = true;
   for (int i = 0; i < cd.ngrids; i++) {
     GridImpl *g = views[i];
     tab.slot_grid[i] = -1;
@@ -392,9 +394,11 @@ psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, Gr
     if (cd.read_lo[i][0] > cd.read_hi[i][0]) continue;  // not read
     if (g == og || g->type != cd.staged_type || g->pub.num_dims != 3 || !tma_eligible(g))
       return PSB_ERR_UNSUPPORTED;
-    for (int k = 0; k < 3; k++)
+    for (int k = 0; k < 3; k++) {
       if (d.lo[k] + cd.read_lo[i][k] < 0 || d.hi[k] - 1 + cd.read_hi[i][k] > g->pub.dim[k] - 1)
-        return PSB_ERR_UNSUPPORTED;
+        inside = false;
+      if (d.hi[k] > g->pub.dim[k]) dom_inside = false;
+    }
     int gi = -1;
     for (int j = 0; j < p.ngrids; j++)
       if (views[p.slots[j]] == g) gi = j;
@@ -409,9 +413,12 @@ psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, Gr
     p.zmax = std::max(p.zmax, cd.read_hi[i][2]);
   }
   if (p.ngrids == 0) return PSB_ERR_UNSUPPORTED;
-  const psb_status st = cd.staged_type == PS_FLOAT ? staged_run<float>(m, cd, p, og, d, tab, s)
-                                                   : staged_run<double>(m, cd, p, og, d, tab, s);
-  if (st == PSB_OK) g_last_compiled_staged = 1;
+  if (!inside && (!cd.staged_checked || !dom_inside)) return PSB_ERR_UNSUPPORTED;
+  const psb_compiled_staged fn = inside ? cd.staged : cd.staged_checked;
+  tab.read_err = r.d_error + 1;  // where the own form reports reads outside a grid
+  const psb_status st = cd.staged_type == PS_FLOAT ? staged_run<float>(m, fn, p, og, d, tab, s)
+                                                   : staged_run<double>(m, fn, p, og, d, tab, s);
+  if (st == PSB_OK) g_last_compiled_staged = inside ? 1 : 2;
   return st;
 }
 

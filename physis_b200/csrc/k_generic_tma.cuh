@@ -60,6 +60,8 @@ struct GtTable {
   // read) and the parameters' extents; `coef` holds the scalar arguments.
   int slot_grid[PSB_MAX_GRIDS];
   int slot_dims[PSB_MAX_GRIDS][3];
+  // The word a checked read outside its grid sets to PSB_ERR_BOUNDS.
+  int *read_err;
 };
 
 struct GtMaps {

@@ -30,7 +30,18 @@ constexpr int kHtTX = 64, kHtTY = 8, kHtV = 4;
 constexpr int kHtBX = kHtTX + 8;           // every box: x from x0 - 4
 constexpr int kHtBY1 = kHtTY + 4;          // input p: y from y0 - 2
 constexpr int kHtBY2 = kHtTY + 2;          // first sweep and coefficients: y from y0 - 1
-constexpr int kHtS1 = 6, kHtS2 = 4, kHtSC = 4;
+// Ring depths (stages) of R1, R2 and RC; build options for measurement.
+#ifndef PSB_HT_S1
+#define PSB_HT_S1 6
+#endif
+#ifndef PSB_HT_S2
+#define PSB_HT_S2 4
+#endif
+#ifndef PSB_HT_SC
+#define PSB_HT_SC 4
+#endif
+constexpr int kHtS1 = PSB_HT_S1, kHtS2 = PSB_HT_S2, kHtSC = PSB_HT_SC;
+static_assert(kHtS1 <= 8 && kHtS2 <= 8 && kHtSC <= 8, "eight barrier slots per ring");
 constexpr int kHtStage1 = (kHtBX * kHtBY1 * 4 + 127) / 128 * 128;
 constexpr int kHtStage2 = (kHtBX * kHtBY2 * 4 + 127) / 128 * 128;
 constexpr int kHtField = kHtStage2;        // one coefficient box

@@ -703,6 +703,7 @@ psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_i
     if (type_size(d.view_type[v]) == 0) return set_status(PSB_ERR_INVALID);
   for (int i = 0; i < d.nparams; i++)
     if (type_size(d.param_type[i]) == 0) return set_status(PSB_ERR_INVALID);
+  if (d.staged_checked && !d.staged) return set_status(PSB_ERR_INVALID);
   if (d.staged) {
     if ((d.staged_type != PS_FLOAT && d.staged_type != PS_DOUBLE) || d.ndims != 3 ||
         d.staged_emit < 0 || d.staged_emit >= d.ngrids)

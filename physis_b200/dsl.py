@@ -629,23 +629,40 @@ __device__ __forceinline__ int __psb_dim(const __psb_grid<T> &g, int d) {
 // goes to that point's result.
 // A read grid of the staged form: the rows the function reads around the
 // current row of the thread's block, in registers (L::id maps a row's grid,
-// dy and dz to its index), and the point's column v in that row. The library
-// runs the staged form only when every read the function can make over the
-// map's domain lies inside its grid, so reads need no bounds check here.
-template <typename T, class L>
+// dy and dz to its index), and the point's column v in that row. Unchecked
+// (C false): the library runs it only when every read the function can make
+// over the map's domain lies inside its grid. Checked (C true): a read that
+// leaves the point on an axis is tested against the grid there and, outside,
+// reads 0 and marks the thread's flag (*bad), which the program turns into
+// PSB_ERR_BOUNDS once per thread like the function's own form reports it.
+// The library runs it only with the domain inside the grid, so a read at
+// the point's own coordinate on an axis needs no test (the offsets are
+// constants after inlining, so each read keeps the tests of its own axes).
+// The test is a select, not a branch, so the points of a thread's block
+// still schedule together.
+template <typename T, class L, bool C>
 struct __psb_rgrid {
   const psb::GtRow<T> *rows;
   int slot, v, x, y, z;
   int n0, n1, n2;
+  int *bad;
 };
 
-template <typename T, class L>
-__device__ __forceinline__ T __psb_get(const __psb_rgrid<T, L> &g, int i, int j = 0, int k = 0) {
-  return g.rows[L::id(g.slot, j - g.y, k - g.z)].e[2 + (i - g.x) + g.v];
+template <typename T, class L, bool C>
+__device__ __forceinline__ T __psb_get(const __psb_rgrid<T, L, C> &g, int i, int j = 0,
+                                       int k = 0) {
+  const int dx = i - g.x, dy = j - g.y, dz = k - g.z;
+  const T val = g.rows[L::id(g.slot, dy, dz)].e[2 + dx + g.v];
+  if (!C) return val;
+  const bool out = ((dx != 0) & ((unsigned)i >= (unsigned)g.n0)) |
+                   ((dy != 0) & ((unsigned)j >= (unsigned)g.n1)) |
+                   ((dz != 0) & ((unsigned)k >= (unsigned)g.n2));
+  *g.bad |= (int)out;
+  return out ? T(0) : val;
 }
 
-template <typename T, class L>
-__device__ __forceinline__ int __psb_dim(const __psb_rgrid<T, L> &g, int d) {
+template <typename T, class L, bool C>
+__device__ __forceinline__ int __psb_dim(const __psb_rgrid<T, L, C> &g, int d) {
   return d == 0 ? g.n0 : (d == 1 ? g.n1 : g.n2);
 }
 
@@ -880,13 +897,16 @@ def _staged_function(info, params, body):
 
 
 def _staged_entry(info):
-    """The point-wise program, kernel and launcher of the staged form.
+    """The point-wise program, kernels and launchers of the staged form,
+    unchecked and checked (psb_dsl_staged_<name>, psb_dsl_staged_checked_<name>).
 
     For each row of the thread's block the rows the function reads -- one
     per (grid, dy, dz) -- are loaded into registers as the generic packed
     form does (a 16-byte load per thread, x neighbours from the adjacent
     lanes); every read of the function then resolves, at compile time, to a
-    register of one of those rows."""
+    register of one of those rows. The checked form tests the reads that
+    leave the point against their grids first (rows outside a grid hold
+    whatever the window holds there and are never returned)."""
     n = info.name
     t = _CTYPE[info.gparams[0].ctype]
     rows = list(info.staged_rows.items())
@@ -906,8 +926,8 @@ def _staged_entry(info):
         if slot == info.emit_slot:
             handles.append("const __psb_ogrid<T> g%d{&acc.v[r][v], %s};" % (slot, dims))
         else:
-            handles.append("const __psb_rgrid<T, __psb_rows_%s> g%d{rows, %d, v, x, y, at.z, %s};"
-                           % (n, slot, slot, dims))
+            handles.append("const __psb_rgrid<T, __psb_rows_%s, C> g%d{rows, %d, v, x, y, at.z, "
+                           "%s, &bad};" % (n, slot, slot, dims))
         args.append("g%d" % slot)
     for k, (_, st) in enumerate(info.scalars):
         args.append("(%s)tab.coef[%d]" % (_CTYPE[st], k))
@@ -918,6 +938,7 @@ struct __psb_rows_{n} {{
   }}
 }};
 
+template <bool C>
 struct __psb_prog_{n} {{
   static constexpr bool kCompiled = true;
   static constexpr bool kPoints = true;
@@ -928,6 +949,7 @@ struct __psb_prog_{n} {{
   static __device__ __forceinline__ void eval_points(const psb::GtTable &tab,
                                                      const psb::GtAt &at, psb::GtBlk<T> &acc) {{
     const int lane = threadIdx.x & 31;
+    int bad = 0;  // a checked read of this thread's block left its grid
 #pragma unroll
     for (int r = 0; r < psb::kGtVY; r++) {{
       psb::GtRow<T> rows[{nrows}];  // every lane loads: the rows share values by shuffles
@@ -942,32 +964,58 @@ struct __psb_prog_{n} {{
         {n}__staged(x, y, at.z, {args});
       }}
     }}
+    if (C && bad) atomicExch(tab.read_err, (int)PSB_ERR_BOUNDS);
   }}
 }};
 
 extern "C" __global__ void __launch_bounds__(psb::kGtThreads, 2) __psb_staged_kernel_{n}(
     const __grid_constant__ psb::GtMaps maps, const __grid_constant__ psb::GtTable tab,
     psb::GridView out, psb::Dom3 d, const __grid_constant__ psb::GtGeom geo, int *err) {{
-  psb::gt_body<{t}, __psb_prog_{n}>(maps, tab, out, d, geo, err);
+  psb::gt_body<{t}, __psb_prog_{n}<false>>(maps, tab, out, d, geo, err);
+}}
+
+extern "C" __global__ void __launch_bounds__(psb::kGtThreads, 2) __psb_staged_checked_kernel_{n}(
+    const __grid_constant__ psb::GtMaps maps, const __grid_constant__ psb::GtTable tab,
+    psb::GridView out, psb::Dom3 d, const __grid_constant__ psb::GtGeom geo, int *err) {{
+  psb::gt_body<{t}, __psb_prog_{n}<true>>(maps, tab, out, d, geo, err);
+}}
+
+typedef void (*__psb_staged_kernel_t_{n})(psb::GtMaps, psb::GtTable, psb::GridView, psb::Dom3,
+                                          psb::GtGeom, int *);
+
+static psb_status __psb_staged_launch_{n}(__psb_staged_kernel_t_{n} k, unsigned *configured,
+                                          const void *maps, const void *table, const void *out,
+                                          const void *dom, const void *geo, int *err,
+                                          unsigned blocks, unsigned smem, void *stream) {{
+  if (smem > *configured) {{
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
+      return PSB_ERR_CUDA;
+    *configured = smem;
+  }}
+  k<<<blocks, psb::kGtThreads, smem, (cudaStream_t)stream>>>(
+      *(const psb::GtMaps *)maps, *(const psb::GtTable *)table, *(const psb::GridView *)out,
+      *(const psb::Dom3 *)dom, *(const psb::GtGeom *)geo, err);
+  return cudaGetLastError() == cudaSuccess ? PSB_OK : PSB_ERR_CUDA;
 }}
 
 extern "C" psb_status psb_dsl_staged_{n}(const void *maps, const void *table, const void *out,
                                          const void *dom, const void *geo, int *err,
                                          unsigned blocks, unsigned smem, void *stream) {{
   static unsigned configured = 0;
-  if (smem > configured) {{
-    if (cudaFuncSetAttribute(__psb_staged_kernel_{n}, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess ||
-        cudaFuncSetAttribute(__psb_staged_kernel_{n},
-                             cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared) != cudaSuccess)
-      return PSB_ERR_CUDA;
-    configured = smem;
-  }}
-  __psb_staged_kernel_{n}<<<blocks, psb::kGtThreads, smem, (cudaStream_t)stream>>>(
-      *(const psb::GtMaps *)maps, *(const psb::GtTable *)table, *(const psb::GridView *)out,
-      *(const psb::Dom3 *)dom, *(const psb::GtGeom *)geo, err);
-  return cudaGetLastError() == cudaSuccess ? PSB_OK : PSB_ERR_CUDA;
+  return __psb_staged_launch_{n}(__psb_staged_kernel_{n}, &configured, maps, table, out, dom,
+                                 geo, err, blocks, smem, stream);
+}}
+
+extern "C" psb_status psb_dsl_staged_checked_{n}(const void *maps, const void *table,
+                                                 const void *out, const void *dom,
+                                                 const void *geo, int *err, unsigned blocks,
+                                                 unsigned smem, void *stream) {{
+  static unsigned configured = 0;
+  return __psb_staged_launch_{n}(__psb_staged_checked_kernel_{n}, &configured, maps, table, out,
+                                 dom, geo, err, blocks, smem, stream);
 }}
 """.format(n=n, t=t, ids=ids, nrows=len(rows), loads="\n      ".join(loads),
            handles="\n        ".join(handles), args=", ".join(args))
@@ -1064,11 +1112,13 @@ extern "C" void psb_dsl_describe_{n}(psb_compiled_stencil *d) {{
   d->staged_type = {stype};
   d->staged_emit = {semit};
   d->staged = {sfn};
+  d->staged_checked = {cfn};
 }}
 """.format(rlo=arr(_read_ranges(info)[0]), rhi=arr(_read_ranges(info)[1]),
            stype=info.gparams[0].ctype if info.staged else 0,
            semit=info.emit_slot if info.staged else 0,
            sfn=("psb_dsl_staged_%s" % n) if info.staged else "nullptr",
+           cfn=("psb_dsl_staged_checked_%s" % n) if info.staged else "nullptr",
            n=n, binds="\n".join(binds), args=", ".join(args), gt=arr(info.grid_types),
            gn=arr(nd for _, _, nd in info.grids), gc=arr(comps), vt=arr(info.view_type),
            ve=arr(info.view_emits), vr=arr(info.view_reads_offset),

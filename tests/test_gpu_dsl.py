@@ -48,29 +48,34 @@ def test_compiled_stencil_matches_golden(name, layout, form, kernels):
     finally:
         ps.set_impl(ps.IMPL_AUTO)
     assert C.dump_text(out, case["fmt"]) == C.golden_text(name)
-    assert staged == (form == "staged" and _staged_fits(kernels[fn].info, case)), \
-        (name, layout, form)
+    want = _staged_form(kernels[fn].info, case) if form == "staged" else 0
+    assert staged == want, (name, layout, form)
 
 
-def _staged_fits(info, case):
-    """Whether the library may run the last map of the case in its staged
-    form: the function has one, the map is not red-black, does not read the
-    grid it emits into, and every read range stays inside its grid over the
-    domain."""
+def _staged_form(info, case):
+    """Which form the library runs for the last map of the case: 0 the
+    function's own, 1 the staged form (every read range inside its grid over
+    the domain), 2 the checked staged form (a read range may leave its grid,
+    the domain lies inside every grid read). The staged forms need a
+    function that has them, no red-black colour and the emitted grid not
+    read."""
     if not info.staged:
-        return False
+        return 0
     slots, color = case["run"][-1]
     if color == 2:
-        return False
+        return 0
     lo, hi = case["dom"]
     out = slots[info.emit_slot]
+    inside = dom_inside = True
     for param, (rlo, rhi) in info.staged_reads.items():
         if slots[param] == out:
-            return False
+            return 0
         dims = case["grids"][slots[param]][1]
         if any(lo[k] + rlo[k] < 0 or hi[k] - 1 + rhi[k] > dims[k] - 1 for k in range(3)):
-            return False
-    return True
+            inside = False
+        if any(hi[k] > dims[k] for k in range(3)):
+            dom_inside = False
+    return 1 if inside else (2 if dom_inside else 0)
 
 
 USER = D.user_cases()
@@ -122,32 +127,90 @@ def test_point_type_stencil_matches_golden(name, tmp_path):
     assert _run_user_case(case, ks) == C.golden_text(name)
 
 
+def _forms_run(form, fn):
+    """fn() under the staged forms (the library's choice) or with the
+    function's own launch forced; returns fn's result."""
+    if form == "own":
+        ps.set_impl(ps.IMPL_GENERIC)
+    try:
+        return fn()
+    finally:
+        ps.set_impl(ps.IMPL_AUTO)
+
+
 @pytest.mark.gpu
-def test_read_outside_the_grid_is_reported_not_performed(tmp_path):
-    """x+1 at the last column leaves the grid: the read returns 0, nothing
-    outside the grid is touched, and psb_sync reports PSB_ERR_BOUNDS."""
+@pytest.mark.parametrize("form", ["staged", "own"])
+@pytest.mark.parametrize("layout", sorted(U.LAYOUTS))
+def test_read_outside_the_grid_is_reported_not_performed(tmp_path, form, layout):
+    """x+1 at the last column and z-2 at the first two planes leave the grid:
+    those reads return 0, nothing outside the grid is touched, and psb_sync
+    reports PSB_ERR_BOUNDS, in the checked staged form as in the function's
+    own form."""
     from physis_b200 import dsl
     k = dsl.compile_stencils("""
     void right(const int x, const int y, const int z, PSGrid3DFloat a, PSGrid3DFloat b) {
-      PSGridEmit(b, PSGridGet(a, x + 1, y, z) + 1.0f);
+      PSGridEmit(b, PSGridGet(a, x + 1, y, z) + 2.0f * PSGridGet(a, x, y, z - 2) + 1.0f);
     }""", str(tmp_path))["right"]
     n = 16
-    a = ps.grid_new(ps.PS_FLOAT, (n, n, n))
-    b = ps.grid_new(ps.PS_FLOAT, (n, n, n))
+    a = ps.grid_new(ps.PS_FLOAT, (n, n, n), U.LAYOUTS[layout])
+    b = ps.grid_new(ps.PS_FLOAT, (n, n, n), U.LAYOUTS[layout])
     src = np.arange(n ** 3, dtype=np.float32).reshape(n, n, n)
     ps.PSGridCopyin(a, src)
-    ps.PSStencilRun(ps.PSStencilMap(k.kernel_id, ps.PSDomain3DNew(0, n, 0, n, 0, n), a, b), 1)
-    with pytest.raises(ps.PhysisError) as e:
-        ps.sync()
-    assert e.value.status == ps.PSB_ERR_BOUNDS
+
+    def run():
+        ps.PSStencilRun(ps.PSStencilMap(k.kernel_id, ps.PSDomain3DNew(0, n, 0, n, 0, n), a, b), 1)
+        with pytest.raises(ps.PhysisError) as e:
+            ps.sync()
+        return e.value.status, ps.compiled_last_staged()
+    status, staged = _forms_run(form, run)
+    assert status == ps.PSB_ERR_BOUNDS
+    assert staged == (2 if form == "staged" else 0)
     ps.sync()  # the error word was cleared
     out = ps.PSGridCopyout(b)
-    expect = np.empty_like(src)
-    expect[:, :, :-1] = src[:, :, 1:] + np.float32(1)
-    expect[:, :, -1] = np.float32(1)
+    right = np.zeros_like(src)
+    right[:, :, :-1] = src[:, :, 1:]
+    down = np.zeros_like(src)
+    down[2:] = src[:-2]
+    expect = (right + np.float32(2) * down) + np.float32(1)
     assert np.array_equal(out, expect)
     for g in (a, b):
         ps.PSGridFree(g)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form", ["staged", "own"])
+@pytest.mark.parametrize("layout", sorted(U.LAYOUTS))
+@pytest.mark.parametrize("dims", [(40, 24, 20), (37, 29, 23), (5, 3, 4)])
+def test_face_test_diffusion_matches_oracle(form, layout, dims):
+    """The reference's 7-point diffusion kernel as written in the DSL (reads
+    under face tests, examples/diffusion-benchmark/diffusion3d_physis.c:29-58)
+    over the whole grid runs the checked staged form and equals the oracle's
+    clamped diffusion bit for bit, like the function's own form; no read
+    leaves the grid, so no error is reported."""
+    from physis_b200 import dsl
+    from physis_b200.workloads import DIFFUSION7_DSL
+    from oracle import oracle as O
+    k = dsl.compile_stencils(DIFFUSION7_DSL)["diffusion7"]
+    coef = [0.1, 0.11, 0.12, 0.13, 0.14, 0.15, 0.25]  # ce cw cn cs ct cb cc
+    field = np.random.default_rng(11).random(dims[::-1], dtype=np.float32)
+    g = [ps.grid_new(ps.PS_FLOAT, dims, U.LAYOUTS[layout]) for _ in range(2)]
+    ps.PSGridCopyin(g[0], field)
+    d = ps.PSDomain3DNew(0, dims[0], 0, dims[1], 0, dims[2])
+
+    def run():
+        m1 = ps.PSStencilMap(k.kernel_id, d, g[0], g[1], *coef)
+        m2 = ps.PSStencilMap(k.kernel_id, d, g[1], g[0], *coef)
+        ps.PSStencilRun(m1, m2, 3)
+        ps.sync()
+        return ps.compiled_last_staged()
+    staged = _forms_run(form, run)
+    out = ps.PSGridCopyout(g[0])
+    for x in g:
+        ps.PSGridFree(x)
+    # Dense rows and planes must be 16-byte multiples for TMA.
+    tma = layout == "pitched" or (dims[0] % 4 == 0 and dims[0] * dims[1] % 4 == 0)
+    assert staged == (2 if form == "staged" and tma else 0)
+    assert U.bits_equal(out, O.diffusion7(field, 6, coef))
 
 
 @pytest.mark.gpu
