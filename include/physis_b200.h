@@ -659,7 +659,10 @@ psb_status psb_last_run_stats(double *device_ms, int64_t *launches);
 
 /* Tile configuration of the fast kernels; the autotuner picks one per
  * (kernel, type, nx, ny, nz) and caches it in a JSON file
- * ($PHYSIS_B200_TUNE_CACHE, default ~/.cache/physis_b200_tune.json). */
+ * ($PHYSIS_B200_TUNE_CACHE, default ~/.cache/physis_b200_tune.json). The
+ * table measured on B200 (physis_b200/tune_b200.json, beside the library)
+ * loads first and the user cache's entries win; PHYSIS_B200_TUNE_SHIPPED=0
+ * leaves it out. */
 typedef struct {
   int impl;         /* psb_impl */
   int tile_x;       /* points per CTA in x */

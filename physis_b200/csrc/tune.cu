@@ -108,7 +108,10 @@ static void load_cache() {
   if (r.tune_loaded) return;
   r.tune_loaded = true;
   r.tune_path = cache_path();
-  std::string shipped = shipped_path();
+  // PHYSIS_B200_TUNE_SHIPPED=0 leaves the shipped table out (only the user
+  // cache and the library's own rules apply).
+  const char *use_shipped = getenv("PHYSIS_B200_TUNE_SHIPPED");
+  std::string shipped = use_shipped && use_shipped[0] == '0' ? "" : shipped_path();
   if (!shipped.empty()) parse_cache_file(shipped);
   parse_cache_file(r.tune_path);
 }
