@@ -475,6 +475,12 @@ def run_ours(args):
     tune = None
     if kname not in ("generic27", "dsl7", "dsl27"):
         tune = ps.autotune(kernel, ptype, dims) if args.tune else ps.tune_get(kernel, ptype, dims)
+        if args.t_depth and kname == "diffusion7" and dt == np.float32:
+            # pin the temporal depth of this shape (profiling)
+            tune = dict(tune, t_depth=args.t_depth)
+            if args.t_depth == 2:
+                tune.update(impl=ps.IMPL_TMA, tile_x=128, tile_y=16)
+            ps.tune_set(kernel, ptype, dims, **tune)
     if args.plain:
         # the thread-per-point shape of the reference's generated kernels
         ps.set_impl(ps.IMPL_GENERIC if kname == "generic27" else ps.IMPL_PLAIN)
@@ -601,7 +607,9 @@ def run_ours(args):
     # bandwidth and may exceed the copy peak.
     achieved = bpl * pts_per_step * args.steps / dev_s / 1e9
     two_sweeps = kname == "himeno" and tune is not None and tune.get("t_depth") == 2
+    two_steps = kname == "diffusion7" and tune is not None and tune.get("t_depth") == 2
     kname_traffic = ("k_himeno_tb2" if two_sweeps else "k_himeno_tma") if kname == "himeno" else \
+        ("k_diff7_tb2_f32" + ("_fma" if fma else "")) if two_steps else \
         "k_generic_tma_f32" if kname == "generic27" else "k_dsl_diffusion7_f32" if kname == "dsl7" \
         else "k_dsl_box27_f32" if kname == "dsl27" else (
         "k_diff7_tma_f32" if dt == np.float32 else "k_diff7_tma_f64") + ("_fma" if fma else "")
@@ -1430,6 +1438,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--tune", action="store_true", help="autotune before timing")
+    ap.add_argument("--t-depth", type=int, default=0, choices=[0, 1, 2],
+                    help="7-point fp32: pin the time steps per launch (2: temporal blocking; "
+                         "profiling)")
     ap.add_argument("--plain", action="store_true", help="time the plain one-launch kernel")
     ap.add_argument("--fp-mode", default="auto", choices=["auto", "exact", "fma"],
                     help="arithmetic of the 7-point TMA kernel (auto: fma, with the exact "

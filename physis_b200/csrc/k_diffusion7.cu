@@ -204,6 +204,7 @@ struct TbGeom {
   int64_t items;
 };
 
+template <bool FAST>
 __global__ void __launch_bounds__(kTbThreads, 1) k_diff7_tb2(const __grid_constant__ CUtensorMap tin,
                                                              GridView out, int nx, int ny, int nz,
                                                              C7<float> k, TbGeom tg, int *err) {
@@ -259,14 +260,16 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_diff7_tb2(const __grid_consta
         return;
       }
     } else if (warp <= kTbS1Warps) {
-      ok = diff7_tb_stage1(R1, p1, R2, p2, threadIdx.x - 32, nx, ny, nz, k, x0, y0, zb, nzl);
+      ok = diff7_tb_stage1<FAST>(R1, p1, R2, p2, threadIdx.x - 32, nx, ny, nz, k, x0, y0, zb,
+                                 nzl);
       if (!ok) {
         if ((threadIdx.x & 31) == 0) atomicExch(err, 1);
         return;
       }
     } else {
-      ok = diff7_consume<float, false, false>(R2, p2, out, nx, ny, nz, d, k, g2, x0, y0, zb, nzl,
-                                              0, nullptr, threadIdx.x - 32 - 32 * kTbS1Warps);
+      ok = diff7_consume<float, false, false, FAST>(R2, p2, out, nx, ny, nz, d, k, g2, x0, y0,
+                                                    zb, nzl, 0, nullptr,
+                                                    threadIdx.x - 32 - 32 * kTbS1Warps);
       if (!ok) {
         if ((threadIdx.x & 31) == 0) atomicExch(err, 1);
         return;
@@ -276,16 +279,19 @@ __global__ void __launch_bounds__(kTbThreads, 1) k_diff7_tb2(const __grid_consta
 }
 
 // Two steps of the clamped float 7-point map m over the whole grid: reads
-// in, writes out (the intermediate step exists only in shared memory).
+// in, writes out (the intermediate step exists only in shared memory). In
+// the FMA arithmetic mode both steps use the contracted form, point for
+// point as the single-step FMA kernel does.
 psb_status diffusion7_tb2_launch(MapImpl &m, GridImpl *in, GridImpl *out, int zchunk,
                                  cudaStream_t s, int64_t *launches) {
   const CUtensorMap *map = nullptr;
   PSB_CHECK(get_tmap(in, kTbBX1, kTbBY1, &map));
-  static bool configured = false;
-  if (!configured) {
-    PSB_TRY(cudaFuncSetAttribute(k_diff7_tb2, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 kTbSmem));
-    configured = true;
+  const bool fast = rt().fp_mode == PSB_FP_FMA;
+  static bool configured[2] = {false, false};
+  if (!configured[fast]) {
+    PSB_TRY(cudaFuncSetAttribute(fast ? k_diff7_tb2<true> : k_diff7_tb2<false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, kTbSmem));
+    configured[fast] = true;
   }
   TbGeom tg;
   tg.ax0 = in->pad_left;
@@ -299,9 +305,8 @@ psb_status diffusion7_tb2_launch(MapImpl &m, GridImpl *in, GridImpl *out, int zc
   C7<float> k{(float)m.params[0], (float)m.params[1], (float)m.params[2], (float)m.params[3],
               (float)m.params[4], (float)m.params[5], (float)m.params[6]};
   const int blocks = (int)std::min<int64_t>(rt().sm_count, tg.items);
-  k_diff7_tb2<<<blocks, kTbThreads, kTbSmem, s>>>(*map, out->view(), in->pub.dim[0],
-                                                  in->pub.dim[1], in->pub.dim[2], k, tg,
-                                                  rt().d_error);
+  (fast ? k_diff7_tb2<true> : k_diff7_tb2<false>)<<<blocks, kTbThreads, kTbSmem, s>>>(
+      *map, out->view(), in->pub.dim[0], in->pub.dim[1], in->pub.dim[2], k, tg, rt().d_error);
   (*launches)++;
   PSB_TRY(cudaGetLastError());
   return PSB_OK;

@@ -457,6 +457,9 @@ constexpr int kTbThreads = 32 + 32 * kTbS1Warps + 32 * kTbS2Warps;
 // input planes zb-2 .. zb+nzl+1 (ring R1, all released), written to ring R2
 // (this group fills its stages; the stage-2 warps release them). t1 is the
 // thread's index in the stage-1 group.
+// FAST: the contracted arithmetic of the FMA mode (diff7_row_fast,
+// diff7_point<FAST>), as the single-step FMA kernel computes each point.
+template <bool FAST = false>
 __device__ __forceinline__ bool diff7_tb_stage1(const Ring &R1, RingPos &p1, const Ring &R2,
                                                 RingPos &p2, int t1, int nx, int ny, int nz,
                                                 const C7<float> k, int x0, int y0, int zb,
@@ -536,9 +539,14 @@ __device__ __forceinline__ bool diff7_tb_stage1(const Ring &R1, RingPos &p1, con
     Vec16<float> res[VY];
     if (!(yedge || zedge)) {
 #pragma unroll
-      for (int r = 0; r < VY; r++)
-        res[r] = diff7_row(kk, vc[r], wl[r], er[r], r == 0 ? vn : vc[r - 1],
-                           r == VY - 1 ? vs : vc[r + 1], vb[r], vt[r], xfix);
+      for (int r = 0; r < VY; r++) {
+        if constexpr (FAST)
+          res[r] = diff7_row_fast(kk, vc[r], wl[r], er[r], r == 0 ? vn : vc[r - 1],
+                                  r == VY - 1 ? vs : vc[r + 1], vb[r], vt[r], xfix);
+        else
+          res[r] = diff7_row(kk, vc[r], wl[r], er[r], r == 0 ? vn : vc[r - 1],
+                             r == VY - 1 ? vs : vc[r + 1], vb[r], vt[r], xfix);
+      }
     } else {
 #pragma unroll
       for (int r = 0; r < VY; r++) {
@@ -558,7 +566,7 @@ __device__ __forceinline__ bool diff7_tb_stage1(const Ring &R1, RingPos &p1, con
           if (y == ny - 1) s = c;
           if (z == 0) bb = c;
           if (z == nz - 1) t = c;
-          res[r].v[v] = diff7_point(k, c, w, e, n, s, bb, t);
+          res[r].v[v] = diff7_point<float, FAST>(k, c, w, e, n, s, bb, t);
         }
       }
     }
@@ -571,7 +579,7 @@ __device__ __forceinline__ bool diff7_tb_stage1(const Ring &R1, RingPos &p1, con
       if (ey == ny - 1) s = ec;
       if (z == 0) bb = ec;
       if (z == nz - 1) t = ec;
-      eres = diff7_point(k, ec, w, e, n, s, bb, t);
+      eres = diff7_point<float, FAST>(k, ec, w, e, n, s, bb, t);
       eb = ec;
       ec = et;
     }

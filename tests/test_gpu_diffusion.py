@@ -147,3 +147,44 @@ def test_temporal_blocking_bit_exact(shape, pairs, zchunk):
     assert U.bits_equal(got2, want2)
     fused = (pairs - 1) & ~1
     assert launches == fused + 2 * (pairs - fused)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape,pairs,zchunk", [
+    ((8, 16, 128), 3, 8),
+    ((37, 50, 130), 5, 16),
+    ((70, 20, 300), 6, 32),
+])
+def test_temporal_blocking_fma_mode_equals_single_fma_steps(shape, pairs, zchunk):
+    """In the FMA arithmetic mode the two-step kernel computes every point as
+    the single-step FMA kernel does: the same bits as single FMA steps."""
+    f = np.random.default_rng(7 + sum(shape)).random(shape, dtype=np.float32)
+    nz, ny, nx = shape
+    dims = (nx, ny, nz)
+    old = ps.tune_get(ps.DIFFUSION7, ps.PS_FLOAT, dims)
+    ps.set_fp_mode(ps.FP_FMA)
+    try:
+        got1, got2, launches = _tb_run(f, pairs, zchunk)
+        ps.tune_set(ps.DIFFUSION7, ps.PS_FLOAT, dims, impl=ps.IMPL_TMA, tile_x=128, tile_y=8,
+                    z_chunk=zchunk, stages=6, t_depth=1)
+        g1 = ps.grid_new(ps.PS_FLOAT, dims)
+        g2 = ps.grid_new(ps.PS_FLOAT, dims)
+        try:
+            ps.PSGridCopyin(g1, f)
+            d = ps.PSDomain3DNew(0, nx, 0, ny, 0, nz)
+            m1 = ps.PSStencilMap(ps.DIFFUSION7, d, g1, g2, *COEF)
+            m2 = ps.PSStencilMap(ps.DIFFUSION7, d, g2, g1, *COEF)
+            ps.PSStencilRun(m1, m2, pairs)
+            want1, want2 = ps.PSGridCopyout(g1), ps.PSGridCopyout(g2)
+        finally:
+            ps.PSGridFree(g1)
+            ps.PSGridFree(g2)
+    finally:
+        ps.set_fp_mode(ps.FP_EXACT)
+        ps.tune_set(ps.DIFFUSION7, ps.PS_FLOAT, dims, **old)
+    fused = (pairs - 1) & ~1
+    assert launches == fused + 2 * (pairs - fused)
+    assert U.bits_equal(got1, want1)
+    assert U.bits_equal(got2, want2)
+    # and not the exact arithmetic's bits (the FMA form ran)
+    assert not U.bits_equal(got1, oracle.diffusion7(f, 2 * pairs, COEF))
