@@ -480,6 +480,8 @@ def run_ours(args):
             tune = dict(tune, t_depth=args.t_depth)
             if args.t_depth == 2:
                 tune.update(impl=ps.IMPL_TMA, tile_x=128, tile_y=16)
+            if args.z_chunk:
+                tune.update(z_chunk=args.z_chunk)
             ps.tune_set(kernel, ptype, dims, **tune)
     if args.plain:
         # the thread-per-point shape of the reference's generated kernels
@@ -1441,6 +1443,8 @@ def main():
     ap.add_argument("--t-depth", type=int, default=0, choices=[0, 1, 2],
                     help="7-point fp32: pin the time steps per launch (2: temporal blocking; "
                          "profiling)")
+    ap.add_argument("--z-chunk", type=int, default=0,
+                    help="with --t-depth: pin the z chunk as well (profiling)")
     ap.add_argument("--plain", action="store_true", help="time the plain one-launch kernel")
     ap.add_argument("--fp-mode", default="auto", choices=["auto", "exact", "fma"],
                     help="arithmetic of the 7-point TMA kernel (auto: fma, with the exact "
