@@ -543,13 +543,18 @@ typedef struct {
    * reads 0 and sets PSB_ERR_BOUNDS, as `launch` does). The library runs it
    * when a read range may leave its grid over the domain (reads under face
    * tests, e.g. `x == 0 ? c : PSGridGet(g, x-1, y, z)`) and the domain lies
-   * inside every grid read. */
+   * inside every grid read.
+   * read_periodic[g] = 1: grid g is read only with PSGridGetPeriodic (within
+   * +-2); the staged forms read its wrapped values from the pitched grid's
+   * halo, which the library refreshes first, so they run for such a grid
+   * only when it is pitched (PSGrid*New). */
   int staged_type;
   int staged_emit;
   int read_lo[PSB_MAX_GRIDS][3];
   int read_hi[PSB_MAX_GRIDS][3];
   psb_compiled_staged staged;
   psb_compiled_staged staged_checked;
+  int read_periodic[PSB_MAX_GRIDS];
 } psb_compiled_stencil;
 
 psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_id);

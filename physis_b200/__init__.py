@@ -123,7 +123,8 @@ class CompiledStencilStruct(ctypes.Structure):
                 ("staged_type", ctypes.c_int), ("staged_emit", ctypes.c_int),
                 ("read_lo", (ctypes.c_int * 3) * PSB_MAX_GRIDS),
                 ("read_hi", (ctypes.c_int * 3) * PSB_MAX_GRIDS), ("staged", ctypes.c_void_p),
-                ("staged_checked", ctypes.c_void_p)]
+                ("staged_checked", ctypes.c_void_p),
+                ("read_periodic", ctypes.c_int * PSB_MAX_GRIDS)]
 
 
 class TuneConfig(ctypes.Structure):

@@ -394,8 +394,12 @@ psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, Gr
     if (cd.read_lo[i][0] > cd.read_hi[i][0]) continue;  // not read
     if (g == og || g->type != cd.staged_type || g->pub.num_dims != 3 || !tma_eligible(g))
       return PSB_ERR_UNSUPPORTED;
+    // Periodic reads take the wrapped values from the halo of a pitched grid.
+    const bool per = cd.read_periodic[i] != 0;
+    if (per && (g->layout != PSB_LAYOUT_PITCHED || g->halo < kGtR)) return PSB_ERR_UNSUPPORTED;
     for (int k = 0; k < 3; k++) {
-      if (d.lo[k] + cd.read_lo[i][k] < 0 || d.hi[k] - 1 + cd.read_hi[i][k] > g->pub.dim[k] - 1)
+      if (!per &&
+          (d.lo[k] + cd.read_lo[i][k] < 0 || d.hi[k] - 1 + cd.read_hi[i][k] > g->pub.dim[k] - 1))
         inside = false;
       if (d.hi[k] > g->pub.dim[k]) dom_inside = false;
     }
@@ -408,12 +412,26 @@ psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, Gr
       p.slots[gi] = i;
       p.mode[gi] = PSB_BOUNDARY_NONE;
     }
+    // One grid bound to parameters read both ways has no single window form.
+    if (p.mode[gi] != PSB_BOUNDARY_NONE && !per) return PSB_ERR_UNSUPPORTED;
+    if (per) {
+      for (int j = 0; j < i; j++)
+        if (views[j] == g && !cd.read_periodic[j] && cd.read_lo[j][0] <= cd.read_hi[j][0])
+          return PSB_ERR_UNSUPPORTED;
+      p.mode[gi] = PSB_BOUNDARY_PERIODIC;
+    }
     tab.slot_grid[i] = gi;
     p.zmin = std::min(p.zmin, cd.read_lo[i][2]);
     p.zmax = std::max(p.zmax, cd.read_hi[i][2]);
   }
   if (p.ngrids == 0) return PSB_ERR_UNSUPPORTED;
   if (!inside && (!cd.staged_checked || !dom_inside)) return PSB_ERR_UNSUPPORTED;
+  // Periodic reads take the halo: refresh it where it is stale.
+  for (int i = 0; i < p.ngrids; i++) {
+    GridImpl *g = views[p.slots[i]];
+    if (p.mode[i] != PSB_BOUNDARY_NONE && g->ghost_valid != p.mode[i])
+      PSB_CHECK(launch_halo_fill(g, p.mode[i], s));
+  }
   const psb_compiled_staged fn = inside ? cd.staged : cd.staged_checked;
   tab.read_err = r.d_error + 1;  // where the own form reports reads outside a grid
   const psb_status st = cd.staged_type == PS_FLOAT ? staged_run<float>(m, fn, p, og, d, tab, s)

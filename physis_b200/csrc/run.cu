@@ -711,7 +711,10 @@ psb_status psb_compiled_register(const psb_compiled_stencil *desc, int *kernel_i
     for (int i = 0; i < d.ngrids; i++) {
       if (d.grid_type[i] != d.staged_type || d.grid_ndims[i] != 3)
         return set_status(PSB_ERR_INVALID);
-      if (d.read_lo[i][0] > d.read_hi[i][0]) continue;  // not read
+      if (d.read_lo[i][0] > d.read_hi[i][0]) {  // not read
+        if (d.read_periodic[i]) return set_status(PSB_ERR_INVALID);
+        continue;
+      }
       if (i == d.staged_emit) return set_status(PSB_ERR_INVALID);
       for (int k = 0; k < 3; k++)
         if (d.read_lo[i][k] < -2 || d.read_hi[i][k] > 2 || d.read_lo[i][k] > d.read_hi[i][k])

@@ -205,6 +205,11 @@ class StencilInfo:
         self.staged_ok = ndims == 3
         self.staged_reads = {}      # grid slot -> [lo[3], hi[3]]
         self.staged_rows = {}       # (slot, dy, dz) -> [dx min, dx max], in first-read order
+        # Grid slots read with PSGridGetPeriodic (only so: a grid read both
+        # ways rules the staged form out); the staged form takes their wrapped
+        # values from the pitched grid's refreshed halo.
+        self.staged_periodic = set()
+        self.staged_plain = set()
         self.emit_count = 0
         self.emit_slot = None
         self.staged = False
@@ -381,11 +386,15 @@ class _Rewriter:
         return [c_ast.ID(n) for n in self.index_names] + [_int(0)] * (3 - len(self.index_names))
 
     def _staged_read(self, slot, p, forms, periodic):
-        """Record a plain read for the staged form, or rule the form out."""
+        """Record a read for the staged form, or rule the form out."""
         if self.info is None:
             return
-        if periodic or p.struct is not None or p.nd != 3 or len(forms) != 3 or \
+        if p.struct is not None or p.nd != 3 or len(forms) != 3 or \
                 any(f is None or f[0] != k or abs(f[1]) > 2 for k, f in enumerate(forms)):
+            self.info.staged_ok = False
+            return
+        (self.info.staged_periodic if periodic else self.info.staged_plain).add(slot)
+        if self.info.staged_periodic & self.info.staged_plain:
             self.info.staged_ok = False
             return
         lo, hi = self.info.staged_reads.setdefault(slot, [[2, 2, 2], [-2, -2, -2]])
@@ -659,6 +668,14 @@ __device__ __forceinline__ T __psb_get(const __psb_rgrid<T, L, C> &g, int i, int
                    ((dz != 0) & ((unsigned)k >= (unsigned)g.n2));
   *g.bad |= (int)out;
   return out ? T(0) : val;
+}
+
+// A periodic read: the window holds the wrapped values (the library
+// refreshes the pitched grid's halo first), so it needs no check.
+template <typename T, class L, bool C>
+__device__ __forceinline__ T __psb_getp(const __psb_rgrid<T, L, C> &g, int i, int j = 0,
+                                        int k = 0) {
+  return g.rows[L::id(g.slot, j - g.y, k - g.z)].e[2 + (i - g.x) + g.v];
 }
 
 template <typename T, class L, bool C>
@@ -1113,12 +1130,16 @@ extern "C" void psb_dsl_describe_{n}(psb_compiled_stencil *d) {{
   d->staged_emit = {semit};
   d->staged = {sfn};
   d->staged_checked = {cfn};
+  const int rper[] = {{{rper}}};
+  for (int i = 0; i < PSB_MAX_GRIDS; i++) d->read_periodic[i] = i < {ng} ? rper[i] : 0;
 }}
 """.format(rlo=arr(_read_ranges(info)[0]), rhi=arr(_read_ranges(info)[1]),
            stype=info.gparams[0].ctype if info.staged else 0,
            semit=info.emit_slot if info.staged else 0,
            sfn=("psb_dsl_staged_%s" % n) if info.staged else "nullptr",
            cfn=("psb_dsl_staged_checked_%s" % n) if info.staged else "nullptr",
+           rper=arr(1 if info.staged and slot in info.staged_periodic else 0
+                    for slot in range(len(info.grids))),
            n=n, binds="\n".join(binds), args=", ".join(args), gt=arr(info.grid_types),
            gn=arr(nd for _, _, nd in info.grids), gc=arr(comps), vt=arr(info.view_type),
            ve=arr(info.view_emits), vr=arr(info.view_reads_offset),

@@ -48,21 +48,24 @@ def test_compiled_stencil_matches_golden(name, layout, form, kernels):
     finally:
         ps.set_impl(ps.IMPL_AUTO)
     assert C.dump_text(out, case["fmt"]) == C.golden_text(name)
-    want = _staged_form(kernels[fn].info, case) if form == "staged" else 0
+    want = _staged_form(kernels[fn].info, case, layout) if form == "staged" else 0
     assert staged == want, (name, layout, form)
 
 
-def _staged_form(info, case):
+def _staged_form(info, case, layout):
     """Which form the library runs for the last map of the case: 0 the
-    function's own, 1 the staged form (every read range inside its grid over
-    the domain), 2 the checked staged form (a read range may leave its grid,
-    the domain lies inside every grid read). The staged forms need a
-    function that has them, no red-black colour and the emitted grid not
-    read."""
+    function's own, 1 the staged form (every plain read range inside its grid
+    over the domain), 2 the checked staged form (a plain read range may leave
+    its grid, the domain lies inside every grid read). The staged forms need
+    a function that has them, no red-black colour, the emitted grid not read,
+    and pitched grids for periodic reads (their wrapped values come from the
+    halo)."""
     if not info.staged:
         return 0
     slots, color = case["run"][-1]
     if color == 2:
+        return 0
+    if info.staged_periodic and layout != "pitched":
         return 0
     lo, hi = case["dom"]
     out = slots[info.emit_slot]
@@ -71,7 +74,8 @@ def _staged_form(info, case):
         if slots[param] == out:
             return 0
         dims = case["grids"][slots[param]][1]
-        if any(lo[k] + rlo[k] < 0 or hi[k] - 1 + rhi[k] > dims[k] - 1 for k in range(3)):
+        if param not in info.staged_periodic and \
+                any(lo[k] + rlo[k] < 0 or hi[k] - 1 + rhi[k] > dims[k] - 1 for k in range(3)):
             inside = False
         if any(hi[k] > dims[k] for k in range(3)):
             dom_inside = False
@@ -290,3 +294,55 @@ def test_point_type_transpose_with_loop_subscripts(tmp_path):
         ps.PSGridFree(a)
         ps.PSGridFree(b)
     assert np.array_equal(out["p"], np.swapaxes(recs["p"], -1, -2))
+
+
+PERIODIC7_DSL = """
+void wrapdiff(const int x, const int y, const int z, PSGrid3DFloat u, PSGrid3DFloat v,
+              float ce, float cw, float cn, float cs, float ct, float cb, float cc) {
+  float c = PSGridGet(u, x, y, z);
+  float w = PSGridGetPeriodic(u, x - 1, y, z);
+  float e = PSGridGetPeriodic(u, x + 1, y, z);
+  float n = PSGridGetPeriodic(u, x, y - 1, z);
+  float s = PSGridGetPeriodic(u, x, y + 1, z);
+  float b = PSGridGetPeriodic(u, x, y, z - 1);
+  float t = PSGridGetPeriodic(u, x, y, z + 1);
+  PSGridEmit(v, cc * c + cw * w + ce * e + cs * s + cn * n + cb * b + ct * t);
+}
+"""
+
+PERIODIC7_ONLY_DSL = PERIODIC7_DSL.replace("wrapdiff", "wrapdiff2").replace(
+    "PSGridGet(u, x, y, z)", "PSGridGetPeriodic(u, x, y, z)")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("layout", sorted(U.LAYOUTS))
+@pytest.mark.parametrize("dims", [(40, 24, 20), (37, 29, 23)])
+def test_periodic_reads_staged_match_oracle(layout, dims, tmp_path):
+    """A 7-point stencil whose neighbour reads wrap (PSGridGetPeriodic) runs
+    staged on pitched grids -- the wrapped values come from the refreshed
+    halo -- and equals the oracle's periodic diffusion bit for bit over a
+    double-buffered run; dense grids (no halo) keep the function's own form.
+    A grid read both plainly and periodically has no staged form."""
+    from physis_b200 import dsl
+    from oracle import oracle as O
+    ks = dsl.compile_stencils(PERIODIC7_DSL + PERIODIC7_ONLY_DSL, str(tmp_path))
+    assert not ks["wrapdiff"].info.staged and ks["wrapdiff2"].info.staged
+    coef = [0.1, 0.11, 0.12, 0.13, 0.14, 0.15, 0.25]  # ce cw cn cs ct cb cc
+    field = np.random.default_rng(5).random(dims[::-1], dtype=np.float32)
+    want = O.diffusion7(field, 6, coef, periodic=True)
+    for name in ("wrapdiff", "wrapdiff2"):
+        g = [ps.grid_new(ps.PS_FLOAT, dims, U.LAYOUTS[layout]) for _ in range(2)]
+        try:
+            ps.PSGridCopyin(g[0], field)
+            d = ps.PSDomain3DNew(0, dims[0], 0, dims[1], 0, dims[2])
+            m1 = ps.PSStencilMap(ks[name].kernel_id, d, g[0], g[1], *coef)
+            m2 = ps.PSStencilMap(ks[name].kernel_id, d, g[1], g[0], *coef)
+            ps.PSStencilRun(m1, m2, 3)
+            ps.sync()
+            staged = ps.compiled_last_staged()
+            out = ps.PSGridCopyout(g[0])
+        finally:
+            for x in g:
+                ps.PSGridFree(x)
+        assert staged == (1 if name == "wrapdiff2" and layout == "pitched" else 0), (name, layout)
+        assert U.bits_equal(out, want), (name, layout)
