@@ -544,10 +544,11 @@ typedef struct {
    * when a read range may leave its grid over the domain (reads under face
    * tests, e.g. `x == 0 ? c : PSGridGet(g, x-1, y, z)`) and the domain lies
    * inside every grid read.
-   * read_periodic[g] = 1: grid g is read only with PSGridGetPeriodic (within
-   * +-2); the staged forms read its wrapped values from the pitched grid's
-   * halo, which the library refreshes first, so they run for such a grid
-   * only when it is pitched (PSGrid*New). */
+   * read_periodic[g] = 1: grid g is read with PSGridGetPeriodic (within
+   * +-2; read_lo/read_hi cover these reads and any plain ones); the staged
+   * forms read its wrapped values from the pitched grid's halo, which the
+   * library refreshes first, so they run for such a grid only when it is
+   * pitched (PSGrid*New). */
   int staged_type;
   int staged_emit;
   int read_lo[PSB_MAX_GRIDS][3];

@@ -395,11 +395,13 @@ psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, Gr
     if (g == og || g->type != cd.staged_type || g->pub.num_dims != 3 || !tma_eligible(g))
       return PSB_ERR_UNSUPPORTED;
     // Periodic reads take the wrapped values from the halo of a pitched grid.
+    // The read range of such a grid covers its plain reads too, so the range
+    // test below stays a sound choice between the two forms (plain reads
+    // outside the grid are checked; periodic ones never are).
     const bool per = cd.read_periodic[i] != 0;
     if (per && (g->layout != PSB_LAYOUT_PITCHED || g->halo < kGtR)) return PSB_ERR_UNSUPPORTED;
     for (int k = 0; k < 3; k++) {
-      if (!per &&
-          (d.lo[k] + cd.read_lo[i][k] < 0 || d.hi[k] - 1 + cd.read_hi[i][k] > g->pub.dim[k] - 1))
+      if (d.lo[k] + cd.read_lo[i][k] < 0 || d.hi[k] - 1 + cd.read_hi[i][k] > g->pub.dim[k] - 1)
         inside = false;
       if (d.hi[k] > g->pub.dim[k]) dom_inside = false;
     }
@@ -412,14 +414,7 @@ psb_status compiled_staged_launch(MapImpl &m, const psb_compiled_stencil &cd, Gr
       p.slots[gi] = i;
       p.mode[gi] = PSB_BOUNDARY_NONE;
     }
-    // One grid bound to parameters read both ways has no single window form.
-    if (p.mode[gi] != PSB_BOUNDARY_NONE && !per) return PSB_ERR_UNSUPPORTED;
-    if (per) {
-      for (int j = 0; j < i; j++)
-        if (views[j] == g && !cd.read_periodic[j] && cd.read_lo[j][0] <= cd.read_hi[j][0])
-          return PSB_ERR_UNSUPPORTED;
-      p.mode[gi] = PSB_BOUNDARY_PERIODIC;
-    }
+    if (per) p.mode[gi] = PSB_BOUNDARY_PERIODIC;
     tab.slot_grid[i] = gi;
     p.zmin = std::min(p.zmin, cd.read_lo[i][2]);
     p.zmax = std::max(p.zmax, cd.read_hi[i][2]);

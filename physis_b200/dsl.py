@@ -205,11 +205,11 @@ class StencilInfo:
         self.staged_ok = ndims == 3
         self.staged_reads = {}      # grid slot -> [lo[3], hi[3]]
         self.staged_rows = {}       # (slot, dy, dz) -> [dx min, dx max], in first-read order
-        # Grid slots read with PSGridGetPeriodic (only so: a grid read both
-        # ways rules the staged form out); the staged form takes their wrapped
-        # values from the pitched grid's refreshed halo.
+        # Grid slots read with PSGridGetPeriodic: the staged form takes their
+        # wrapped values from the pitched grid's refreshed halo (plain reads
+        # of the same grid stay inside it or are checked, so they never see
+        # the halo).
         self.staged_periodic = set()
-        self.staged_plain = set()
         self.emit_count = 0
         self.emit_slot = None
         self.staged = False
@@ -393,10 +393,8 @@ class _Rewriter:
                 any(f is None or f[0] != k or abs(f[1]) > 2 for k, f in enumerate(forms)):
             self.info.staged_ok = False
             return
-        (self.info.staged_periodic if periodic else self.info.staged_plain).add(slot)
-        if self.info.staged_periodic & self.info.staged_plain:
-            self.info.staged_ok = False
-            return
+        if periodic:
+            self.info.staged_periodic.add(slot)
         lo, hi = self.info.staged_reads.setdefault(slot, [[2, 2, 2], [-2, -2, -2]])
         for k, f in enumerate(forms):
             lo[k] = min(lo[k], f[1])

@@ -54,10 +54,10 @@ def test_compiled_stencil_matches_golden(name, layout, form, kernels):
 
 def _staged_form(info, case, layout):
     """Which form the library runs for the last map of the case: 0 the
-    function's own, 1 the staged form (every plain read range inside its grid
-    over the domain), 2 the checked staged form (a plain read range may leave
-    its grid, the domain lies inside every grid read). The staged forms need
-    a function that has them, no red-black colour, the emitted grid not read,
+    function's own, 1 the staged form (every read range inside its grid over
+    the domain), 2 the checked staged form (a read range may leave its grid,
+    the domain lies inside every grid read). The staged forms need a
+    function that has them, no red-black colour, the emitted grid not read,
     and pitched grids for periodic reads (their wrapped values come from the
     halo)."""
     if not info.staged:
@@ -74,8 +74,7 @@ def _staged_form(info, case, layout):
         if slots[param] == out:
             return 0
         dims = case["grids"][slots[param]][1]
-        if param not in info.staged_periodic and \
-                any(lo[k] + rlo[k] < 0 or hi[k] - 1 + rhi[k] > dims[k] - 1 for k in range(3)):
+        if any(lo[k] + rlo[k] < 0 or hi[k] - 1 + rhi[k] > dims[k] - 1 for k in range(3)):
             inside = False
         if any(hi[k] > dims[k] for k in range(3)):
             dom_inside = False
@@ -321,12 +320,14 @@ def test_periodic_reads_staged_match_oracle(layout, dims, tmp_path):
     """A 7-point stencil whose neighbour reads wrap (PSGridGetPeriodic) runs
     staged on pitched grids -- the wrapped values come from the refreshed
     halo -- and equals the oracle's periodic diffusion bit for bit over a
-    double-buffered run; dense grids (no halo) keep the function's own form.
-    A grid read both plainly and periodically has no staged form."""
+    double-buffered run, whether its centre read is plain (wrapdiff) or
+    periodic too (wrapdiff2); dense grids (no halo) keep the function's own
+    form. The wrapped reads leave the grid's extent at its faces, so the
+    checked staged form runs (it never checks a periodic read)."""
     from physis_b200 import dsl
     from oracle import oracle as O
     ks = dsl.compile_stencils(PERIODIC7_DSL + PERIODIC7_ONLY_DSL, str(tmp_path))
-    assert not ks["wrapdiff"].info.staged and ks["wrapdiff2"].info.staged
+    assert ks["wrapdiff"].info.staged and ks["wrapdiff2"].info.staged
     coef = [0.1, 0.11, 0.12, 0.13, 0.14, 0.15, 0.25]  # ce cw cn cs ct cb cc
     field = np.random.default_rng(5).random(dims[::-1], dtype=np.float32)
     want = O.diffusion7(field, 6, coef, periodic=True)
@@ -344,5 +345,5 @@ def test_periodic_reads_staged_match_oracle(layout, dims, tmp_path):
         finally:
             for x in g:
                 ps.PSGridFree(x)
-        assert staged == (1 if name == "wrapdiff2" and layout == "pitched" else 0), (name, layout)
+        assert staged == (2 if layout == "pitched" else 0), (name, layout)
         assert U.bits_equal(out, want), (name, layout)
