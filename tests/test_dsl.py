@@ -102,6 +102,53 @@ def test_generated_library_builds_for_sm100a(tmp_path):
         assert list(d.view_emits)[:d.nviews] == info.view_emits
         assert list(d.view_reads_offset)[:d.nviews] == info.view_reads_offset
         assert d.nparams == len(info.scalars) and d.launch
+        # The staged forms: both entry points or neither, the read ranges and
+        # the periodic flags of the grids the form reads.
+        assert bool(d.staged) == info.staged and bool(d.staged_checked) == info.staged
+        for slot in range(d.ngrids):
+            r = info.staged_reads.get(slot) if info.staged else None
+            lo, hi = list(d.read_lo[slot]), list(d.read_hi[slot])
+            if r is None:
+                assert lo[0] > hi[0] and not d.read_periodic[slot], (name, slot)
+            else:
+                assert [lo, hi] == r, (name, slot)
+                assert d.read_periodic[slot] == (slot in info.staged_periodic), (name, slot)
+
+
+def test_staged_form_eligibility():
+    """Which functions get staged forms: constant offsets within +-2, one
+    top-level emit into a grid not read; reads under face tests (checked at
+    run time) and periodic reads (from the halo), alone or mixed, qualify;
+    offsets beyond the halo, reads at run-time offsets and a read of the
+    emitted grid do not."""
+    src = """
+    void faces(const int x, const int y, const int z, PSGrid3DFloat u, PSGrid3DFloat v) {
+      float c = PSGridGet(u, x, y, z);
+      float w = x == 0 ? c : PSGridGet(u, x - 1, y, z);
+      PSGridEmit(v, c + w);
+    }
+    void wrap(const int x, const int y, const int z, PSGrid3DFloat u, PSGrid3DFloat v) {
+      PSGridEmit(v, PSGridGetPeriodic(u, x - 2, y, z) + PSGridGet(u, x, y, z + 1));
+    }
+    void far(const int x, const int y, const int z, PSGrid3DFloat u, PSGrid3DFloat v) {
+      PSGridEmit(v, PSGridGet(u, x + 3, y, z));
+    }
+    void moving(const int x, const int y, const int z, PSGrid3DFloat u, PSGrid3DFloat v,
+                int k) {
+      PSGridEmit(v, PSGridGet(u, x + k, y, z));
+    }
+    void inplace(const int x, const int y, const int z, PSGrid3DFloat u, PSGrid3DFloat v) {
+      PSGridEmit(v, PSGridGet(v, x, y, z) + PSGridGet(u, x, y, z));
+    }
+    """
+    _, infos = dsl.translate(src)
+    assert infos["faces"].staged and not infos["faces"].staged_periodic
+    assert infos["faces"].staged_reads == {0: [[-1, 0, 0], [0, 0, 0]]}
+    assert infos["wrap"].staged and infos["wrap"].staged_periodic == {0}
+    assert infos["wrap"].staged_reads == {0: [[-2, 0, 0], [0, 0, 1]]}
+    assert not infos["far"].staged
+    assert not infos["moving"].staged
+    assert not infos["inplace"].staged
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_TESTS), reason="reference sources not present")
